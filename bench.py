@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Throughput of the forced pseudospectral DNS step with droplets on one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the 256^3 configuration - FP32 fields and transforms, nu = 2.5e-3, dt = 1e-3,
+constant power eps = 0.1 on shells 1..2, RK2 + viscous integrating factor, end-of-step
+projection; 1e6 droplets with lognormal radii (median 0.002*2pi, sigma 0.3), tau ~ r^2 with median
+St = 0.5, tricubic interpolation, Stokes drag + settling g = 0.1, FP64 positions.  Inputs are
+seeded synthetic data of those shapes (the reference publishes no dataset); the working set
+(~1.3 GB per step) is far larger than L2, so no flush is needed between steps.
+
+A "step" is one full time step (two flow stages, two droplet stages, epilogue).  ``value`` is
+steps/s of the whole job (N replicas, one per GPU: the single-box step does not shard), timed on
+the device with CUDA events between barriers, max over ranks.  ``e2e`` is the same metric through
+ForcedDNS.step_host() with the state in pinned host memory (copied in and out every step).
+``--impl reference`` times the CPU restatement of the same step (FP64 NumPy/SciPy, all host
+cores) on rank 0.
+"""
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "steps/s at 256^3+1M droplets: FP32+learned interp vs plain FP64, same error"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--nd", type=int, default=1_000_000)
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--interp", choices=["trilinear", "tricubic", "cosine"], default="tricubic")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=150.0)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------------------------
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.proc = None
+        self.lines = []
+        try:
+            import torch
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={uuid}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel of the step
+# ---------------------------------------------------------------------------------------------
+def algorithmic_bytes(plan, nd):
+    """Compulsory HBM bytes per launch: every input read once, every output written once."""
+    N, My, Mzp, kc = plan.N, plan.My, plan.Mzp, plan.kc
+    r = 4 if plan.precision == "f32" else 8
+    c = 2 * r
+    cube = plan.Mx * My * Mzp * c
+    xrows = N * My * Mzp * c      # (N, My, Mzp): after/before the x pass
+    yrows = N * N * Mzp * c       # (N, N, Mzp): after/before the y pass
+    zin = N * N * (kc + 1) * c    # kz <= kc of one (N, N) set of rows
+    phys = N ** 3 * r
+    drop = 24 + 3 * r + r         # pos, vel, tau
+    return {
+        "xinv": 3 * cube + 6 * xrows,
+        "yinv": 6 * xrows + 6 * yrows,
+        "zcross": 6 * zin + 3 * yrows + 3 * phys,
+        "yfwd": 3 * yrows + 3 * xrows,
+        "xfwd_update": 3 * xrows + 7.5 * cube,       # mean of the two RK2 stages (9 and 6 cube fields)
+        "epilogue": 6 * cube,
+        "droplet1": nd * (drop + 3 * r) + 3 * phys,  # + a1 written; field read once
+        "droplet2": nd * (drop + 3 * r + 24 + 3 * r) + 3 * phys,
+        "forcing": 0,
+    }
+
+
+def load_traffic(kernel, N, precision):
+    """dram bytes per launch from the committed ncu summary (profiles/traffic.json), if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(f"{kernel}/{N}/{precision}")
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------------
+def build_workload(a, seed):
+    import torch
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    from lucky_droplets_b200.init import init_flow, init_droplets
+    nu, dt = (2.5e-3, 1e-3) if a.N == 256 else ((1e-3, 5e-4) if a.N == 512 else (0.01, 2e-3))
+    dns = ForcedDNS.config(a.N, nu, dt, eps=0.1, kf=2, precision=a.precision)
+    init_flow(dns, seed)
+    d = None
+    if a.nd > 0:
+        pos, tau, _ = init_droplets(a.nd, seed, "lognormal_r", nu=nu)
+        d = Droplets(dns.plan, pos, np.zeros((a.nd, 3)), tau, method=a.interp, g=0.1)
+        u = dns.velocity()
+        d.vel.copy_(d.gather(u))  # droplets start at the interpolated fluid velocity
+        del u
+        dns.attach(d)
+    torch.cuda.synchronize()
+    return dns, d
+
+
+def time_steps(dns, K, W, world):
+    import torch
+    s = torch.cuda.current_stream()
+    dns.step(W)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    dns.step(K)
+    e1.record(s)
+    torch.cuda.synchronize()
+    barrier(world)
+    return e0.elapsed_time(e1)
+
+
+def time_e2e(dns, d, K, W, world):
+    import torch
+    uk_h = torch.empty_like(dns.uk, device="cpu").pin_memory()
+    uk_h.copy_(dns.uk)
+    pos_h = vel_h = None
+    if d is not None:
+        pos_h = torch.empty_like(d.pos, device="cpu").pin_memory()
+        vel_h = torch.empty_like(d.vel, device="cpu").pin_memory()
+        pos_h.copy_(d.pos)
+        vel_h.copy_(d.vel)
+    for _ in range(W):
+        dns.step_host(uk_h, pos_h, vel_h)
+    barrier(world)
+    torch.cuda.synchronize()
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(K):
+        dns.step_host(uk_h, pos_h, vel_h)
+    e1.record(s)
+    torch.cuda.synchronize()
+    barrier(world)
+    nbytes = uk_h.numel() * uk_h.element_size()
+    if d is not None:
+        nbytes += pos_h.numel() * pos_h.element_size() + vel_h.numel() * vel_h.element_size()
+    return e0.elapsed_time(e1), nbytes
+
+
+def profile_kernels(dns, d, P):
+    """Per-kernel device time over P steps with launch-bracketing events on the launch stream."""
+    import torch
+    p = dns.plan
+    p.profile_read(reset=True)
+    p.profile(True)
+    dns.step(P)
+    torch.cuda.synchronize()
+    prof = p.profile_read(reset=True)
+    p.profile(False)
+    return prof
+
+
+def cpu_baseline(dns, d, a):
+    """The FP64 CPU restatement of the same step (oracle/config_np) on this host's cores, one
+    step from the same state: a bounded sample of the workload."""
+    import torch
+    from oracle import config_np as C
+    N = dns.N
+    grid = C.ConfigGrid(N)
+    prm = C.ConfigParams(N=N, nu=dns.nu, dt=dns.dt, eps=0.1, kf=2, g=0.1)
+    uk = dns.uk_full()
+    pos = d.pos.cpu().numpy() if d is not None else None
+    vel = d.vel.cpu().numpy().astype(np.float64) if d is not None else None
+    tau = d.tau.cpu().numpy().astype(np.float64) if d is not None else None
+    del torch
+    t0 = time.perf_counter()
+    C.step(grid, prm, uk, pos, vel, tau, a.interp)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": "steps/s", "cores": C._WORKERS, "kind": "port",
+            "sample": f"1 full step of the same workload ({N}^3 FP64 RK2+IF flow, {a.nd} droplets "
+                      f"{a.interp}), {dt:.2f} s; NumPy/SciPy FP64 restatement, scipy.fft workers={C._WORKERS}"}
+
+
+def run_ours(a):
+    import torch
+    world, rank, local = dist_setup()
+    from lucky_droplets_b200 import _lib
+    dns, d = build_workload(a, a.seed + 1000 * rank)
+    clocks = ClockSampler(local)
+    ms = time_steps(dns, a.steps, a.warmup, world)
+    clk = clocks.stop()
+    flags = dns.check()
+    ms = allreduce_max(ms, world)
+    ms_per_step = ms / a.steps
+    value = world * a.steps / (ms / 1e3)
+    # per-kernel timing and the roofline of the dominant kernel
+    P = max(1, a.profile_steps)
+    prof = profile_kernels(dns, d, P)
+    launches_per_step = sum(c for c, _ in prof.values()) / P
+    algo = algorithmic_bytes(dns.plan, a.nd)
+    kernels = {}
+    for name, (cnt, tms) in prof.items():
+        avg = tms / cnt
+        b = algo.get(name)
+        kernels[name] = {"launches_per_step": cnt / P, "avg_ms": avg, "share": tms / sum(t for _, t in prof.values()),
+                         "algo_bytes": b, "gbs": (b / (avg * 1e-3) / 1e9) if b else None}
+    dom = max((k for k in kernels if algo.get(k)), key=lambda k: kernels[k]["share"] * 1.0)
+    peak, peak_kind = measured_peaks()
+    kd = kernels[dom]
+    roof = {"bound": "hbm", "kernel": dom, "achieved": kd["gbs"], "peak": peak, "unit": "GB/s",
+            "frac": kd["gbs"] / peak, "peak_source": peak_kind,
+            "traffic": load_traffic(dom, a.N, a.precision),
+            "algo_bytes_per_launch": kd["algo_bytes"], "avg_launch_ms": kd["avg_ms"]}
+    step_bytes = sum((algo.get(k) or 0) * v["launches_per_step"] for k, v in kernels.items())
+    out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32" if a.precision == "f32" else "f64", "data": "synthetic",
+           "config": {"workload": f"{a.N}^3 DNS RK2+IF (nu=2.5e-3, dt=1e-3, eps=0.1 on shells 1-2) + "
+                                  f"{a.nd} droplets {a.interp}, Heun, settling g=0.1",
+                      "N": a.N, "n_droplets": a.nd, "interp": a.interp, "precision": a.precision,
+                      "parallelism": f"replicas x{world}", "l2": "working set > 1 GB per step (> L2); no flush"},
+           "droplet_steps_per_s": value * a.nd,
+           "step_algo_gbs": step_bytes / (ms_per_step * 1e-3) / 1e9,
+           "roofline": roof,
+           "kernels": kernels,
+           "gpu_launches": int(round(launches_per_step * a.steps)),
+           "status_flags": flags,
+           "clocks": clk}
+    if not a.no_e2e:
+        Ke = max(3, min(a.steps, 10))
+        ems, nbytes = time_e2e(dns, d, Ke, 1, world)
+        ems = allreduce_max(ems, world)
+        out["e2e"] = {"value": world * Ke / (ems / 1e3), "unit": "steps/s", "h2d_bytes_per_step": nbytes,
+                      "d2h_bytes_per_step": nbytes, "api": "ForcedDNS.step_host (pinned host state in/out)"}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(dns, d, a)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------------------------
+# reference arm: the CPU restatement of the same step on this host
+# ---------------------------------------------------------------------------------------------
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from oracle import config_np as C
+    nu, dt = (2.5e-3, 1e-3) if a.N == 256 else ((1e-3, 5e-4) if a.N == 512 else (0.01, 2e-3))
+    prm = C.ConfigParams(N=a.N, nu=nu, dt=dt, eps=0.1, kf=2, g=0.1)
+    grid = C.ConfigGrid(a.N)
+    uk, u = C.init_flow(grid, prm, a.seed)
+    pos = tau = vel = None
+    if a.nd > 0:
+        pos, tau, _ = C.init_droplets(prm, a.seed, "lognormal_r", nd=a.nd)
+        vel = C.gather(u, pos, a.interp)
+    del u
+    t_first = None
+    done, total = 0, 0.0
+    for i in range(max(0, min(a.warmup, 1))):
+        t0 = time.perf_counter()
+        uk, pos, vel = C.step(grid, prm, uk, pos, vel, tau, a.interp)
+        t_first = time.perf_counter() - t0
+    for i in range(a.steps):
+        t0 = time.perf_counter()
+        uk, pos, vel = C.step(grid, prm, uk, pos, vel, tau, a.interp)
+        total += time.perf_counter() - t0
+        done += 1
+        if total > a.cpu_budget_s:
+            break
+    value = done / total
+    sample = (f"{done} of {a.steps} requested steps timed (bounded to ~{a.cpu_budget_s:.0f} s), "
+              f"warm-up {min(a.warmup, 1)}; FP64 NumPy/SciPy restatement of the step, scipy.fft workers={C._WORKERS}")
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+           "steps": done, "warmup": min(a.warmup, 1), "ms_per_step": 1e3 * total / done, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"{a.N}^3 DNS RK2+IF (nu={nu}, dt={dt}, eps=0.1 on shells 1-2) + "
+                                  f"{a.nd} droplets {a.interp}, Heun, settling g=0.1",
+                      "N": a.N, "n_droplets": a.nd, "interp": a.interp},
+           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": C._WORKERS, "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main(argv=None):
+    a = parse_args(argv)
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

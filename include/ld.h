@@ -1,0 +1,167 @@
+/*
+ * lucky-droplets B200: C ABI of the forced pseudospectral DNS step with droplets.
+ *
+ * The reference (Rajarshi-prime/lucky-droplets) is a pair of Python scripts with no FFI; the
+ * entry points below replace its Python functions one for one, with plain pointers and sizes.
+ * Citations are file:line in the reference (forced-dns-sm.py = F, particles.py = P).
+ *
+ * Conventions
+ *  - Every pointer is a device pointer unless its name ends in _host.  The caller owns every
+ *    buffer; a plan owns only its twiddle tables, operator tables and transform workspace.
+ *  - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).  No call
+ *    synchronises the host except ld_status() and the *_host copies it documents.
+ *  - Return value: LD_OK (0) or a negative LD_ERR_*.  ld_last_error() describes the last failure
+ *    of the calling thread.  A plan is not thread-safe: use one plan per stream.
+ *  - Precision of a plan: LD_F32 (float / complex float) or LD_F64 (double / complex double);
+ *    droplet positions are double in both.
+ *
+ * Spectral layouts (complex, kz fastest):
+ *  - reference layout "full": (N, N, N/2+1) indexed (kx, ky, kz) with kx, ky in FFT order, exactly
+ *    the array rfft_mpi returns on one rank (F:201-206, F:158);
+ *  - "cube": the dealiased cube (Mx, My, Mzp) with Mx = My = 2 kc + 1, kc = floor(N/3),
+ *    kx, ky in [-kc, kc] stored 0..kc then -kc..-1, kz in [0, kc] padded with zeros to Mzp (a
+ *    multiple of 8).  Every mode the spherical mask of F:129 keeps lies in the cube.
+ * Physical layout: (N, N, N) real indexed (x, y, z), z fastest, as u[c] of F:150.
+ */
+#ifndef LUCKY_DROPLETS_LD_H
+#define LUCKY_DROPLETS_LD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LD_API __attribute__((visibility("default")))
+#else
+#define LD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LD_OK 0
+#define LD_ERR_ARG (-1)
+#define LD_ERR_CUDA (-2)
+#define LD_ERR_UNSUPPORTED (-3)
+#define LD_ERR_CAPACITY (-4)
+#define LD_ERR_NOMEM (-5)
+
+#define LD_F32 0
+#define LD_F64 1
+
+/* Device status word bits (ld_status). */
+#define LD_STATUS_NONFINITE 1u     /* NaN/Inf met in the state                          */
+#define LD_STATUS_BLOWUP 2u        /* max Re(uk) > 100 N^3, the abort test of F:618-620  */
+#define LD_STATUS_PAIR_OVERFLOW 4u /* collision pair list exceeded its capacity          */
+#define LD_STATUS_WAIT_TIMEOUT 8u  /* a bounded device wait gave up                      */
+
+/* Droplet interpolation kernels. */
+#define LD_INTERP_TRILINEAR 0
+#define LD_INTERP_TRICUBIC 1   /* tensor-product 4-point Lagrange on offsets -1..2          */
+#define LD_INTERP_COSINE 2     /* (1 + cos(pi r / 2dx)) / 4 on offsets -1..2, P:6-20, P:435-511 */
+
+typedef struct ld_plan ld_plan;
+
+/* Flow parameters of one time step. */
+typedef struct ld_flow_params {
+  double dt;        /* time step h (F:29, F:559)                                     */
+  double nu;        /* kinematic viscosity (F:83)                                    */
+  double f0;        /* power injected per forced shell (F:97)                        */
+  int32_t kf_lo;    /* first forced shell (F:90: shell_no = 1..nshells)              */
+  int32_t kf_hi;    /* last forced shell                                             */
+} ld_flow_params;
+
+/* ---- library ------------------------------------------------------------------------- */
+LD_API int ld_version(void);
+LD_API const char* ld_last_error(void);
+
+/* ---- plans: grid and spectral operators of F:49-141 ---------------------------------- */
+/* Builds the twiddle tables (FP64, rounded once to the plan precision), operator tables and
+ * transform workspace for an N^3 grid, N a power of two in [16, 512]. */
+LD_API int ld_plan_create(ld_plan** plan, int n, int precision);
+LD_API int ld_plan_destroy(ld_plan* plan);
+/* dims[0..7] = N, kc, Mx, My, Mz, Mzp, Nf, precision; work_bytes = transform workspace. */
+LD_API int ld_plan_dims(const ld_plan* plan, int32_t* dims, size_t* work_bytes);
+
+/* ---- transforms, F:201-213 ---------------------------------------------------------- */
+/* rfft_mpi (F:201-206) on one GPU: ncomp real (N,N,N) fields -> ncomp full-layout spectra,
+ * unnormalised forward transform (scipy.fft convention). */
+LD_API int ld_rfft_mpi(ld_plan* plan, const void* u, void* fu, int ncomp, void* stream);
+/* irfft_mpi (F:208-213): full-layout spectra -> real fields, 1/N^3 normalisation; the imaginary
+ * parts of the kz = 0 and kz = N/2 coefficients are ignored, as pocketfft's c2r does. */
+LD_API int ld_irfft_mpi(ld_plan* plan, const void* fu, void* u, int ncomp, void* stream);
+/* Dealiased transforms in the cube layout: the same transforms restricted to the modes of the
+ * spherical mask (F:129) - the form every transform of the DNS step takes. */
+LD_API int ld_irfft_cube(ld_plan* plan, const void* uk, void* u, int ncomp, void* stream);
+LD_API int ld_rfft_cube(ld_plan* plan, const void* u, void* uk, int ncomp, void* stream);
+/* full -> cube: dealias * full (F:567-569 applies dealias after rfft_mpi); cube -> full. */
+LD_API int ld_spec_to_cube(ld_plan* plan, const void* full, void* cube, int ncomp, void* stream);
+LD_API int ld_spec_from_cube(ld_plan* plan, const void* cube, void* full, int ncomp, void* stream);
+
+/* ---- spectrum and forcing, F:232-275 ------------------------------------------------- */
+/* Shell energy spectrum e3d_to_e1d(0.5 |uk|^2 normalize) (F:232-233, F:243-245) of a cube-layout
+ * 3-vector, FP64, ek[0..N/2] (modes with |k| > N/2 + 1/2 are not counted, as np.histogram drops
+ * them).  Deterministic: fixed-order FP64 reduction. */
+LD_API int ld_shell_spectrum(ld_plan* plan, const void* uk, double* ek, void* stream);
+
+/* ---- flow right-hand side, F:287-316 -------------------------------------------------- */
+/* ku = P[(u x omega)^ + f] * dealias - visc * nu k^2 uk for a cube-layout 3-vector uk, with
+ * the constant-power forcing f of F:239-275 on shells kf_lo..kf_hi (f0 = 0 switches it off).
+ * If u_out is not NULL the physical velocity (3, N, N, N) is written too. */
+LD_API int ld_velocity_rhs(ld_plan* plan, const void* uk, void* ku, void* u_out,
+                    const ld_flow_params* prm, double visc, void* stream);
+
+/* ---- time integration ----------------------------------------------------------------- */
+/* RK2 (Heun) with viscous integrating factor E = exp(-nu k^2 h), one stage per call:
+ *   stage 1: N1 = N(uk);    ustar = E (uk + h N1);  acc = E (uk + h/2 N1)
+ *   stage 2: N2 = N(ustar); uk = acc + h/2 N2
+ * N is the RHS above without the viscous term.  u_out (nullable) receives the physical
+ * velocity of the stage input (uk at stage 1, ustar at stage 2) for the droplet stages. */
+LD_API int ld_rk2if_stage(ld_plan* plan, int stage, void* uk, void* ustar, void* acc, void* u_out,
+                   const ld_flow_params* prm, void* stream);
+/* Classical RK4 with explicit viscosity, one stage per call (F:335-362):
+ *   stage s evaluates ku_s = RHS(y_s) with y_1 = uk and
+ *   s=1: acc = uk + h/6 ku1, y = uk + h/2 ku1;  s=2: acc += h/3 ku2, y = uk + h/2 ku2;
+ *   s=3: acc += h/3 ku3, y = uk + h ku3;        s=4: uk = acc + h/6 ku4.
+ * u_out (nullable) receives the physical velocity of y_s. */
+LD_API int ld_rk4_stage(ld_plan* plan, int stage, void* uk, void* y, void* acc, void* u_out,
+                 const ld_flow_params* prm, void* stream);
+/* End of a time step, F:596-620: the irfft->rfft "reality" round trip (which symmetrises the
+ * kz = 0 plane: uk(k) <- (uk(k) + conj uk(-k)) / 2), the div-free projection, and the blow-up
+ * and NaN test, which raises LD_STATUS_BLOWUP / LD_STATUS_NONFINITE in the status word. */
+LD_API int ld_step_epilogue(ld_plan* plan, void* uk, void* stream);
+
+/* ---- droplets, P:52-111, P:435-511, P:817-837 ----------------------------------------- */
+/* Interpolate ncomp physical fields (ncomp, N, N, N) at n positions (n, 3) double:
+ * out (n, ncomp) in the plan precision.  Positions are taken modulo L = 2 pi. */
+LD_API int ld_gather(ld_plan* plan, const void* field, int ncomp, const double* pos, int64_t n,
+              int method, void* out, void* stream);
+/* Droplet Heun stage on one flow stage (x' = v, v' = (u(x) - v)/tau - g z; the reference's drag
+ * and gravity terms, P:831-834, with tau given per droplet):
+ *   stage 1: a1 = (u(x) - v)/tau - g z                                         (writes a1)
+ *   stage 2: xs = x + h v, vs = v + h a1, a2 = (u(xs) - vs)/tau - g z,
+ *            x <- x + h/2 (v + vs), v <- v + h/2 (a1 + a2)                      (writes x, v)
+ * pos (n,3) double, vel (n,3) and a1 (n,3) and tau (n) in the plan precision. */
+LD_API int ld_droplet_stage(ld_plan* plan, int stage, const void* u, double* pos, void* vel,
+                     const void* tau, void* a1, int64_t n, int method, double h, double g,
+                     void* stream);
+
+/* ---- tracing -------------------------------------------------------------------------- */
+/* The reference times only whole steps on the wall clock (F:565-577, F:627).  With tracing on, a
+ * plan brackets each of its kernel launches with CUDA events on the launching stream. */
+LD_API int ld_profile(ld_plan* plan, int enable);
+/* Per kernel id: launches and summed device time (ms) since the last reset; synchronises the
+ * recorded events.  Writes up to cap entries and their number to *n_out. */
+LD_API int ld_profile_read(ld_plan* plan, int32_t* kid, int64_t* count, double* total_ms, int cap,
+                           int32_t* n_out, int reset);
+/* Name of a kernel id ("zcross", "xfwd_update", ...), or NULL. */
+LD_API const char* ld_kernel_name(int kid);
+
+/* ---- status ------------------------------------------------------------------------- */
+/* Reads (and with clear != 0 resets) the plan's device status word.  Synchronises `stream`. */
+LD_API int ld_status(ld_plan* plan, uint32_t* flags, int clear, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUCKY_DROPLETS_LD_H */

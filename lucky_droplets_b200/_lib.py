@@ -1,0 +1,101 @@
+"""ctypes binding of liblucky_droplets.so (the C ABI declared in include/ld.h).
+
+The library is built in-tree by ``python -m lucky_droplets_b200.build``.  There is no CPU
+fallback: if the library is missing or no CUDA device is present, every entry point raises.
+"""
+import ctypes
+import pathlib
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "liblucky_droplets.so"
+
+LD_OK = 0
+LD_F32, LD_F64 = 0, 1
+LD_INTERP = {"trilinear": 0, "tricubic": 1, "cosine": 2}
+STATUS_NONFINITE = 1
+STATUS_BLOWUP = 2
+STATUS_PAIR_OVERFLOW = 4
+STATUS_WAIT_TIMEOUT = 8
+
+_c_p = ctypes.c_void_p
+_c_i = ctypes.c_int
+_c_i32 = ctypes.c_int32
+_c_i64 = ctypes.c_int64
+_c_d = ctypes.c_double
+_c_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class FlowParams(ctypes.Structure):
+    """ld_flow_params of include/ld.h."""
+    _fields_ = [("dt", _c_d), ("nu", _c_d), ("f0", _c_d), ("kf_lo", _c_i32), ("kf_hi", _c_i32)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "ld_version": (_c_i, []),
+    "ld_last_error": (ctypes.c_char_p, []),
+    "ld_plan_create": (_c_i, [ctypes.POINTER(_c_p), _c_i, _c_i]),
+    "ld_plan_destroy": (_c_i, [_c_p]),
+    "ld_plan_dims": (_c_i, [_c_p, ctypes.POINTER(_c_i32), ctypes.POINTER(ctypes.c_size_t)]),
+    "ld_rfft_mpi": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_irfft_mpi": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_irfft_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_rfft_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_spec_to_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_spec_from_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_shell_spectrum": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
+    "ld_velocity_rhs": (_c_i, [_c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_d, _c_p]),
+    "ld_rk2if_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_p]),
+    "ld_rk4_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_p]),
+    "ld_step_epilogue": (_c_i, [_c_p, _c_p, _c_p]),
+    "ld_gather": (_c_i, [_c_p, _c_p, _c_i, _c_p, _c_i64, _c_i, _c_p, _c_p]),
+    "ld_droplet_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_i, _c_d, _c_d, _c_p]),
+    "ld_profile": (_c_i, [_c_p, _c_i]),
+    "ld_profile_read": (_c_i, [_c_p, ctypes.POINTER(_c_i32), ctypes.POINTER(_c_i64), _c_dp, _c_i,
+                               ctypes.POINTER(_c_i32), _c_i]),
+    "ld_kernel_name": (ctypes.c_char_p, [_c_i]),
+    "ld_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),
+}
+
+
+class LDError(RuntimeError):
+    """A negative status from the C ABI, with ld_last_error()'s message."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"lucky_droplets error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the library once and declare every signature; raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH.name} is not built; run `python -m lucky_droplets_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != LD_OK:
+        raise LDError(rc, lib().ld_last_error().decode(errors="replace"))
+    return rc
+
+
+def ptr(t):
+    """Raw device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream_ptr(stream=None):
+    import torch
+    s = torch.cuda.current_stream() if stream is None else stream
+    return ctypes.c_void_p(s.cuda_stream)

@@ -1,0 +1,780 @@
+// Kernel templates of the DNS step: the three axis passes of the 3D real transform, the fused
+// nonlinear-term z pass, the k-space update epilogues, spectra/forcing and the droplet kernels.
+//
+// Data layout (see include/ld.h): physical fields (N,N,N) z fastest; spectra either in the
+// reference's full layout (N, N, Nf) or in the dealiased cube (Mx, My, Mzp).
+//
+// Transform structure for the DNS (cube layout, c = complex element):
+//   inverse : x pass (cube rows kx -> N rows x)  |  y pass (My rows ky -> N rows y)
+//             |  z pass (kz <= kc -> N reals z)
+//   forward : z pass (N reals -> kz < Mzp)  |  y pass (N rows -> My rows)  |  x pass (N -> Mx)
+// Rows that are zero on input (|k| > kc) are never read and rows outside the cube are never
+// written, so each pass moves only the data the dealiased spectrum needs.
+#pragma once
+#include <type_traits>
+
+#include "ld_fft.cuh"
+
+namespace ld {
+
+// ------------------------------------------------------------------------------------------
+// index helpers
+// ------------------------------------------------------------------------------------------
+// logical FFT index n in [0, N) -> compact cube row, or -1 when |freq| > kc
+__device__ __forceinline__ int crow(int n, int N, int kc) {
+  return n <= kc ? n : (n >= N - kc ? n - (N - 2 * kc - 1) : -1);
+}
+// compact cube row -> signed frequency
+__device__ __forceinline__ int cfreq(int i, int kc) { return i <= kc ? i : i - (2 * kc + 1); }
+// logical FFT index -> signed frequency (fftfreq convention: N/2 -> -N/2)
+__device__ __forceinline__ int nfreq(int n, int N) { return n < N / 2 ? n : n - N; }
+
+template <int N> struct Cfg {
+  // column passes: E elements per thread, TB columns per CTA
+  static constexpr int EC = (N == 32 || N == 64) ? 8 : 16;
+  static constexpr int NTC = N / EC;
+  static constexpr int TB = N == 16 ? 64 : (N == 32 ? 32 : 16);
+  static constexpr int COL_THREADS = TB * NTC;
+  // z passes: E elements per thread, NTZ threads per row (a row never spans two warps)
+  static constexpr int EZ = N >= 512 ? 16 : 8;
+  static constexpr int NTZ = N / EZ;
+  static constexpr int ZTHREADS = 256;
+  static constexpr int ZROWS = ZTHREADS / NTZ;  // row units per CTA
+  static constexpr int LOGEZ = ilog2(EZ);
+  static constexpr int ZBUF = N + N / EZ;       // padded row buffer (bank-conflict free)
+};
+
+// ------------------------------------------------------------------------------------------
+// column (strided axis) passes
+// ------------------------------------------------------------------------------------------
+// Plain strided loader/storer: element (f, o, row, col) at f*fs + o*os + row*rs + col, with an
+// optional cube row map (kc >= 0) on the transform axis.
+template <typename T> struct RowsIO {
+  cplx<T>* p;
+  long long fs, os;
+  int rs;
+  int kc;  // < 0: identity row map
+  T scale;
+  __device__ __forceinline__ long long at(int f, int o, int r, int col) const {
+    return (long long)f * fs + (long long)o * os + (long long)r * rs + col;
+  }
+};
+
+template <typename T, int N> struct LdRows {
+  RowsIO<T> io;
+  __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
+    const int r = io.kc < 0 ? n : crow(n, N, io.kc);
+    if (r < 0) return czero<cplx<T>>();
+    cplx<T> v = io.p[io.at(f, o, r, col)];
+    return cscale(v, io.scale);
+  }
+};
+
+template <typename T, int N> struct StRows {
+  RowsIO<T> io;
+  __device__ __forceinline__ void operator()(int f, int o, int n, int col, cplx<T> v) const {
+    const int r = io.kc < 0 ? n : crow(n, N, io.kc);
+    if (r < 0) return;
+    io.p[io.at(f, o, r, col)] = v;
+  }
+};
+
+// Storer into the cube that also applies the spherical mask round(|k|) <= kc (F:129): the last
+// (x) pass of a forward cube transform.  Columns are the flat (ky, kz) index of a kx plane.
+template <typename T, int N> struct StCube {
+  RowsIO<T> io;  // io.kc = kc (compact rows), io.rs = My * Mzp
+  int Mzp;
+  __device__ __forceinline__ void operator()(int f, int o, int n, int col, cplx<T> v) const {
+    const int kc = io.kc;
+    const int r = crow(n, N, kc);
+    if (r < 0) return;
+    const int kx = n <= kc ? n : n - N;
+    const int iy = col / Mzp;
+    const int ky = cfreq(iy, kc), kz = col - iy * Mzp;
+    if (kz > kc || kx * kx + ky * ky + kz * kz > kc * kc + kc) v = czero<cplx<T>>();
+    io.p[io.at(f, o, r, col)] = v;
+  }
+};
+
+// Inverse x-pass loader producing [u_x, u_y, u_z, w_x, w_y, w_z] from a cube 3-vector:
+// w = i k x u (F:295-297).  Columns are the flat (ky, kz) index of a kx plane.
+template <typename T, int N> struct LdCurl {
+  const cplx<T>* u;
+  long long cs;  // component stride (cube elements)
+  int kc, My, Mzp;
+  __device__ __forceinline__ cplx<T> operator()(int f, int, int n, int col) const {
+    const int r = crow(n, N, kc);
+    if (r < 0) return czero<cplx<T>>();
+    const long long b = (long long)r * My * Mzp + col;
+    if (f < 3) return u[f * cs + b];
+    const T kx = T(n <= kc ? n : n - N);
+    const int iy = col / Mzp;
+    const T ky = T(cfreq(iy, kc));
+    const T kz = T(col - iy * Mzp);
+    cplx<T> w;
+    if (f == 3) {        // i (ky u_z - kz u_y)
+      cplx<T> uy = u[cs + b], uz = u[2 * cs + b];
+      w = cmuli(csub(cscale(uz, ky), cscale(uy, kz)));
+    } else if (f == 4) { // i (kz u_x - kx u_z)
+      cplx<T> ux = u[b], uz = u[2 * cs + b];
+      w = cmuli(csub(cscale(ux, kz), cscale(uz, kx)));
+    } else {             // i (kx u_y - ky u_x)
+      cplx<T> ux = u[b], uy = u[cs + b];
+      w = cmuli(csub(cscale(uy, kx), cscale(ux, ky)));
+    }
+    return w;
+  }
+};
+
+// One CTA = TB columns x NT threads; blockIdx.x = tile * nf + field (fields of a tile launch
+// together so their shared inputs are served from L2), blockIdx.y = outer index.
+template <typename T, int N, bool INV, class Ld, class St>
+__global__ void __launch_bounds__(Cfg<N>::COL_THREADS)
+k_colfft(Ld ld, St st, int ncols, int nf, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int c = threadIdx.x % TB, j = threadIdx.x / TB;
+  const int field = blockIdx.x % nf;
+  const int col = (blockIdx.x / nf) * TB + c;
+  const bool ok = col < ncols;
+  const int outer = blockIdx.y;
+  cplx<T> a[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) a[m] = ok ? ld(field, outer, j + NT * m, col) : czero<cplx<T>>();
+  fft_run<T, N, E, INV, false>(a, sbuf + c, TB, j, tw, SyncBlock());
+  if (ok) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) st(field, outer, j + NT * m, col, a[m]);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// k-space update epilogue of the forward x pass (F:304-316 + the time integrators)
+// ------------------------------------------------------------------------------------------
+enum UpdMode : int {
+  UPD_RHS = 0,     // s0 <- P[nl + f] - visc nu k^2 s1               (s1 = stage input)
+  UPD_RK2_1 = 1,   // s1 = uk: s0 <- E (uk + h N1) [ustar], s2 <- E (uk + h/2 N1) [acc]
+  UPD_RK2_2 = 2,   // s1 = ustar: s0 <- s2 + h/2 N2                   (s0 = uk, s2 = acc)
+  UPD_RK4_1 = 3,   // s0 = un, s1 = stage input, s2 = acc, s3 = next stage input
+  UPD_RK4_2 = 4,
+  UPD_RK4_3 = 5,
+  UPD_RK4_4 = 6,
+};
+
+template <typename T> struct UpdArgs {
+  const cplx<T>* nl;  // forward-transformed (u x w): (3, N, My, Mzp) rows x = N
+  long long nls;      // component stride of nl
+  cplx<T>* s0;
+  cplx<T>* s1;
+  cplx<T>* s2;
+  cplx<T>* s3;
+  long long cs;       // component stride of the cube
+  const double* factor;  // forcing factor per shell (FP64), shells kf_lo..kf_hi
+  int kf_lo, kf_hi;
+  const T* ifac;         // exp(-nu h k^2) by k^2
+  T h, nu, visc;
+  int kc, My, Mzp;
+  unsigned* status;
+};
+
+template <typename T, int N, int MODE>
+__global__ void __launch_bounds__(Cfg<N>::COL_THREADS)
+k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int c = threadIdx.x % TB, j = threadIdx.x / TB;
+  const int col = blockIdx.x * TB + c;
+  const bool ok = col < ncols;
+  cplx<T> res[3][E];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+#pragma unroll
+    for (int m = 0; m < E; ++m)
+      res[f][m] = ok ? A.nl[f * A.nls + (long long)(j + NT * m) * ncols + col] : czero<cplx<T>>();
+    if (f) __syncthreads();
+    fft_run<T, N, E, false, false>(res[f], sbuf + c, TB, j, tw, SyncBlock());
+  }
+  if (!ok) return;
+  const int iy = col / A.Mzp;
+  const int kzi = col - iy * A.Mzp;
+  const int kyi = cfreq(iy, A.kc);
+  const T ky = T(kyi), kz = T(kzi);
+  const int kc = A.kc;
+  unsigned flags = 0;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int n = j + NT * m;
+    const int r = crow(n, N, kc);
+    if (r < 0) continue;
+    const int kxi = n <= kc ? n : n - N;
+    const T kx = T(kxi);
+    const int k2 = kxi * kxi + kyi * kyi + kzi * kzi;
+    const long long idx = (long long)r * A.My * A.Mzp + col;
+    const bool keep = (kzi <= kc) && (k2 <= kc * kc + kc);  // round(|k|) <= kc  (F:129)
+    cplx<T> y[3];  // the stage input
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) y[cc] = A.s1[cc * A.cs + idx];
+    cplx<T> rhs[3];
+    if (keep) {
+      // forcing on shells kf_lo..kf_hi: factor[kint] * y  (F:253-264)
+      T fac = T(0);
+      if (k2 <= A.kf_hi * A.kf_hi + A.kf_hi) {
+        int s = 0;
+        while (s * s + s < k2) ++s;  // s = round(sqrt(k2))
+        if (s >= A.kf_lo) fac = T(A.factor[s]);
+      }
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) rhs[cc] = cadd(res[cc][m], cscale(y[cc], fac));
+      if (k2 > 0) {  // pressure projection, invlap = -1/k^2 (F:309-316)
+        const T inv = T(1) / T(k2);
+        cplx<T> kd = cadd(cadd(cscale(rhs[0], kx), cscale(rhs[1], ky)), cscale(rhs[2], kz));
+        kd = cscale(kd, inv);
+        rhs[0] = csub(rhs[0], cscale(kd, kx));
+        rhs[1] = csub(rhs[1], cscale(kd, ky));
+        rhs[2] = csub(rhs[2], cscale(kd, kz));
+      }
+    } else {
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) rhs[cc] = czero<cplx<T>>();
+    }
+    const T h = A.h;
+    if (MODE == UPD_RHS) {
+      const T lv = A.visc * A.nu * T(k2);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) A.s0[cc * A.cs + idx] = csub(rhs[cc], cscale(y[cc], lv));
+    } else if (MODE == UPD_RK2_1) {
+      const T Ef = keep ? A.ifac[k2] : T(0);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        cplx<T> us = cscale(cadd(y[cc], cscale(rhs[cc], h)), Ef);
+        cplx<T> ac = cscale(cadd(y[cc], cscale(rhs[cc], T(0.5) * h)), Ef);
+        A.s0[cc * A.cs + idx] = us;
+        A.s2[cc * A.cs + idx] = ac;
+      }
+    } else if (MODE == UPD_RK2_2) {
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        cplx<T> v = cadd(A.s2[cc * A.cs + idx], cscale(rhs[cc], T(0.5) * h));
+        if (!keep) v = czero<cplx<T>>();
+        if (!(isfinite(v.x) && isfinite(v.y))) flags |= LD_STATUS_NONFINITE;
+        A.s0[cc * A.cs + idx] = v;
+      }
+    } else {
+      // RK4 (F:341-360): ku = rhs - nu k^2 y ;  y = stage input
+      const T lv = A.nu * T(k2);
+      cplx<T> ku[3];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) ku[cc] = csub(rhs[cc], cscale(y[cc], lv));
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const long long o = cc * A.cs + idx;
+        if (MODE == UPD_RK4_1) {
+          cplx<T> un = y[cc];
+          A.s2[o] = cadd(un, cscale(ku[cc], h / T(6)));
+          A.s3[o] = cadd(un, cscale(ku[cc], h / T(2)));
+        } else if (MODE == UPD_RK4_2 || MODE == UPD_RK4_3) {
+          cplx<T> un = A.s0[o];
+          A.s2[o] = cadd(A.s2[o], cscale(ku[cc], h / T(3)));
+          A.s3[o] = cadd(un, cscale(ku[cc], MODE == UPD_RK4_2 ? h / T(2) : h));
+        } else {
+          cplx<T> v = cadd(A.s2[o], cscale(ku[cc], h / T(6)));
+          if (!(isfinite(v.x) && isfinite(v.y))) flags |= LD_STATUS_NONFINITE;
+          A.s0[o] = v;
+        }
+      }
+    }
+  }
+  if (flags) atomicOr(A.status, flags);
+}
+
+// ------------------------------------------------------------------------------------------
+// z passes (contiguous axis): one thread group of NTZ threads per row unit, inside one warp
+// ------------------------------------------------------------------------------------------
+// Exchange barrier of the z passes: warp-level when a row unit owns a whole warp (N >= 256),
+// block-wide when several row units share a warp (the warp-level form gave wrong results for
+// N <= 32 in the fused pass; the block-wide form is verified at every size).
+template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ >= 32), SyncWarp, SyncBlock>::type;
+template <typename T, int N> struct ZIdx {
+  static __device__ __forceinline__ int p(int i) { return i + (i >> Cfg<N>::LOGEZ); }
+};
+
+// Hermitian-extended load of Y[k] = A[k] + i B[k] (k = j + NT m), A/B spectral rows with Kin
+// valid coefficients; imaginary parts of k = 0 and k = N/2 are dropped (pocketfft c2r).
+template <typename T, int N>
+__device__ __forceinline__ void zload_pair(cplx<T>* a, const cplx<T>* A, const cplx<T>* B, int Kin,
+                                           int j, T s) {
+  constexpr int NT = Cfg<N>::NTZ, E = Cfg<N>::EZ;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = j + NT * m;
+    T yr = 0, yi = 0;
+    if (k == 0 || k == N / 2) {
+      if (k < Kin) {
+        yr = A[k].x;
+        if (B) yi = B[k].x;
+      }
+    } else if (k < N / 2) {
+      if (k < Kin) {
+        cplx<T> av = A[k];
+        cplx<T> bv = B ? B[k] : czero<cplx<T>>();
+        yr = av.x - bv.y;
+        yi = av.y + bv.x;
+      }
+    } else {
+      const int kk = N - k;
+      if (kk < Kin) {
+        cplx<T> av = A[kk];
+        cplx<T> bv = B ? B[kk] : czero<cplx<T>>();
+        yr = av.x + bv.y;
+        yi = bv.x - av.y;
+      }
+    }
+    a[m] = cmk(yr * s, yi * s);
+  }
+}
+
+// After a forward FFT of (a + i b): split Y into A[k], B[k] for k < Kout (zero for k >= Kval).
+// Writes Y to the row buffer first; caller must have synced the buffer.
+template <typename T, int N, class Sync>
+__device__ __forceinline__ void zstore_pair(const cplx<T>* a, cplx<T>* sb, cplx<T>* A, cplx<T>* B,
+                                            int Kout, int Kval, int j, bool ok, Sync sync) {
+  constexpr int NT = Cfg<N>::NTZ, E = Cfg<N>::EZ;
+  if (B == nullptr) {
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int k = j + NT * m;
+      if (ok && k < Kout) A[k] = k < Kval ? a[m] : czero<cplx<T>>();
+    }
+    return;
+  }
+#pragma unroll
+  for (int m = 0; m < E; ++m) sb[ZIdx<T, N>::p(j + NT * m)] = a[m];
+  sync();
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = j + NT * m;
+    if (ok && k < Kout) {
+      cplx<T> ra = czero<cplx<T>>(), rb = czero<cplx<T>>();
+      if (k < Kval) {
+        const cplx<T> y = a[m];
+        const cplx<T> z = sb[ZIdx<T, N>::p((N - k) & (N - 1))];
+        ra = cmk(T(0.5) * (y.x + z.x), T(0.5) * (y.y - z.y));
+        rb = cmk(T(0.5) * (y.y + z.y), T(-0.5) * (y.x - z.x));
+      }
+      A[k] = ra;
+      B[k] = rb;
+    }
+  }
+}
+
+// Generic C2R: pairs of rows (2p, 2p+1) of nrows rows per field; spectral rows of stride ss
+// (Kin valid), real rows of stride N.  Scale s (1/N^3 for the 3D inverse).
+template <typename T, int N>
+__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
+k_z_c2r(const cplx<T>* __restrict__ X, T* __restrict__ x, long long nrows, int ss, int Kin, T s,
+        long long xfs, long long Xfs, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EZ, NT = Cfg<N>::NTZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
+  cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
+  const long long pair = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;
+  const int f = blockIdx.y;
+  const bool ok = 2 * pair < nrows;
+  const long long r0 = ok ? 2 * pair : 0;
+  const cplx<T>* A = X + f * Xfs + r0 * ss;
+  const cplx<T>* B = (r0 + 1 < nrows) ? A + ss : nullptr;
+  cplx<T> a[E];
+  if (ok) zload_pair<T, N>(a, A, B, Kin, j, s);
+  else for (int m = 0; m < E; ++m) a[m] = czero<cplx<T>>();
+  // the row buffer is private to this unit (one warp or part of one): warp-level sync suffices
+  fft_run<T, N, E, true, true>(a, sb, 1, j, tw, ZSync<N>());
+  if (!ok) return;
+  T* xa = x + f * xfs + r0 * N;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int n = j + NT * m;
+    xa[n] = a[m].x;
+    if (B) xa[N + n] = a[m].y;
+  }
+}
+
+// Generic R2C: pairs of real rows -> spectral rows (stride ss), Kout stored (zeros for k >= Kval).
+template <typename T, int N>
+__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
+k_z_r2c(const T* __restrict__ x, cplx<T>* __restrict__ X, long long nrows, int ss, int Kout,
+        int Kval, long long xfs, long long Xfs, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EZ, NT = Cfg<N>::NTZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
+  cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
+  const long long pair = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;
+  const int f = blockIdx.y;
+  const bool ok = 2 * pair < nrows;
+  const long long r0 = ok ? 2 * pair : 0;
+  const bool hasb = r0 + 1 < nrows;
+  const T* xa = x + f * xfs + r0 * N;
+  cplx<T> a[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int n = j + NT * m;
+    a[m] = ok ? cmk(xa[n], hasb ? xa[N + n] : T(0)) : czero<cplx<T>>();
+  }
+  fft_run<T, N, E, false, true>(a, sb, 1, j, tw, ZSync<N>());
+  ZSync<N>()();
+  cplx<T>* A = X + f * Xfs + r0 * ss;
+  zstore_pair<T, N>(a, sb, A, hasb ? A + ss : nullptr, Kout, Kval, j, ok, ZSync<N>());
+}
+
+// Fused z pass of the nonlinear term: for each (x, y) row, C2R of the six y-transformed fields
+// [u, w] (cube kz rows), optional store of physical u, u x w (F:299-301), R2C of the three
+// products (kz < Mzp kept, zero beyond kc).  W: (6, N*N, Mzp) in; P: (3, N*N, Mzp) out.
+template <typename T, int N>
+__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
+k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int Mzp,
+          int kc, T s, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EZ, NT = Cfg<N>::NTZ;
+  constexpr long long NR = (long long)N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
+  cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
+  const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR exactly
+  const long long fs = NR * Mzp;
+  const int Kin = kc + 1;
+  cplx<T> p0[E], p1[E], p2[E];
+  // pair (u_x, u_y)
+  zload_pair<T, N>(p0, W + row * Mzp, W + fs + row * Mzp, Kin, j, s);
+  fft_run<T, N, E, true, true>(p0, sb, 1, j, tw, ZSync<N>());
+  ZSync<N>()();
+  // pair (u_z, w_x)
+  zload_pair<T, N>(p1, W + 2 * fs + row * Mzp, W + 3 * fs + row * Mzp, Kin, j, s);
+  fft_run<T, N, E, true, true>(p1, sb, 1, j, tw, ZSync<N>());
+  ZSync<N>()();
+  // pair (w_y, w_z)
+  zload_pair<T, N>(p2, W + 4 * fs + row * Mzp, W + 5 * fs + row * Mzp, Kin, j, s);
+  fft_run<T, N, E, true, true>(p2, sb, 1, j, tw, ZSync<N>());
+  ZSync<N>()();
+  if (uphys) {
+    const long long NN3 = NR * N;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int n = j + NT * m;
+      uphys[row * N + n] = p0[m].x;
+      uphys[NN3 + row * N + n] = p0[m].y;
+      uphys[2 * NN3 + row * N + n] = p1[m].x;
+    }
+  }
+  // products: (u x w) = (uy wz - uz wy, uz wx - ux wz, ux wy - uy wx)
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const T ux = p0[m].x, uy = p0[m].y, uz = p1[m].x, wx = p1[m].y, wy = p2[m].x, wz = p2[m].y;
+    p0[m] = cmk(wz * uy - wy * uz, wx * uz - wz * ux);
+    p1[m] = cmk(wy * ux - wx * uy, T(0));
+  }
+  fft_run<T, N, E, false, true>(p0, sb, 1, j, tw, ZSync<N>());
+  ZSync<N>()();
+  zstore_pair<T, N>(p0, sb, P + row * Mzp, P + fs + row * Mzp, Mzp, Kin, j, true, ZSync<N>());
+  ZSync<N>()();
+  fft_run<T, N, E, false, true>(p1, sb, 1, j, tw, ZSync<N>());
+  zstore_pair<T, N>(p1, sb, P + 2 * fs + row * Mzp, (cplx<T>*)nullptr, Mzp, Kin, j, true, ZSync<N>());
+}
+
+// ------------------------------------------------------------------------------------------
+// cube <-> reference layout, spectra, forcing, epilogue
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void k_to_cube(const cplx<T>* __restrict__ full, cplx<T>* __restrict__ cube, int N, int kc,
+                          int My, int Mzp, long long total) {
+  const int Nf = N / 2 + 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long per = (long long)My * My * Mzp;
+    const int comp = (int)(e / per);
+    long long r = e - comp * per;
+    const int ix = (int)(r / ((long long)My * Mzp));
+    r -= (long long)ix * My * Mzp;
+    const int iy = (int)(r / Mzp);
+    const int kz = (int)(r - (long long)iy * Mzp);
+    const int kx = cfreq(ix, kc), ky = cfreq(iy, kc);
+    const int k2 = kx * kx + ky * ky + kz * kz;
+    cplx<T> v = czero<cplx<T>>();
+    if (kz <= kc && k2 <= kc * kc + kc) {
+      const int nx = kx < 0 ? kx + N : kx, ny = ky < 0 ? ky + N : ky;
+      v = full[(long long)comp * N * N * Nf + ((long long)nx * N + ny) * Nf + kz];
+    }
+    cube[e] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_from_cube(const cplx<T>* __restrict__ cube, cplx<T>* __restrict__ full, int N, int kc,
+                            int My, int Mzp, long long total) {
+  const int Nf = N / 2 + 1;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long per = (long long)N * N * Nf;
+    const int comp = (int)(e / per);
+    long long r = e - comp * per;
+    const int nx = (int)(r / ((long long)N * Nf));
+    r -= (long long)nx * N * Nf;
+    const int ny = (int)(r / Nf);
+    const int kz = (int)(r - (long long)ny * Nf);
+    const int ix = crow(nx, N, kc), iy = crow(ny, N, kc);
+    cplx<T> v = czero<cplx<T>>();
+    if (ix >= 0 && iy >= 0 && kz <= kc)
+      v = cube[(long long)comp * My * My * Mzp + ((long long)ix * My + iy) * Mzp + kz];
+    full[e] = v;
+  }
+}
+
+// Shell sums of 0.5 |u|^2 normalize over the modes listed for each shell (CSR of cube indices);
+// one CTA per shell, fixed-order FP64 reduction (deterministic).  With `factor` != nullptr the
+// block writes the constant-power factor f0 / (2 E_s) of F:250-254 instead of E_s.
+template <typename T>
+__global__ void k_shell_sum(const cplx<T>* __restrict__ u, long long cs, const int* __restrict__ off,
+                            const int* __restrict__ idx, int Mzp, int shell0,
+                            double norm0, double* __restrict__ out, double f0, int as_factor) {
+  __shared__ double red[256];
+  const int s = shell0 + blockIdx.x;
+  double acc = 0.0;
+  for (int t = off[s] + threadIdx.x; t < off[s + 1]; t += blockDim.x) {
+    const int e = idx[t];
+    const double w = (e % Mzp) ? 2.0 : 1.0;  // Hermitian weight of F:136 (kz < N/2 here)
+    double m = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cplx<T> v = u[c * cs + e];
+      m += double(v.x) * double(v.x) + double(v.y) * double(v.y);
+    }
+    acc += 0.5 * m * w * norm0;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double e = red[0];
+    if (as_factor) {
+      if (fabs(e) < 1e-10) e = INFINITY;  // F:250
+      out[s] = f0 / (2.0 * e);
+    } else {
+      out[s] = e;
+    }
+  }
+}
+
+// End-of-step epilogue (F:596-620) on the cube: symmetrise kz = 0 (the irfft->rfft round trip),
+// div-free projection, NaN and blow-up tests.  One thread per (kx, ky, kz) column element; the
+// kz = 0 pair (k, -k) is handled by the lexicographically smaller member.
+template <typename T>
+__global__ void k_epilogue(cplx<T>* __restrict__ u, long long cs, int kc, int My, int Mzp,
+                           T blowup, unsigned* status) {
+  const long long total = (long long)My * My * Mzp;
+  unsigned flags = 0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e / ((long long)My * Mzp));
+    const long long r = e - (long long)ix * My * Mzp;
+    const int iy = (int)(r / Mzp);
+    const int kz = (int)(r - (long long)iy * Mzp);
+    const int kx = cfreq(ix, kc), ky = cfreq(iy, kc);
+    cplx<T> v[3];
+    if (kz == 0) {
+      // partner -k
+      const int jx = kx == 0 ? 0 : (-kx < 0 ? -kx + 2 * kc + 1 : -kx);
+      const int jy = ky == 0 ? 0 : (-ky < 0 ? -ky + 2 * kc + 1 : -ky);
+      const bool mine = (kx > 0) || (kx == 0 && ky >= 0);
+      if (!mine) continue;
+      const long long ep = ((long long)jx * My + jy) * Mzp;
+      cplx<T> w[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx<T> a = u[c * cs + e], b = u[c * cs + ep];
+        v[c] = cmk(T(0.5) * (a.x + b.x), T(0.5) * (a.y - b.y));
+        w[c] = cconj(v[c]);
+      }
+      // project both members with their own k
+      for (int side = 0; side < 2; ++side) {
+        cplx<T>* q = side ? w : v;
+        const T qx = T(side ? -kx : kx), qy = T(side ? -ky : ky);
+        const int k2 = kx * kx + ky * ky;
+        if (k2 > 0 && k2 <= kc * kc + kc) {
+          cplx<T> kd = cscale(cadd(cscale(q[0], qx), cscale(q[1], qy)), T(1) / T(k2));
+          q[0] = csub(q[0], cscale(kd, qx));
+          q[1] = csub(q[1], cscale(kd, qy));
+        }
+        if (k2 > kc * kc + kc) { q[0] = q[1] = q[2] = czero<cplx<T>>(); }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        u[c * cs + e] = v[c];
+        if (ep != e) u[c * cs + ep] = w[c];
+        if (!(isfinite(v[c].x) && isfinite(v[c].y))) flags |= LD_STATUS_NONFINITE;
+        if (v[c].x > blowup || w[c].x > blowup) flags |= LD_STATUS_BLOWUP;
+      }
+      continue;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = u[c * cs + e];
+    const int k2 = kx * kx + ky * ky + kz * kz;
+    if (kz <= kc && k2 <= kc * kc + kc) {
+      const T qx = T(kx), qy = T(ky), qz = T(kz);
+      cplx<T> kd = cscale(cadd(cadd(cscale(v[0], qx), cscale(v[1], qy)), cscale(v[2], qz)), T(1) / T(k2));
+      v[0] = csub(v[0], cscale(kd, qx));
+      v[1] = csub(v[1], cscale(kd, qy));
+      v[2] = csub(v[2], cscale(kd, qz));
+    } else {
+      v[0] = v[1] = v[2] = czero<cplx<T>>();
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      u[c * cs + e] = v[c];
+      if (!(isfinite(v[c].x) && isfinite(v[c].y))) flags |= LD_STATUS_NONFINITE;
+      if (v[c].x > blowup) flags |= LD_STATUS_BLOWUP;
+    }
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+template <typename T>
+__global__ void k_ifac(T* __restrict__ tab, int n, double nuh) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    tab[i] = T(exp(-nuh * double(i)));
+}
+
+// ------------------------------------------------------------------------------------------
+// droplets
+// ------------------------------------------------------------------------------------------
+// Stencil along one axis: base index (periodic) and weights for offsets (lo .. lo+W-1).
+template <typename T, int METHOD> struct AxisW;
+
+template <typename T> struct AxisW<T, LD_INTERP_TRILINEAR> {
+  static constexpr int W = 2, LO = 0;
+  __device__ __forceinline__ static void get(double p, int N, double L, int& i0, T* w) {
+    const double s = p * (double(N) / L);
+    double fl = floor(s);
+    const double t = s - fl;
+    long long ii = (long long)fl % N;
+    if (ii < 0) ii += N;
+    i0 = int(ii);
+    w[0] = T(1.0 - t);
+    w[1] = T(t);
+  }
+};
+
+template <typename T> struct AxisW<T, LD_INTERP_TRICUBIC> {
+  static constexpr int W = 4, LO = -1;
+  __device__ __forceinline__ static void get(double p, int N, double L, int& i0, T* w) {
+    const double s = p * (double(N) / L);
+    double fl = floor(s);
+    const double t = s - fl;
+    long long ii = (long long)fl % N;
+    if (ii < 0) ii += N;
+    i0 = int(ii);
+    w[0] = T(-t * (t - 1.0) * (t - 2.0) / 6.0);
+    w[1] = T((t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0);
+    w[2] = T(-(t + 1.0) * t * (t - 2.0) / 2.0);
+    w[3] = T((t + 1.0) * t * (t - 1.0) / 6.0);
+  }
+};
+
+// The reference's cosine kernel (P:9-16, P:441, P:456): offsets -1..2 around floor(pos/dx),
+// weight (1 + cos((pos - X_j) pi / (2 dx))) / 4 with X_j on the periodic index.
+template <typename T> struct AxisW<T, LD_INTERP_COSINE> {
+  static constexpr int W = 4, LO = -1;
+  __device__ __forceinline__ static void get(double p, int N, double L, int& i0, T* w) {
+    const double dx = L / double(N);
+    const double pm = p - L * floor(p / L);
+    long long ii = (long long)floor(pm / dx);
+    ii %= N;
+    if (ii < 0) ii += N;
+    i0 = int(ii);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      int jx = (i0 - 1 + a) % N;
+      if (jx < 0) jx += N;
+      const double Xj = double(jx) * dx;
+      w[a] = T((1.0 + cos((pm - Xj) * (3.14159265358979323846 / (2.0 * dx)))) / 4.0);
+    }
+  }
+};
+
+template <typename T, int METHOD>
+__device__ __forceinline__ void gather_point(const T* __restrict__ f, int ncomp, long long fstride, int N,
+                                             double L, double px, double py, double pz, T* out) {
+  using A = AxisW<T, METHOD>;
+  constexpr int W = A::W, LO = A::LO;
+  int ix, iy, iz;
+  T wx[W], wy[W], wz[W];
+  A::get(px, N, L, ix, wx);
+  A::get(py, N, L, iy, wy);
+  A::get(pz, N, L, iz, wz);
+  int jz[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) jz[c] = (iz + LO + c + N) & (N - 1);
+  for (int c = 0; c < ncomp; ++c) out[c] = T(0);
+#pragma unroll
+  for (int a = 0; a < W; ++a) {
+    const int jx = (ix + LO + a + N) & (N - 1);
+#pragma unroll
+    for (int b = 0; b < W; ++b) {
+      const int jy = (iy + LO + b + N) & (N - 1);
+      const long long base = ((long long)jx * N + jy) * N;
+      const T wab = wx[a] * wy[b];
+      for (int c = 0; c < ncomp; ++c) {
+        const T* fc = f + c * fstride + base;
+        T acc = T(0);
+#pragma unroll
+        for (int q = 0; q < W; ++q) acc += wz[q] * __ldg(fc + jz[q]);
+        out[c] += wab * acc;
+      }
+    }
+  }
+}
+
+template <typename T, int METHOD>
+__global__ void k_gather(const T* __restrict__ f, int ncomp, int N, double L, const double* __restrict__ pos,
+                         long long n, T* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T v[8];
+    gather_point<T, METHOD>(f, ncomp, (long long)N * N * N, N, L, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], v);
+    for (int c = 0; c < ncomp; ++c) out[i * ncomp + c] = v[c];
+  }
+}
+
+template <typename T, int METHOD, int STAGE>
+__global__ void k_droplet_stage(const T* __restrict__ u, int N, double L, double* __restrict__ pos,
+                                T* __restrict__ vel, const T* __restrict__ tau, T* __restrict__ a1,
+                                long long n, double h, T g) {
+  const long long fs = (long long)N * N * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+    const T vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
+    const T it = T(1) / tau[i];
+    T up[3];
+    if (STAGE == 1) {
+      gather_point<T, METHOD>(u, 3, fs, N, L, px, py, pz, up);
+      a1[3 * i] = (up[0] - vx) * it;
+      a1[3 * i + 1] = (up[1] - vy) * it;
+      a1[3 * i + 2] = (up[2] - vz) * it - g;
+    } else {
+      const T ax = a1[3 * i], ay = a1[3 * i + 1], az = a1[3 * i + 2];
+      const T hh = T(h);
+      const T sx = vx + hh * ax, sy = vy + hh * ay, sz = vz + hh * az;  // vs = v + h a1
+      const double qx = px + h * double(vx), qy = py + h * double(vy), qz = pz + h * double(vz);
+      gather_point<T, METHOD>(u, 3, fs, N, L, qx, qy, qz, up);
+      const T bx = (up[0] - sx) * it, by = (up[1] - sy) * it, bz = (up[2] - sz) * it - g;
+      pos[3 * i] = px + 0.5 * h * (double(vx) + double(sx));
+      pos[3 * i + 1] = py + 0.5 * h * (double(vy) + double(sy));
+      pos[3 * i + 2] = pz + 0.5 * h * (double(vz) + double(sz));
+      vel[3 * i] = vx + T(0.5) * hh * (ax + bx);
+      vel[3 * i + 1] = vy + T(0.5) * hh * (ay + by);
+      vel[3 * i + 2] = vz + T(0.5) * hh * (az + bz);
+    }
+  }
+}
+
+}  // namespace ld

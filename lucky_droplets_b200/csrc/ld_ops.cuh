@@ -1,0 +1,342 @@
+// Launch sequences for one (precision, N) instance.  Included by the ld_inst_*.cu units, each
+// of which instantiates one OpsTable; compiling the twelve instances separately keeps the build
+// parallel.
+#pragma once
+#include <cmath>
+#include <type_traits>
+
+#include "ld_internal.cuh"
+#include "ld_kernels.cuh"
+
+namespace ld_impl {
+
+using namespace ld;
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+template <class K> int set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) { ld_set_last_error(e); return LD_ERR_CUDA; }
+  }
+  return LD_OK;
+}
+
+inline long long cdiv(long long a, long long b) { return (a + b - 1) / b; }
+
+inline int grid1d(long long n, int threads) {
+  long long b = cdiv(n, threads);
+  if (b > 148LL * 32) b = 148LL * 32;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <typename T, int N> struct Ops {
+  using C = cplx<T>;
+  static constexpr int TB = Cfg<N>::TB;
+  static constexpr size_t COL_SMEM = sizeof(C) * N * TB;
+  static constexpr size_t Z_SMEM = sizeof(C) * Cfg<N>::ZROWS * Cfg<N>::ZBUF;
+
+  template <bool INV, class Ld, class St>
+  static int colpass(ld_plan* p, int kid, Ld ld, St st, int ncols, int nf, int nouter, const C* tw, cudaStream_t s) {
+    ProfScope ps(p, kid, s);
+    auto k = k_colfft<T, N, INV, Ld, St>;
+    if (int rc = set_smem(k, COL_SMEM)) return rc;
+    dim3 grid((unsigned)(cdiv(ncols, TB) * nf), (unsigned)nouter);
+    k<<<grid, Cfg<N>::COL_THREADS, COL_SMEM, s>>>(ld, st, ncols, nf, tw);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  static RowsIO<T> io(const void* p, long long fs, long long os, int rs, int kc, T scale = T(1)) {
+    RowsIO<T> r;
+    r.p = (C*)p; r.fs = fs; r.os = os; r.rs = rs; r.kc = kc; r.scale = scale;
+    return r;
+  }
+
+  static int z_c2r(ld_plan* p, const C* X, T* x, long long nrows, int ss, int Kin, T sc, long long xfs, long long Xfs,
+                   int nf, const C* tw, cudaStream_t s) {
+    ProfScope ps(p, KID_ZC2R, s);
+    auto k = k_z_c2r<T, N>;
+    if (int rc = set_smem(k, Z_SMEM)) return rc;
+    dim3 grid((unsigned)cdiv(nrows / 2, Cfg<N>::ZROWS), (unsigned)nf);
+    k<<<grid, Cfg<N>::ZTHREADS, Z_SMEM, s>>>(X, x, nrows, ss, Kin, sc, xfs, Xfs, tw);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  static int z_r2c(ld_plan* p, const T* x, C* X, long long nrows, int ss, int Kout, int Kval, long long xfs, long long Xfs,
+                   int nf, const C* tw, cudaStream_t s) {
+    ProfScope ps(p, KID_ZR2C, s);
+    auto k = k_z_r2c<T, N>;
+    if (int rc = set_smem(k, Z_SMEM)) return rc;
+    dim3 grid((unsigned)cdiv(nrows / 2, Cfg<N>::ZROWS), (unsigned)nf);
+    k<<<grid, Cfg<N>::ZTHREADS, Z_SMEM, s>>>(x, X, nrows, ss, Kout, Kval, xfs, Xfs, tw);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  // ---- reference-layout transforms --------------------------------------------------------
+  static int rfft_full(ld_plan* p, const T* u, C* fu, int ncomp, cudaStream_t s) {
+    const int Nf = p->Nf;
+    const C* tw = (const C*)p->tw;
+    const long long NN = (long long)N * N;
+    if (int rc = z_r2c(p, u, fu, NN, Nf, Nf, Nf, NN * N, NN * Nf, ncomp, tw, s)) return rc;
+    // y pass in place: columns kz (Nf), rows y, outer x
+    auto yio = io(fu, NN * Nf, (long long)N * Nf, Nf, -1);
+    if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{yio}, StRows<T, N>{yio}, Nf, ncomp, N, tw, s)) return rc;
+    // x pass in place: columns (ky, kz) flat, rows x
+    auto xio = io(fu, NN * Nf, 0, N * Nf, -1);
+    return colpass<false>(p, KID_XPASS, LdRows<T, N>{xio}, StRows<T, N>{xio}, N * Nf, ncomp, 1, tw, s);
+  }
+
+  static int irfft_full(ld_plan* p, const C* fu, T* u, int ncomp, cudaStream_t s) {
+    const int Nf = p->Nf;
+    const C* tw = (const C*)p->tw;
+    const long long NN = (long long)N * N;
+    const long long per = NN * Nf;
+    const int chunk = (int)(((long long)6 * NN * p->Mzp) / per);  // fields that fit in W2
+    C* W = (C*)p->W2;
+    for (int c0 = 0; c0 < ncomp; c0 += chunk) {
+      const int nc = ncomp - c0 < chunk ? ncomp - c0 : chunk;
+      auto xin = io(fu + c0 * per, per, 0, N * Nf, -1);
+      auto xout = io(W, per, 0, N * Nf, -1);
+      if (int rc = colpass<true>(p, KID_XPASS, LdRows<T, N>{xin}, StRows<T, N>{xout}, N * Nf, nc, 1, tw, s)) return rc;
+      auto yio = io(W, per, (long long)N * Nf, Nf, -1);
+      if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yio}, StRows<T, N>{yio}, Nf, nc, N, tw, s)) return rc;
+      const T sc = T(1.0 / (double(N) * N * N));
+      if (int rc = z_c2r(p, W, u + (long long)c0 * NN * N, NN, Nf, Nf, sc, NN * N, per, nc, tw, s)) return rc;
+    }
+    return LD_OK;
+  }
+
+  // ---- cube-layout (dealiased) transforms -----------------------------------------------------
+  static int irfft_cube(ld_plan* p, const C* uk, T* u, int ncomp, cudaStream_t s) {
+    const int kc = p->kc, My = p->My, Mzp = p->Mzp;
+    const C* tw = (const C*)p->tw;
+    const long long NN = (long long)N * N;
+    const long long cs = p->cube_elems();
+    C* W1 = (C*)p->W1;
+    C* W2 = (C*)p->W2;
+    const long long w1s = (long long)N * My * Mzp, w2s = NN * Mzp;
+    for (int c0 = 0; c0 < ncomp; c0 += 6) {
+      const int nc = ncomp - c0 < 6 ? ncomp - c0 : 6;
+      auto xin = io(uk + c0 * cs, cs, 0, My * Mzp, kc);
+      auto xout = io(W1, w1s, 0, My * Mzp, -1);
+      if (int rc = colpass<true>(p, KID_XPASS, LdRows<T, N>{xin}, StRows<T, N>{xout}, My * Mzp, nc, 1, tw, s)) return rc;
+      auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
+      auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
+      if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, nc, N, tw, s)) return rc;
+      const T sc = T(1.0 / (double(N) * N * N));
+      if (int rc = z_c2r(p, W2, u + (long long)c0 * NN * N, NN, Mzp, kc + 1, sc, NN * N, w2s, nc, tw, s)) return rc;
+    }
+    return LD_OK;
+  }
+
+  static int rfft_cube(ld_plan* p, const T* u, C* uk, int ncomp, cudaStream_t s) {
+    const int kc = p->kc, My = p->My, Mzp = p->Mzp;
+    const C* tw = (const C*)p->tw;
+    const long long NN = (long long)N * N;
+    const long long cs = p->cube_elems();
+    C* W1 = (C*)p->W1;
+    C* W2 = (C*)p->W2;
+    const long long w1s = (long long)N * My * Mzp, w2s = NN * Mzp;
+    for (int c0 = 0; c0 < ncomp; c0 += 6) {
+      const int nc = ncomp - c0 < 6 ? ncomp - c0 : 6;
+      if (int rc = z_r2c(p, u + (long long)c0 * NN * N, W2, NN, Mzp, Mzp, kc + 1, NN * N, w2s, nc, tw, s)) return rc;
+      auto yin = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
+      auto yout = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
+      if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, nc, N, tw, s)) return rc;
+      auto xin = io(W1, w1s, 0, My * Mzp, -1);
+      auto xout = io(uk + c0 * cs, cs, 0, My * Mzp, kc);
+      if (int rc = colpass<false>(p, KID_XPASS, LdRows<T, N>{xin}, StCube<T, N>{xout, Mzp}, My * Mzp, nc, 1, tw, s)) return rc;
+    }
+    return LD_OK;
+  }
+
+  // ---- forcing factor for the stage input -----------------------------------------------------
+  static int forcing_factor(ld_plan* p, const C* y, const ld_flow_params* prm, cudaStream_t s) {
+    if (prm->kf_hi < prm->kf_lo || prm->f0 == 0.0) return LD_OK;
+    ProfScope ps(p, KID_FORCING, s);
+    const double norm0 = std::pow(2.0 * M_PI, 3) / std::pow((double)N, 6);
+    k_shell_sum<T><<<prm->kf_hi - prm->kf_lo + 1, 256, 0, s>>>(y, p->cube_elems(), p->shell_off, p->shell_idx,
+                                                               p->Mzp, prm->kf_lo, norm0, p->factor, prm->f0, 1);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  static int ensure_ifac(ld_plan* p, double nuh, cudaStream_t s) {
+    if (p->ifac_key == nuh) return LD_OK;
+    ProfScope ps(p, KID_IFAC, s);
+    k_ifac<T><<<grid1d(p->nifac, 256), 256, 0, s>>>((T*)p->ifac, p->nifac, nuh);
+    LD_LAUNCH_CHECK();
+    p->ifac_key = nuh;
+    return LD_OK;
+  }
+
+  // ---- RHS pipeline: y (stage input) -> update epilogue ------------------------------------------
+  template <int MODE>
+  static int rhs(ld_plan* p, C* s0, C* s1, C* s2, T* uout, const ld_flow_params* prm, double visc,
+                 cudaStream_t s, C* s3 = nullptr) {
+    const int kc = p->kc, My = p->My, Mzp = p->Mzp;
+    const C* tw = (const C*)p->tw;
+    const long long NN = (long long)N * N;
+    const long long cs = p->cube_elems();
+    C* W1 = (C*)p->W1;
+    C* W2 = (C*)p->W2;
+    const long long w1s = (long long)N * My * Mzp, w2s = NN * Mzp;
+    const C* y = s1;  // stage input in every mode
+    if (int rc = forcing_factor(p, y, prm, s)) return rc;
+    // inverse x pass with the curl: 6 fields [u, w]
+    LdCurl<T, N> lc{y, cs, kc, My, Mzp};
+    auto xout = io(W1, w1s, 0, My * Mzp, -1);
+    if (int rc = colpass<true>(p, KID_XINV, lc, StRows<T, N>{xout}, My * Mzp, 6, 1, tw, s)) return rc;
+    // inverse y pass
+    auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
+    auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
+    if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, 6, N, tw, s)) return rc;
+    // fused z pass: u, w -> u x w  (W2 -> W1 as (3, N*N, Mzp))
+    {
+      ProfScope ps(p, KID_ZCROSS, s);
+      auto k = k_z_cross<T, N>;
+      if (int rc = set_smem(k, Z_SMEM)) return rc;
+      const T sc = T(1.0 / (double(N) * N * N));
+      k<<<(unsigned)(NN / Cfg<N>::ZROWS), Cfg<N>::ZTHREADS, Z_SMEM, s>>>(W2, W1, uout, Mzp, kc, sc, tw);
+      LD_LAUNCH_CHECK();
+    }
+    // forward y pass (W1 -> W2 as (3, N, My, Mzp))
+    auto fyin = io(W1, w2s, (long long)N * Mzp, Mzp, -1);
+    auto fyout = io(W2, w1s, (long long)My * Mzp, Mzp, kc);
+    if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{fyin}, StRows<T, N>{fyout}, Mzp, 3, N, tw, s)) return rc;
+    // forward x pass + k-space update
+    UpdArgs<T> A;
+    A.nl = W2; A.nls = w1s;
+    A.s0 = s0; A.s1 = s1; A.s2 = s2; A.s3 = s3; A.cs = cs;
+    A.factor = p->factor; A.kf_lo = prm->kf_lo; A.kf_hi = (prm->f0 == 0.0) ? -1 : prm->kf_hi;
+    A.ifac = (const T*)p->ifac;
+    A.h = T(prm->dt); A.nu = T(prm->nu); A.visc = T(visc);
+    A.kc = kc; A.My = My; A.Mzp = Mzp; A.status = p->status;
+    ProfScope ps(p, KID_XFWD_UPD, s);
+    auto k = k_xfwd_update<T, N, MODE>;
+    if (int rc = set_smem(k, COL_SMEM)) return rc;
+    k<<<(unsigned)cdiv((long long)My * Mzp, TB), Cfg<N>::COL_THREADS, COL_SMEM, s>>>(A, My * Mzp, tw);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  static int gather(ld_plan* p, const T* f, int ncomp, const double* pos, long long n, int method, T* out,
+                    cudaStream_t s) {
+    ProfScope ps(p, KID_GATHER, s);
+    const int th = 256;
+    const int g = grid1d(n, th);
+    const double L = 2.0 * M_PI;
+    if (method == LD_INTERP_TRILINEAR) k_gather<T, LD_INTERP_TRILINEAR><<<g, th, 0, s>>>(f, ncomp, N, L, pos, n, out);
+    else if (method == LD_INTERP_TRICUBIC) k_gather<T, LD_INTERP_TRICUBIC><<<g, th, 0, s>>>(f, ncomp, N, L, pos, n, out);
+    else k_gather<T, LD_INTERP_COSINE><<<g, th, 0, s>>>(f, ncomp, N, L, pos, n, out);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  template <int M>
+  static int dstage_m(ld_plan* p, int stage, const T* u, double* pos, T* vel, const T* tau, T* a1, long long n, double h,
+                      double g, cudaStream_t s) {
+    ProfScope ps(p, stage == 1 ? KID_DROPLET1 : KID_DROPLET2, s);
+    const int th = 256;
+    const int gr = grid1d(n, th);
+    const double L = 2.0 * M_PI;
+    if (stage == 1) k_droplet_stage<T, M, 1><<<gr, th, 0, s>>>(u, N, L, pos, vel, tau, a1, n, h, T(g));
+    else k_droplet_stage<T, M, 2><<<gr, th, 0, s>>>(u, N, L, pos, vel, tau, a1, n, h, T(g));
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
+  static int dstage(ld_plan* p, int stage, int method, const T* u, double* pos, T* vel, const T* tau, T* a1, long long n,
+                    double h, double g, cudaStream_t s) {
+    if (method == LD_INTERP_TRILINEAR) return dstage_m<LD_INTERP_TRILINEAR>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
+    if (method == LD_INTERP_TRICUBIC) return dstage_m<LD_INTERP_TRICUBIC>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
+    return dstage_m<LD_INTERP_COSINE>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
+  }
+};
+
+
+// ---- type-erased wrappers ------------------------------------------------------------------
+template <typename T, int N> struct Table {
+  using O = Ops<T, N>;
+  using C = ld::cplx<T>;
+  static int rfft_full(ld_plan* p, const void* u, void* fu, int nc, cudaStream_t s) {
+    return O::rfft_full(p, (const T*)u, (C*)fu, nc, s);
+  }
+  static int irfft_full(ld_plan* p, const void* fu, void* u, int nc, cudaStream_t s) {
+    return O::irfft_full(p, (const C*)fu, (T*)u, nc, s);
+  }
+  static int irfft_cube(ld_plan* p, const void* uk, void* u, int nc, cudaStream_t s) {
+    return O::irfft_cube(p, (const C*)uk, (T*)u, nc, s);
+  }
+  static int rfft_cube(ld_plan* p, const void* u, void* uk, int nc, cudaStream_t s) {
+    return O::rfft_cube(p, (const T*)u, (C*)uk, nc, s);
+  }
+  static int to_cube(ld_plan* p, const void* full, void* cube, int nc, cudaStream_t s) {
+    ProfScope ps(p, KID_CONVERT, s);
+    const long long total = p->cube_elems() * nc;
+    ld::k_to_cube<T><<<grid1d(total, 256), 256, 0, s>>>((const C*)full, (C*)cube, p->N, p->kc, p->My, p->Mzp, total);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+  static int from_cube(ld_plan* p, const void* cube, void* full, int nc, cudaStream_t s) {
+    ProfScope ps(p, KID_CONVERT, s);
+    const long long total = (long long)p->N * p->N * p->Nf * nc;
+    ld::k_from_cube<T><<<grid1d(total, 256), 256, 0, s>>>((const C*)cube, (C*)full, p->N, p->kc, p->My, p->Mzp, total);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+  static int shell_spectrum(ld_plan* p, const void* uk, double* ek, cudaStream_t s) {
+    ProfScope ps(p, KID_SHELL, s);
+    const double norm0 = std::pow(2.0 * M_PI, 3) / std::pow((double)N, 6);
+    ld::k_shell_sum<T><<<p->Nf, 256, 0, s>>>((const C*)uk, p->cube_elems(), p->shell_off, p->shell_idx, p->Mzp, 0,
+                                             norm0, ek, 0.0, 0);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+  static int rhs(ld_plan* p, int mode, void* s0, void* s1, void* s2, void* s3, void* uout,
+                 const ld_flow_params* prm, double visc, cudaStream_t s) {
+    C *a = (C*)s0, *b = (C*)s1, *c = (C*)s2, *d = (C*)s3;
+    if (mode == ld::UPD_RK2_1 || mode == ld::UPD_RK2_2)
+      if (int rc = O::ensure_ifac(p, prm->nu * prm->dt, s)) return rc;
+    switch (mode) {
+      case ld::UPD_RHS: return O::template rhs<ld::UPD_RHS>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK2_1: return O::template rhs<ld::UPD_RK2_1>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK2_2: return O::template rhs<ld::UPD_RK2_2>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK4_1: return O::template rhs<ld::UPD_RK4_1>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK4_2: return O::template rhs<ld::UPD_RK4_2>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK4_3: return O::template rhs<ld::UPD_RK4_3>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      case ld::UPD_RK4_4: return O::template rhs<ld::UPD_RK4_4>(p, a, b, c, (T*)uout, prm, visc, s, d);
+      default: return ld_fail(LD_ERR_ARG, "bad update mode %d", mode);
+    }
+  }
+  static int epilogue(ld_plan* p, void* uk, cudaStream_t s) {
+    ProfScope ps(p, KID_EPILOGUE, s);
+    const long long total = p->cube_elems();
+    const double blow = 100.0 * (double)N * N * N;
+    ld::k_epilogue<T><<<grid1d(total, 256), 256, 0, s>>>((C*)uk, total, p->kc, p->My, p->Mzp, T(blow), p->status);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+  static int gather(ld_plan* p, const void* f, int nc, const double* pos, long long n, int method, void* out,
+                    cudaStream_t s) {
+    return O::gather(p, (const T*)f, nc, pos, n, method, (T*)out, s);
+  }
+  static int dstage(ld_plan* p, int stage, int method, const void* u, double* pos, void* vel, const void* tau,
+                    void* a1, long long n, double h, double g, cudaStream_t s) {
+    return O::dstage(p, stage, method, (const T*)u, pos, (T*)vel, (const T*)tau, (T*)a1, n, h, g, s);
+  }
+  static const OpsTable* get() {
+    static const OpsTable t = {rfft_full, irfft_full, irfft_cube, rfft_cube, to_cube, from_cube,
+                               shell_spectrum, rhs, epilogue, gather, dstage};
+    return &t;
+  }
+};
+
+}  // namespace ld_impl
+
+#define LD_DEFINE_TABLE(P, TT, N) \
+  const OpsTable* ops_table_##P##_##N() { return ld_impl::Table<TT, N>::get(); }

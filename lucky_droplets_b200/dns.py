@@ -1,0 +1,192 @@
+"""The time loop of forced-dns-sm.py (F:556-627) on one GPU, with inertial droplets.
+
+``ForcedDNS`` keeps the reference's driver parameters (N, nu, dt, f0, shell_no) and advances
+the dealiased spectral velocity with either
+  * ``integrator="rk4"``   - the reference's classical RK4 with explicit viscosity (F:335-362),
+  * ``integrator="rk2if"`` - Heun with the viscous integrating factor exp(-nu k^2 h);
+and after every step applies the reference's end-of-step epilogue (F:596-620: reality round
+trip, div-free projection, blow-up test).  ``Droplets`` advances one-way-coupled droplets
+(x' = v, v' = (u(x) - v)/tau - g z) by Heun on the two RK2 stages.
+
+All device work goes through liblucky_droplets.so; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+from .spectral import Plan, flow_params, TWO_PI
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class BlowUpError(FloatingPointError):
+    """The state met the abort test of forced-dns-sm.py:618-620 or became non-finite."""
+
+
+class ForcedDNS:
+    """Forced, triply periodic pseudospectral DNS in [0, 2 pi)^3 on one GPU."""
+
+    def __init__(self, N, nu, dt, f0, shell_no=(1,), integrator="rk2if", precision="f32", device=None,
+                 epilogue=True):
+        if integrator not in ("rk2if", "rk4"):
+            raise ValueError("integrator must be 'rk2if' or 'rk4'")
+        self.plan = Plan(N, precision, device)
+        self.N, self.nu, self.dt, self.f0 = N, float(nu), float(dt), float(f0)
+        self.shell_no = tuple(shell_no)
+        self.integrator = integrator
+        self.epilogue = epilogue
+        self.prm = flow_params(dt, nu, f0, shell_no)
+        p = self.plan
+        self.uk = p.empty_cube(3)
+        self.aux = p.empty_cube(3)   # ustar (rk2if) or the stage input y (rk4)
+        self.acc = p.empty_cube(3)
+        self.u_phys = None
+        self.droplets = None
+        self.t = 0.0
+        self.nstep = 0
+
+    # ---- constructors with the reference's and the configurations' parameters --------------------
+    @classmethod
+    def reference(cls, N, precision="f64", nshells=1, nu0=0.8, m=1.5, **kw):
+        """Parameters of forced-dns-sm.py as functions of N: dt = 0.256/N (F:29),
+        nu = nu0 (3m/N)^(4/3) (F:83), f0 = nu0^3 (2pi)^3 / nshells (F:97), RK4 (F:21)."""
+        dt = 0.256 / N
+        nu = nu0 * (3 * m / N) ** (2 * (1 - 1 / 3))
+        f0 = nu0 ** 3 * TWO_PI ** 3 / nshells
+        kw.setdefault("integrator", "rk4")
+        return cls(N, nu, dt, f0, shell_no=tuple(range(1, nshells + 1)), precision=precision, **kw)
+
+    @classmethod
+    def config(cls, N, nu, dt, eps=0.1, kf=2, precision="f32", **kw):
+        """Configuration semantics: constant power eps on shells 1..kf, RK2 + integrating factor."""
+        f0 = eps * TWO_PI ** 3 / kf
+        return cls(N, nu, dt, f0, shell_no=tuple(range(1, kf + 1)), precision=precision, **kw)
+
+    # ---- state -----------------------------------------------------------------------------------
+    def set_velocity(self, u):
+        """uk = dealias * rfft(u) from a physical (3, N, N, N) velocity (F:567-569)."""
+        torch = _torch()
+        p = self.plan
+        ut = torch.as_tensor(u).to(device=p.device, dtype=p.rdtype).contiguous()
+        p.rfft_cube(ut, self.uk)
+        self.t = 0.0
+        return self
+
+    def set_uk_full(self, uk_full):
+        """Load a reference-layout spectrum (3, N, N, N/2+1); modes outside the mask are dropped."""
+        torch = _torch()
+        p = self.plan
+        ft = torch.as_tensor(uk_full).to(device=p.device, dtype=p.cdtype).contiguous()
+        p.to_cube(ft, self.uk)
+        return self
+
+    def uk_full(self):
+        """The state in the reference's layout (3, N, N, N/2+1), complex128 numpy."""
+        return self.plan.from_cube(self.uk).cpu().numpy().astype(np.complex128)
+
+    def velocity(self, out=None):
+        """Physical velocity (3, N, N, N) on the device."""
+        return self.plan.irfft_cube(self.uk, out)
+
+    def energy_spectrum(self):
+        """Shell spectrum ek_arr of F:423, F:431 (FP64 numpy)."""
+        return self.plan.e3d_to_e1d(self.uk).cpu().numpy()
+
+    def attach(self, droplets):
+        """Advance ``droplets`` with the flow; allocates the physical-velocity buffer."""
+        self.droplets = droplets
+        if self.u_phys is None:
+            self.u_phys = self.plan.empty_phys(3)
+        return self
+
+    # ---- stepping ---------------------------------------------------------------------------------
+    def step(self, nsteps=1, stream=None):
+        L = _lib.lib()
+        h = self.plan.handle
+        st = stream_ptr(stream)
+        prm = ctypes.byref(self.prm)
+        d = self.droplets
+        up = ptr(self.u_phys) if d is not None else None
+        for _ in range(nsteps):
+            if self.integrator == "rk2if":
+                check(L.ld_rk2if_stage(h, 1, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
+                if d is not None:
+                    d.stage(1, self.u_phys, self.dt, stream)
+                check(L.ld_rk2if_stage(h, 2, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
+                if d is not None:
+                    d.stage(2, self.u_phys, self.dt, stream)
+            else:
+                for s in (1, 2, 3, 4):
+                    check(L.ld_rk4_stage(h, s, ptr(self.uk), ptr(self.aux), ptr(self.acc), None, prm, st))
+            if self.epilogue:
+                check(L.ld_step_epilogue(h, ptr(self.uk), st))
+            self.t += self.dt
+            self.nstep += 1
+
+    def step_host(self, uk_host, pos_host=None, vel_host=None, nsteps=1, stream=None):
+        """Drop-in for one call of the reference's time-loop body with host state (F:582-610):
+        copies the cube-layout spectrum (and droplet positions/velocities) from host memory,
+        advances ``nsteps`` steps and copies the new state back into the same host arrays.
+        Host tensors should be pinned for asynchronous copies.  Returns the host tensors."""
+        torch = _torch()
+        s = torch.cuda.current_stream() if stream is None else stream
+        with torch.cuda.stream(s):
+            self.uk.copy_(uk_host, non_blocking=True)
+            d = self.droplets
+            if d is not None and pos_host is not None:
+                d.pos.copy_(pos_host, non_blocking=True)
+                d.vel.copy_(vel_host, non_blocking=True)
+            self.step(nsteps, stream=s)
+            uk_host.copy_(self.uk, non_blocking=True)
+            if d is not None and pos_host is not None:
+                pos_host.copy_(d.pos, non_blocking=True)
+                vel_host.copy_(d.vel, non_blocking=True)
+        s.synchronize()
+        return uk_host, pos_host, vel_host
+
+    def check(self, stream=None):
+        """Host check of the device status word (the blow-up abort of F:618-620)."""
+        flags = self.plan.status(clear=True, stream=stream)
+        if flags & (_lib.STATUS_BLOWUP | _lib.STATUS_NONFINITE):
+            raise BlowUpError(f"threshold exceeded or non-finite state at t={self.t:.6g} (flags={flags})")
+        return flags
+
+
+class Droplets:
+    """One-way-coupled inertial droplets: pos (n,3) FP64, vel (n,3), tau (n) on the device."""
+
+    def __init__(self, plan, pos, vel, tau, method="tricubic", g=0.0):
+        torch = _torch()
+        self.plan = plan
+        dev = plan.device
+        self.pos = torch.as_tensor(pos).to(device=dev, dtype=torch.float64).contiguous()
+        self.vel = torch.as_tensor(vel).to(device=dev, dtype=plan.rdtype).contiguous()
+        self.tau = torch.as_tensor(tau).to(device=dev, dtype=plan.rdtype).contiguous()
+        self.a1 = torch.zeros_like(self.vel)
+        self.n = int(self.pos.shape[0])
+        if self.pos.shape != (self.n, 3) or self.vel.shape != (self.n, 3) or self.tau.shape != (self.n,):
+            raise ValueError("pos (n,3), vel (n,3), tau (n,) expected")
+        self.method = method
+        self.m = _lib.LD_INTERP[method]
+        self.g = float(g)
+
+    def gather(self, field, pos=None, out=None, stream=None):
+        """Interpolate the (C, N, N, N) field at pos (default: the droplet positions)."""
+        torch = _torch()
+        pos = self.pos if pos is None else pos
+        C = int(field.shape[0])
+        if out is None:
+            out = torch.empty((pos.shape[0], C), dtype=self.plan.rdtype, device=self.plan.device)
+        check(_lib.lib().ld_gather(self.plan.handle, ptr(field), C, ptr(pos), int(pos.shape[0]), self.m,
+                                   ptr(out), stream_ptr(stream)))
+        return out
+
+    def stage(self, s, u_phys, h, stream=None):
+        check(_lib.lib().ld_droplet_stage(self.plan.handle, int(s), ptr(u_phys), ptr(self.pos), ptr(self.vel),
+                                          ptr(self.tau), ptr(self.a1), self.n, self.m, float(h), self.g,
+                                          stream_ptr(stream)))

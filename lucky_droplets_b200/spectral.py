@@ -1,0 +1,194 @@
+"""Grid, transforms and spectral operators on one GPU (forced-dns-sm.py:49-233).
+
+``Plan`` wraps one ``ld_plan`` of the C ABI.  Its buffers are torch tensors on the plan's
+device; the methods keep the reference's names and argument meaning where one exists:
+
+    rfft_mpi(u, fu)  -> fu        forced-dns-sm.py:201-206  (one GPU: no slab all-to-all)
+    irfft_mpi(fu, u) -> u         forced-dns-sm.py:208-213
+    e3d_to_e1d(uk)   -> ek_arr    forced-dns-sm.py:232-233, 243-245  (shell spectrum, FP64)
+
+plus the dealiased "cube" layout every transform of the DNS step uses internally.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+
+TWO_PI = 2.0 * np.pi
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Plan:
+    """One N^3 grid in FP32 ("f32") or FP64 ("f64") on a CUDA device."""
+
+    def __init__(self, N, precision="f32", device=None):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise RuntimeError("lucky_droplets_b200 needs a CUDA device (no CPU fallback)")
+        dev = torch.device(device if device is not None else "cuda")
+        if dev.type != "cuda":
+            raise ValueError("a Plan lives on a CUDA device")
+        self.device = torch.device("cuda", dev.index if dev.index is not None else torch.cuda.current_device())
+        self.precision = precision
+        prec = {"f32": _lib.LD_F32, "f64": _lib.LD_F64}[precision]
+        self.rdtype = torch.float32 if precision == "f32" else torch.float64
+        self.cdtype = torch.complex64 if precision == "f32" else torch.complex128
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(L.ld_plan_create(ctypes.byref(h), int(N), prec))
+        self._h = h
+        dims = (ctypes.c_int32 * 8)()
+        wb = ctypes.c_size_t()
+        check(L.ld_plan_dims(h, dims, ctypes.byref(wb)))
+        self.N, self.kc, self.Mx, self.My, self.Mz, self.Mzp, self.Nf = list(dims)[:7]
+        self.work_bytes = wb.value
+        self.L = TWO_PI
+        self.dx = TWO_PI / self.N
+
+    # ---- lifetime -----------------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ld_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- buffers ---------------------------------------------------------------------------------
+    def empty_cube(self, ncomp=3):
+        return _torch().zeros((ncomp, self.Mx, self.My, self.Mzp), dtype=self.cdtype, device=self.device)
+
+    def empty_phys(self, ncomp=3):
+        return _torch().empty((ncomp, self.N, self.N, self.N), dtype=self.rdtype, device=self.device)
+
+    def empty_full(self, ncomp=3):
+        return _torch().empty((ncomp, self.N, self.N, self.Nf), dtype=self.cdtype, device=self.device)
+
+    def _chk(self, t, dtype, tail):
+        if t.device != self.device or t.dtype != dtype or not t.is_contiguous():
+            raise ValueError(f"expected a contiguous {dtype} tensor on {self.device}")
+        if tuple(t.shape[-len(tail):]) != tuple(tail):
+            raise ValueError(f"expected trailing shape {tail}, got {tuple(t.shape)}")
+        return int(np.prod(t.shape[:-len(tail)])) if t.dim() > len(tail) else 1
+
+    # ---- transforms --------------------------------------------------------------------------------
+    def rfft_mpi(self, u, fu=None, stream=None):
+        """Forward R2C of (..., N, N, N) real fields into the reference layout (..., N, N, N/2+1)."""
+        N = self.N
+        nc = self._chk(u, self.rdtype, (N, N, N))
+        if fu is None:
+            fu = _torch().empty(tuple(u.shape[:-3]) + (N, N, self.Nf), dtype=self.cdtype, device=self.device)
+        self._chk(fu, self.cdtype, (N, N, self.Nf))
+        check(_lib.lib().ld_rfft_mpi(self._h, ptr(u), ptr(fu), nc, stream_ptr(stream)))
+        return fu
+
+    def irfft_mpi(self, fu, u=None, stream=None):
+        """Inverse C2R of reference-layout spectra (1/N^3 normalisation, scipy convention)."""
+        N = self.N
+        nc = self._chk(fu, self.cdtype, (N, N, self.Nf))
+        if u is None:
+            u = _torch().empty(tuple(fu.shape[:-3]) + (N, N, N), dtype=self.rdtype, device=self.device)
+        self._chk(u, self.rdtype, (N, N, N))
+        check(_lib.lib().ld_irfft_mpi(self._h, ptr(fu), ptr(u), nc, stream_ptr(stream)))
+        return u
+
+    def rfft_cube(self, u, uk=None, stream=None):
+        """Forward transform keeping only the dealiased cube (modes outside it are dropped)."""
+        N = self.N
+        nc = self._chk(u, self.rdtype, (N, N, N))
+        if uk is None:
+            uk = _torch().empty(tuple(u.shape[:-3]) + (self.Mx, self.My, self.Mzp), dtype=self.cdtype,
+                                device=self.device)
+        self._chk(uk, self.cdtype, (self.Mx, self.My, self.Mzp))
+        check(_lib.lib().ld_rfft_cube(self._h, ptr(u), ptr(uk), nc, stream_ptr(stream)))
+        return uk
+
+    def irfft_cube(self, uk, u=None, stream=None):
+        """Inverse transform of cube-layout spectra (zero outside the cube)."""
+        N = self.N
+        nc = self._chk(uk, self.cdtype, (self.Mx, self.My, self.Mzp))
+        if u is None:
+            u = _torch().empty(tuple(uk.shape[:-3]) + (N, N, N), dtype=self.rdtype, device=self.device)
+        self._chk(u, self.rdtype, (N, N, N))
+        check(_lib.lib().ld_irfft_cube(self._h, ptr(uk), ptr(u), nc, stream_ptr(stream)))
+        return u
+
+    def to_cube(self, full, cube=None, stream=None):
+        """dealias * full, restricted to the cube (the dealias of F:567-569)."""
+        nc = self._chk(full, self.cdtype, (self.N, self.N, self.Nf))
+        if cube is None:
+            cube = _torch().empty(tuple(full.shape[:-3]) + (self.Mx, self.My, self.Mzp), dtype=self.cdtype,
+                                  device=self.device)
+        check(_lib.lib().ld_spec_to_cube(self._h, ptr(full), ptr(cube), nc, stream_ptr(stream)))
+        return cube
+
+    def from_cube(self, cube, full=None, stream=None):
+        """Cube layout -> reference layout (zeros outside the cube)."""
+        nc = self._chk(cube, self.cdtype, (self.Mx, self.My, self.Mzp))
+        if full is None:
+            full = _torch().empty(tuple(cube.shape[:-3]) + (self.N, self.N, self.Nf), dtype=self.cdtype,
+                                  device=self.device)
+        check(_lib.lib().ld_spec_from_cube(self._h, ptr(cube), ptr(full), nc, stream_ptr(stream)))
+        return full
+
+    # ---- spectra and RHS ---------------------------------------------------------------------------
+    def e3d_to_e1d(self, uk, out=None, stream=None):
+        """Shell energy spectrum of a cube-layout 3-vector (FP64, length N/2+1)."""
+        self._chk(uk, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        if out is None:
+            out = _torch().zeros(self.Nf, dtype=_torch().float64, device=self.device)
+        check(_lib.lib().ld_shell_spectrum(self._h, ptr(uk), ptr(out), stream_ptr(stream)))
+        return out
+
+    def velocity_rhs(self, uk, nu, f0=0.0, shell_no=(1,), visc=1.0, ku=None, u_out=None, stream=None):
+        """ku = P[(u x w)^ + f] dealias - visc nu k^2 uk  (full_RHS velocity part, F:287-316)."""
+        self._chk(uk, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        if ku is None:
+            ku = self.empty_cube(3)
+        prm = flow_params(0.0, nu, f0, shell_no)
+        check(_lib.lib().ld_velocity_rhs(self._h, ptr(uk), ptr(ku), ptr(u_out), ctypes.byref(prm), float(visc),
+                                         stream_ptr(stream)))
+        return ku
+
+    def profile(self, enable=True):
+        """Start/stop bracketing every kernel launch of this plan with CUDA events."""
+        check(_lib.lib().ld_profile(self._h, int(bool(enable))))
+
+    def profile_read(self, reset=True):
+        """{kernel name: (launches, total device ms)} since the last reset (synchronises)."""
+        cap = 64
+        kid = (ctypes.c_int32 * cap)()
+        cnt = (ctypes.c_int64 * cap)()
+        ms = (ctypes.c_double * cap)()
+        n = ctypes.c_int32()
+        check(_lib.lib().ld_profile_read(self._h, kid, cnt, ms, cap, ctypes.byref(n), int(bool(reset))))
+        L = _lib.lib()
+        return {(L.ld_kernel_name(kid[i]) or b"k%d" % kid[i]).decode(): (int(cnt[i]), float(ms[i]))
+                for i in range(min(n.value, cap))}
+
+    def status(self, clear=True, stream=None):
+        v = ctypes.c_uint32()
+        check(_lib.lib().ld_status(self._h, ctypes.byref(v), int(bool(clear)), stream_ptr(stream)))
+        return v.value
+
+
+def flow_params(dt, nu, f0, shell_no):
+    shells = list(shell_no) if shell_no is not None else []
+    lo, hi = (min(shells), max(shells)) if shells else (1, 0)
+    if shells and shells != list(range(lo, hi + 1)):
+        raise ValueError("forced shells must be consecutive (shell_no = 1..nshells, F:89-90)")
+    return _lib.FlowParams(float(dt), float(nu), float(f0) if shells else 0.0, int(lo), int(hi))

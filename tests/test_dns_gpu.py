@@ -1,0 +1,143 @@
+"""GPU DNS step against the reference (golden vectors from the reference's own run) and the
+FP64 oracles: full_RHS velocity part, RK4 time loop, RK2 + integrating factor, shell spectrum."""
+import numpy as np
+import pytest
+
+from oracle import reference_np as R
+from oracle import config_np as C
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f32": 2e-5, "f64": 1e-12}
+
+
+def rel(a, b):
+    return np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-300)
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+@pytest.mark.parametrize("name", ["N16", "N32"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_velocity_rhs_matches_reference(torch, golden, name, prec):
+    """ku of full_RHS (F:287-316) from the reference's own run, on its initial state."""
+    from lucky_droplets_b200.spectral import Plan
+    g = golden(name)
+    N = int(g["N"])
+    prm = R.ReferenceParams(N)
+    p = Plan(N, prec)
+    uk = p.to_cube(torch.as_tensor(g["uk0"]).to("cuda", p.cdtype).contiguous())
+    ku = p.velocity_rhs(uk, prm.nu, prm.f0, prm.shell_no, visc=1.0)
+    full = p.from_cube(ku).cpu().numpy()
+    grid = R.Grid(N)
+    ref = g["rhs_ku"] * grid.dealias  # the reference keeps roundoff outside the mask
+    assert rel(full, ref) < TOL[prec]
+
+
+@pytest.mark.parametrize("N", [64, 128, 256])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_velocity_rhs_matches_oracle(torch, N, prec):
+    """The same RHS at larger N against the FP64 restatement, on a seeded initial field."""
+    from lucky_droplets_b200.spectral import Plan
+    prm = C.ConfigParams(N=N, nu=2.5e-3, dt=1e-3)
+    grid = C.ConfigGrid(N)
+    uk0, _ = C.init_flow(grid, prm, seed=N)
+    p = Plan(N, prec)
+    uk = p.to_cube(torch.as_tensor(uk0).to("cuda", p.cdtype).contiguous())
+    u_out = p.empty_phys(3)
+    ku = p.velocity_rhs(uk, prm.nu, prm.f0, prm.shell_no, visc=1.0, u_out=u_out)
+    fk, _ = R.forcing(grid, uk0, prm.f0, prm.shell_no)
+    ref, u_ref, _ = R.velocity_rhs(grid, uk0, prm.nu, fk, 1.0)
+    assert rel(p.from_cube(ku).cpu().numpy(), ref * grid.dealias) < TOL[prec]
+    assert rel(u_out.cpu().numpy(), u_ref) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_shell_spectrum_matches_reference(torch, golden, prec):
+    from lucky_droplets_b200.spectral import Plan
+    g = golden("N16")
+    p = Plan(16, prec)
+    uk = p.to_cube(torch.as_tensor(g["uk0"]).to("cuda", p.cdtype).contiguous())
+    ek = p.e3d_to_e1d(uk).cpu().numpy()
+    grid = R.Grid(16)
+    ref = grid.shell_sum(grid.energy3d(g["uk0"]))
+    assert np.allclose(ek, ref, rtol=1e-6 if prec == "f32" else 1e-13, atol=1e-12 * ref.max())
+
+
+@pytest.mark.parametrize("name", ["N16", "N32"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_rk4_time_loop_matches_reference(torch, golden, name, prec):
+    """nsteps of the reference's own RK4 loop (F:571-623) from the same initial state."""
+    from lucky_droplets_b200.dns import ForcedDNS
+    g = golden(name)
+    N = int(g["N"])
+    dns = ForcedDNS.reference(N, precision=prec)
+    dns.set_uk_full(g["uk0"])
+    dns.step(int(g["nsteps"]))
+    assert dns.check() == 0
+    grid = R.Grid(N)
+    assert rel(dns.uk_full(), g["run_uk"] * grid.dealias) < TOL[prec]
+
+
+@pytest.mark.parametrize("N", [32, 64])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_rk2if_matches_oracle(torch, N, prec):
+    """RK2 + integrating factor against the FP64 NumPy restatement, 5 steps."""
+    from lucky_droplets_b200.dns import ForcedDNS
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3)
+    grid = C.ConfigGrid(N)
+    uk0, _ = C.init_flow(grid, prm, seed=5)
+    dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision=prec)
+    dns.set_uk_full(uk0)
+    uk = uk0.copy()
+    for _ in range(5):
+        uk, _, _ = C.rk2if_step(grid, prm, uk)
+        uk = grid.project(np.stack([grid.rfft(grid.irfft(uk[c])) for c in range(3)]))
+    dns.step(5)
+    assert rel(dns.uk_full(), uk * grid.dealias) < TOL[prec] * 5
+
+
+@pytest.mark.parametrize("method", ["trilinear", "tricubic", "cosine"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_gather_matches_oracle(torch, method, prec):
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200.dns import Droplets
+    N = 32
+    rng = np.random.default_rng(9)
+    field = rng.standard_normal((3, N, N, N))
+    pos = rng.uniform(-1.0, 2 * np.pi + 1.0, (4000, 3))  # includes positions outside [0, 2pi)
+    p = Plan(N, prec)
+    d = Droplets(p, pos, np.zeros((4000, 3)), np.ones(4000), method=method)
+    out = d.gather(torch.as_tensor(field).to("cuda", p.rdtype).contiguous()).cpu().numpy()
+    ref = C.gather(field, pos, method)
+    assert np.abs(out - ref).max() < (2e-5 if prec == "f32" else 1e-12)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_coupled_step_matches_oracle(torch, prec):
+    """Flow RK2+IF + droplet Heun (tricubic, settling) against the FP64 oracle, 3 steps."""
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3, g=0.1)
+    grid = C.ConfigGrid(N)
+    uk0, u0 = C.init_flow(grid, prm, seed=2)
+    pos, tau, _ = C.init_droplets(prm, 2, "uniform_tau", nd=2000)
+    vel = C.gather(u0, pos, "tricubic")
+    dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision=prec)
+    dns.set_uk_full(uk0)
+    d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g)
+    dns.attach(d)
+    uk, p_, v_ = uk0.copy(), pos.copy(), vel.copy()
+    for _ in range(3):
+        uk, p_, v_ = C.step(grid, prm, uk, p_, v_, tau, "tricubic")
+        uk = grid.project(np.stack([grid.rfft(grid.irfft(uk[c])) for c in range(3)]))
+    dns.step(3)
+    assert rel(dns.uk_full(), uk * grid.dealias) < TOL[prec] * 5
+    tol_x = 1e-9 if prec == "f32" else 1e-13
+    assert np.abs(d.pos.cpu().numpy() - p_).max() < tol_x * 1e3
+    assert rel(d.vel.cpu().numpy(), v_) < TOL[prec] * 5
