@@ -61,6 +61,7 @@ extern "C" {
 #define LD_INTERP_COSINE 2     /* (1 + cos(pi r / 2dx)) / 4 on offsets -1..2, P:6-20, P:435-511 */
 
 typedef struct ld_plan ld_plan;
+typedef struct ld_collider ld_collider;
 
 /* Flow parameters of one time step. */
 typedef struct ld_flow_params {
@@ -145,6 +146,28 @@ LD_API int ld_gather(ld_plan* plan, const void* field, int ncomp, const double* 
 LD_API int ld_droplet_stage(ld_plan* plan, int stage, const void* u, double* pos, void* vel,
                      const void* tau, void* a1, int64_t n, int method, double h, double g,
                      void* stream);
+
+/* ---- collisions (no counterpart in the reference: droplets there never collide) ----------- */
+/* A collider owns the workspace of the cell-list search for up to nmax droplets on an
+ * nc x nc x nc cell grid (nc = floor(L / cell_size), cell_size >= 2 * max radius, nc >= 1). */
+LD_API int ld_collider_create(ld_collider** collider, int64_t nmax, int32_t nc);
+LD_API int ld_collider_destroy(ld_collider* collider);
+/* Colliding pairs of n droplets, pos (n,3) double, radius (n) double, in a periodic box of side L:
+ * wrapped positions, cell = min(int(p / (L/nc)), nc-1) per axis, minimum-image FP64 distance
+ * ((dx*dx + dy*dy) + dz*dz < (ri + rj)^2, no fused multiply-add).  pairs (cap, 2) int32 receive
+ * (i, j), i < j, sorted by (i, j); *count (device int64) receives the number of colliding pairs,
+ * which may exceed cap: then only cap pairs are written and LD_STATUS_PAIR_OVERFLOW is raised
+ * in the collider's status word (ld_collider_status). */
+LD_API int ld_collide(ld_collider* collider, const double* pos, const double* radius, int64_t n, double L,
+                      int32_t* pairs, int64_t cap, int64_t* count, void* stream);
+LD_API int ld_collider_status(ld_collider* collider, uint32_t* flags, int clear, void* stream);
+/* Device pointers to the cell keys and droplet ids of the last ld_collide call, in cell order
+ * (valid until the next call): the order that keeps droplet gathers local. */
+LD_API int ld_collider_sorted(ld_collider* collider, const uint32_t** keys, const uint32_t** ids);
+/* Stable LSD radix sort of n (key, value) pairs on the low `bits` bits of the keys, in place,
+ * using the collider's workspace (n <= nmax). */
+LD_API int ld_radix_sort_u32(ld_collider* collider, uint32_t* keys, uint32_t* values, int64_t n, int bits,
+                             void* stream);
 
 /* ---- tracing -------------------------------------------------------------------------- */
 /* The reference times only whole steps on the wall clock (F:565-577, F:627).  With tracing on, a

@@ -55,6 +55,12 @@ SIGNATURES = {
                                ctypes.POINTER(_c_i32), _c_i]),
     "ld_kernel_name": (ctypes.c_char_p, [_c_i]),
     "ld_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),
+    "ld_collider_create": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32]),
+    "ld_collider_destroy": (_c_i, [_c_p]),
+    "ld_collide": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_i64, _c_p, _c_p]),
+    "ld_collider_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),
+    "ld_collider_sorted": (_c_i, [_c_p, ctypes.POINTER(_c_p), ctypes.POINTER(_c_p)]),
+    "ld_radix_sort_u32": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p]),
 }
 
 

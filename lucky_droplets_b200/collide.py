@@ -1,0 +1,62 @@
+"""Cell-list collision detection of droplets (no counterpart in the reference, whose droplets
+never collide).  The pair rule is bit-exact FP64 - see ld_collide in include/ld.h."""
+import ctypes
+import math
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+
+TWO_PI = 2.0 * math.pi
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Collider:
+    """Workspace for the collision search of up to ``nmax`` droplets with cells >= cell_size."""
+
+    def __init__(self, nmax, cell_size, L=TWO_PI, device=None):
+        torch = _torch()
+        self.L = float(L)
+        self.nc = max(1, int(math.floor(self.L / float(cell_size))))
+        self.nmax = int(nmax)
+        self.device = torch.device(device if device is not None else "cuda")
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().ld_collider_create(ctypes.byref(h), self.nmax, self.nc))
+        self._h = h
+        self.count = torch.zeros(1, dtype=torch.int64, device=self.device)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ld_collider_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def collide(self, pos, radius, pairs=None, cap=None, stream=None):
+        """Pairs (i, j), i < j, sorted, as an int32 (M, 2) tensor view; the device count is in
+        ``self.count`` (reading it synchronises)."""
+        torch = _torch()
+        n = int(pos.shape[0])
+        if pairs is None:
+            cap = cap or max(1024, 4 * n)
+            pairs = torch.empty((cap, 2), dtype=torch.int32, device=self.device)
+        cap = int(pairs.shape[0])
+        check(_lib.lib().ld_collide(self._h, ptr(pos), ptr(radius), n, self.L, ptr(pairs), cap, ptr(self.count),
+                                    stream_ptr(stream)))
+        m = int(self.count.item())
+        if m > cap:
+            raise RuntimeError(f"pair capacity {cap} exceeded ({m} colliding pairs)")
+        return pairs[:m]
+
+    def status(self, clear=True, stream=None):
+        v = ctypes.c_uint32()
+        check(_lib.lib().ld_collider_status(self._h, ctypes.byref(v), int(bool(clear)), stream_ptr(stream)))
+        return v.value

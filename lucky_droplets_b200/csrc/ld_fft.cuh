@@ -64,27 +64,43 @@ __host__ __device__ constexpr int bitrev(int i, int bits) {
 }
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
-// In-place length-R DFT of a[0..R-1] (natural order in and out), R in {1,2,4,8,16}.
-template <typename T, int R, bool INV> __device__ __forceinline__ void dft(cplx<T>* a) {
-  if constexpr (R == 1) return;
-  constexpr int B = ilog2(R);
+// One radix-2 pass (butterfly span LEN) of an in-place length-R DIT DFT, then the next pass.
+// LEN is a template constant so every loop has a compile-time trip count and every index into
+// a[] is static: the array stays in registers.
+template <typename T, int R, int LEN, bool INV> __device__ __forceinline__ void dft_pass(cplx<T>* a) {
+  if constexpr (LEN <= R) {
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int k = bitrev(i, B);
-    if (k > i) { cplx<T> t = a[i]; a[i] = a[k]; a[k] = t; }
-  }
+    for (int i = 0; i < R; i += LEN) {
 #pragma unroll
-  for (int len = 2; len <= R; len <<= 1) {
-#pragma unroll
-    for (int i = 0; i < R; i += len) {
-#pragma unroll
-      for (int q = 0; q < len / 2; ++q) {
-        cplx<T> u = a[i + q];
-        cplx<T> v = w16mul<T, INV>(a[i + q + len / 2], q * (16 / len));
+      for (int q = 0; q < LEN / 2; ++q) {
+        const cplx<T> u = a[i + q];
+        const cplx<T> v = w16mul<T, INV>(a[i + q + LEN / 2], q * (16 / LEN));
         a[i + q] = cadd(u, v);
-        a[i + q + len / 2] = csub(u, v);
+        a[i + q + LEN / 2] = csub(u, v);
       }
     }
+    dft_pass<T, R, 2 * LEN, INV>(a);
+  }
+}
+
+// Bit-reversal permutation of a[0..R-1], one compile-time swap at a time.
+template <typename T, int R, int I> __device__ __forceinline__ void bitrev_swaps(cplx<T>* a) {
+  if constexpr (I < R) {
+    constexpr int K = bitrev(I, ilog2(R));
+    if constexpr (K > I) {
+      const cplx<T> t = a[I];
+      a[I] = a[K];
+      a[K] = t;
+    }
+    bitrev_swaps<T, R, I + 1>(a);
+  }
+}
+
+// In-place length-R DFT of a[0..R-1] (natural order in and out), R in {1,2,4,8,16}.
+template <typename T, int R, bool INV> __device__ __forceinline__ void dft(cplx<T>* a) {
+  if constexpr (R > 1) {
+    bitrev_swaps<T, R, 0>(a);
+    dft_pass<T, R, 2, INV>(a);
   }
 }
 
@@ -96,8 +112,22 @@ template <typename T, bool INV> __device__ __forceinline__ cplx<T> twid(const cp
 }
 
 // Barrier kinds for the exchanges.
-struct SyncBlock { __device__ __forceinline__ void operator()() const { __syncthreads(); } };
-struct SyncWarp  { __device__ __forceinline__ void operator()() const { __syncwarp(); } };
+// Each barrier is bracketed by compiler memory clobbers so that no shared-memory access of the
+// exchange is moved across it.
+struct SyncBlock {
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("" ::: "memory");
+    __syncthreads();
+    asm volatile("" ::: "memory");
+  }
+};
+struct SyncWarp {
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("" ::: "memory");
+    __syncwarp();
+    asm volatile("" ::: "memory");
+  }
+};
 
 // Shared-memory slot of element p: with PAD one spare slot per E elements, which makes the
 // stride-E writes of stage 0 bank-conflict free for row buffers (sstride = 1).
