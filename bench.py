@@ -93,40 +93,52 @@ def allreduce_max(x, world):
 # clocks during the timed region
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    """Samples SM clock, max clock, power and clock-event reasons every 20 ms through NVML while
+    the timed region runs (read-only queries)."""
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
-    def __init__(self, device_index):
-        self.proc = None
-        self.lines = []
+    def __init__(self, device_index, period=0.02):
+        import threading
+        self.rows, self.err = [], None
+        self._stop = threading.Event()
+        self._t = None
         try:
+            import pynvml as nv
             import torch
-            uuid = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={uuid}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.proc = None
+            nv.nvmlInit()
+            pr = torch.cuda.get_device_properties(device_index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            self.nv = nv
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+
+            def loop():
+                while not self._stop.is_set():
+                    try:
+                        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                        pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                        self.rows.append((sm, pw, rs))
+                    except Exception as e:  # keep sampling; report the first error
+                        self.err = self.err or str(e)
+                    self._stop.wait(period)
+
+            self._t = threading.Thread(target=loop, daemon=True)
+            self._t.start()
+        except Exception as e:
+            self.err = str(e)
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except Exception:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
-        rows = [r.split(",") for r in out.strip().splitlines() if r.count(",") >= 7]
-        if not rows:
-            return None
-        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
-        smax = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].strip().lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self._t is None:
+            return {"error": self.err or "NVML unavailable"}
+        self._stop.set()
+        self._t.join(timeout=2)
+        if not self.rows:
+            return {"error": self.err or "no samples"}
+        sm = [r[0] for r in self.rows]
+        reasons = sorted({name for r in self.rows for bit, name in self.REASONS.items() if r[2] & bit})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.smax, "reasons": reasons,
+                "power_w_max": max(r[1] for r in self.rows), "samples": len(self.rows)}
 
 
 def measured_peaks():
