@@ -91,6 +91,16 @@ LD_API int ld_rfft_mpi(ld_plan* plan, const void* u, void* fu, int ncomp, void* 
 /* irfft_mpi (F:208-213): full-layout spectra -> real fields, 1/N^3 normalisation; the imaginary
  * parts of the kz = 0 and kz = N/2 coefficients are ignored, as pocketfft's c2r does. */
 LD_API int ld_irfft_mpi(ld_plan* plan, const void* fu, void* u, int ncomp, void* stream);
+/* irfft_mpi without any allocation - no counterpart in the reference.  For callers that must not
+ * allocate device memory: code running while a stream is captured into a CUDA graph in the
+ * global capture mode (cudaMalloc is not permitted there) and host frameworks that hand out all
+ * device memory from their own pool.  No plan: the scratch is a file-scope device array sized for
+ * N <= 64 (64*64*33 complex floats, 1.08 MB, held by every GPU that loads the library until the
+ * process exits) plus static twiddle tables.  FP32 only, N in {16, 32, 64}; larger N returns
+ * LD_ERR_UNSUPPORTED.  fu (ncomp, N, N, N/2+1) complex float, u (ncomp, N, N, N) float.  The first
+ * call on a device sets that device up (symbol-address lookup and a synchronous twiddle copy), so
+ * make it before any stream capture.  Calls share the scratch: calls that overlap on the GPU race. */
+LD_API int ld_irfft_mpi_noalloc(int n, const void* fu, void* u, int ncomp, void* stream);
 /* Dealiased transforms in the cube layout: the same transforms restricted to the modes of the
  * spherical mask (F:129) - the form every transform of the DNS step takes. */
 LD_API int ld_irfft_cube(ld_plan* plan, const void* uk, void* u, int ncomp, void* stream);

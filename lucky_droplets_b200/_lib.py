@@ -39,6 +39,7 @@ SIGNATURES = {
     "ld_plan_dims": (_c_i, [_c_p, ctypes.POINTER(_c_i32), ctypes.POINTER(ctypes.c_size_t)]),
     "ld_rfft_mpi": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
     "ld_irfft_mpi": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_irfft_mpi_noalloc": (_c_i, [_c_i, _c_p, _c_p, _c_i, _c_p]),
     "ld_irfft_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
     "ld_rfft_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
     "ld_spec_to_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
