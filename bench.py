@@ -47,6 +47,7 @@ def parse_args(argv=None):
     ap.add_argument("--interp", choices=["trilinear", "tricubic", "cosine"], default="tricubic")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--sort-every", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=150.0)
@@ -176,6 +177,11 @@ def algorithmic_bytes(plan, nd):
         "droplet1": nd * (drop + 3 * r) + 3 * phys,  # + a1 written; field read once
         "droplet2": nd * (drop + 3 * r + 24 + 3 * r) + 3 * phys,
         "forcing": 0,
+        # collisions: keys (read pos, write key+id) + 3 radix passes (read+write key+id);
+        # ranges, sorted copy (read pos+radius+id, write 32 B), count and emit (read 32 B each)
+        "collide_sort": nd * (24 + 8 + 3 * 16),
+        "collide_pairs": nd * (4 + 36 + 32 + 32 + 32 + 8),
+        "cell_order": nd * (24 + 8 + 3 * 16 + 4),
     }
 
 
@@ -203,12 +209,16 @@ def build_workload(a, seed):
     init_flow(dns, seed)
     d = None
     if a.nd > 0:
-        pos, tau, _ = init_droplets(a.nd, seed, "lognormal_r", nu=nu)
-        d = Droplets(dns.plan, pos, np.zeros((a.nd, 3)), tau, method=a.interp, g=0.1)
+        from lucky_droplets_b200.collide import Collider
+        pos, tau, radius = init_droplets(a.nd, seed, "lognormal_r", nu=nu)
+        d = Droplets(dns.plan, pos, np.zeros((a.nd, 3)), tau, method=a.interp, g=0.1, radius=radius)
         u = dns.velocity()
         d.vel.copy_(d.gather(u))  # droplets start at the interpolated fluid velocity
         del u
-        dns.attach(d)
+        # collision cells of 2 max radius; colliding pairs found after every step; droplets
+        # re-sorted into that cell order every sort_every steps
+        col = Collider(a.nd, 2.0 * float(radius.max()), device=dns.plan.device)
+        dns.attach(d, collider=col, sort_every=a.sort_every)
     torch.cuda.synchronize()
     return dns, d
 
@@ -281,13 +291,18 @@ def cpu_baseline(dns, d, a):
     pos = d.pos.cpu().numpy() if d is not None else None
     vel = d.vel.cpu().numpy().astype(np.float64) if d is not None else None
     tau = d.tau.cpu().numpy().astype(np.float64) if d is not None else None
+    radius = d.radius.cpu().numpy() if d is not None else None
     del torch
+    from oracle import collide_np as K
     t0 = time.perf_counter()
-    C.step(grid, prm, uk, pos, vel, tau, a.interp)
+    _, pos1, _ = C.step(grid, prm, uk, pos, vel, tau, a.interp)
+    if pos1 is not None:
+        K.collide(pos1, radius, 2.0 * radius.max())
     dt = time.perf_counter() - t0
     return {"value": 1.0 / dt, "unit": "steps/s", "cores": C._WORKERS, "kind": "port",
             "sample": f"1 full step of the same workload ({N}^3 FP64 RK2+IF flow, {a.nd} droplets "
-                      f"{a.interp}), {dt:.2f} s; NumPy/SciPy FP64 restatement, scipy.fft workers={C._WORKERS}"}
+                      f"{a.interp}, cell-list collisions), {dt:.2f} s; NumPy/SciPy/numba FP64 restatement, "
+                      f"scipy.fft workers={C._WORKERS}"}
 
 
 def run_ours(a):
@@ -299,6 +314,7 @@ def run_ours(a):
     ms = time_steps(dns, a.steps, a.warmup, world)
     clk = clocks.stop()
     flags = dns.check()
+    pairs = int(dns.collider.count.item()) if getattr(dns, "collider", None) is not None else None
     ms = allreduce_max(ms, world)
     ms_per_step = ms / a.steps
     value = world * a.steps / (ms / 1e3)
@@ -334,6 +350,7 @@ def run_ours(a):
            "kernels": kernels,
            "gpu_launches": int(round(launches_per_step * a.steps)),
            "status_flags": flags,
+           "collision_pairs_last_step": pairs,
            "clocks": clk}
     if not a.no_e2e:
         Ke = max(3, min(a.steps, 10))
@@ -363,9 +380,9 @@ def run_reference(a):
     prm = C.ConfigParams(N=a.N, nu=nu, dt=dt, eps=0.1, kf=2, g=0.1)
     grid = C.ConfigGrid(a.N)
     uk, u = C.init_flow(grid, prm, a.seed)
-    pos = tau = vel = None
+    pos = tau = vel = radius = None
     if a.nd > 0:
-        pos, tau, _ = C.init_droplets(prm, a.seed, "lognormal_r", nd=a.nd)
+        pos, tau, radius = C.init_droplets(prm, a.seed, "lognormal_r", nd=a.nd)
         vel = C.gather(u, pos, a.interp)
     del u
     t_first = None
@@ -374,9 +391,12 @@ def run_reference(a):
         t0 = time.perf_counter()
         uk, pos, vel = C.step(grid, prm, uk, pos, vel, tau, a.interp)
         t_first = time.perf_counter() - t0
+    from oracle import collide_np as K
     for i in range(a.steps):
         t0 = time.perf_counter()
         uk, pos, vel = C.step(grid, prm, uk, pos, vel, tau, a.interp)
+        if pos is not None:
+            K.collide(pos, radius, 2.0 * radius.max())
         total += time.perf_counter() - t0
         done += 1
         if total > a.cpu_budget_s:

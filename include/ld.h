@@ -127,14 +127,15 @@ LD_API int ld_velocity_rhs(ld_plan* plan, const void* uk, void* ku, void* u_out,
  *   stage 1: N1 = N(uk);    ustar = E (uk + h N1);  acc = E (uk + h/2 N1)
  *   stage 2: N2 = N(ustar); uk = acc + h/2 N2
  * N is the RHS above without the viscous term.  u_out (nullable) receives the physical
- * velocity of the stage input (uk at stage 1, ustar at stage 2) for the droplet stages. */
+ * velocity of the stage input (uk at stage 1, ustar at stage 2) for the droplet stages,
+ * interleaved (N, N, N, 4) as (u, v, w, 0) per grid point. */
 LD_API int ld_rk2if_stage(ld_plan* plan, int stage, void* uk, void* ustar, void* acc, void* u_out,
                    const ld_flow_params* prm, void* stream);
 /* Classical RK4 with explicit viscosity, one stage per call (F:335-362):
  *   stage s evaluates ku_s = RHS(y_s) with y_1 = uk and
  *   s=1: acc = uk + h/6 ku1, y = uk + h/2 ku1;  s=2: acc += h/3 ku2, y = uk + h/2 ku2;
  *   s=3: acc += h/3 ku3, y = uk + h ku3;        s=4: uk = acc + h/6 ku4.
- * u_out (nullable) receives the physical velocity of y_s. */
+ * u_out (nullable) receives the physical velocity of y_s, interleaved (N, N, N, 4). */
 LD_API int ld_rk4_stage(ld_plan* plan, int stage, void* uk, void* y, void* acc, void* u_out,
                  const ld_flow_params* prm, void* stream);
 /* End of a time step, F:596-620: the irfft->rfft "reality" round trip (which symmetrises the
@@ -152,10 +153,52 @@ LD_API int ld_gather(ld_plan* plan, const void* field, int ncomp, const double* 
  *   stage 1: a1 = (u(x) - v)/tau - g z                                         (writes a1)
  *   stage 2: xs = x + h v, vs = v + h a1, a2 = (u(xs) - vs)/tau - g z,
  *            x <- x + h/2 (v + vs), v <- v + h/2 (a1 + a2)                      (writes x, v)
- * pos (n,3) double, vel (n,3) and a1 (n,3) and tau (n) in the plan precision. */
+ * u is the interleaved (N, N, N, 4) velocity the stage functions write; pos (n,3) double, vel (n,3),
+ * a1 (n,3) and tau (n) in the plan precision. */
 LD_API int ld_droplet_stage(ld_plan* plan, int stage, const void* u, double* pos, void* vel,
                      const void* tau, void* a1, int64_t n, int method, double h, double g,
                      void* stream);
+
+/* ---- exact spectral velocity (no counterpart in the reference) ------------------------- */
+/* u_c(x) = (1/N^3) sum_k w_kz Re(uk_c(k) exp(i k.x)) over the modes of the spherical mask of a
+ * cube-layout 3-vector uk, in FP64, at n points pos (n,3) double -> out (n,3) double.  This is
+ * the continuous extension of irfft_mpi (F:208-213): at grid points the two agree.  Used as the
+ * judge of the interpolation error. */
+LD_API int ld_exact_sum(ld_plan* plan, const void* uk, const double* pos, int64_t n, double* out, void* stream);
+
+/* ---- learned interpolation (no counterpart in the reference) ------------------------------ */
+/* MLP 195 -> 128 SiLU -> 128 SiLU -> 3 on BF16 tensor-core tiles with FP32 accumulation, predicting
+ * (exact spectral - tricubic) / scale from the 4x4x4 stencil of (u, v, w) divided by its RMS
+ * `scale` and the fractional cell offsets minus 1/2.  Parameters: one FP32 vector of n_params
+ * (layout in csrc/ld_mlp.cu); the kernels read a packed BF16 copy (n_packed) made by ld_mlp_pack. */
+LD_API int ld_mlp_sizes(int64_t* n_params, int64_t* n_packed, int32_t* k_in, int32_t* batch_tile);
+LD_API int ld_mlp_pack(const float* params, void* packed, void* stream);
+/* Fused gather + tricubic + MLP at n droplets from the interleaved (N,N,N,4) velocity:
+ * out (n,3) = tricubic + scale * MLP(features). */
+LD_API int ld_mlp_infer(ld_plan* plan, const void* u4, const double* pos, int64_t n, const void* packed,
+                        const float* params, void* out, void* stream);
+/* uk * exp(i k.(s dx)) for a cube-layout 3-vector: the field translated so that its grid values are
+ * the original field's values at x_j + s dx (s in grid units). */
+LD_API int ld_phase_shift(ld_plan* plan, const void* uk, void* out, double sx, double sy, double sz, void* stream);
+/* Training samples at grid points idx[i] + s (grid units): X (ns, k_in) bf16 features from the
+ * interleaved field u4, T (ns,3) = (exact - tricubic)/scale with exact = ue (planar (3,N^3), the
+ * field phase-shifted by s) at idx[i], aux (ns,4) = tricubic xyz and scale. */
+LD_API int ld_mlp_samples(ld_plan* plan, const void* u4, const void* ue, const int64_t* idx, int64_t ns, double sx,
+                          double sy, double sz, void* X, float* T, float* aux, void* stream);
+/* Interpolation of an interleaved (N,N,N,4) velocity at n positions -> out (n,3). */
+LD_API int ld_gather4(ld_plan* plan, const void* u4, const double* pos, int64_t n, int method, void* out,
+                      void* stream);
+/* planar (3, N^3) -> interleaved (N^3, 4) in the plan precision. */
+LD_API int ld_interleave3(ld_plan* plan, const void* planar, void* out, void* stream);
+/* Floats of workspace ld_mlp_grad needs for a batch of nb samples. */
+LD_API int64_t ld_mlp_partial_floats(int64_t nb);
+/* Mean-squared-error loss and its exact gradient over a batch of nb samples (X bf16 (nb, k_in),
+ * T (nb,3)): deterministic fixed-order reductions.  grad: n_params floats; loss: 1 float. */
+LD_API int ld_mlp_grad(const void* X, const float* T, int64_t nb, const float* params, const void* packed,
+                       float* work, float* grad, float* loss, void* stream);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the FP32 parameters, then re-packs the BF16 copy. */
+LD_API int ld_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t step, float lr, void* packed,
+                       void* stream);
 
 /* ---- collisions (no counterpart in the reference: droplets there never collide) ----------- */
 /* A collider owns the workspace of the cell-list search for up to nmax droplets on an
@@ -165,15 +208,27 @@ LD_API int ld_collider_destroy(ld_collider* collider);
 /* Colliding pairs of n droplets, pos (n,3) double, radius (n) double, in a periodic box of side L:
  * wrapped positions, cell = min(int(p / (L/nc)), nc-1) per axis, minimum-image FP64 distance
  * ((dx*dx + dy*dy) + dz*dz < (ri + rj)^2, no fused multiply-add).  pairs (cap, 2) int32 receive
- * (i, j), i < j, sorted by (i, j); *count (device int64) receives the number of colliding pairs,
+ * (i, j), i < j, in a deterministic order (by the cell of the pair, with nc >= 3; by i with
+ * nc < 3); *count (device int64) receives the number of colliding pairs,
  * which may exceed cap: then only cap pairs are written and LD_STATUS_PAIR_OVERFLOW is raised
  * in the collider's status word (ld_collider_status). */
 LD_API int ld_collide(ld_collider* collider, const double* pos, const double* radius, int64_t n, double L,
                       int32_t* pairs, int64_t cap, int64_t* count, void* stream);
 LD_API int ld_collider_status(ld_collider* collider, uint32_t* flags, int clear, void* stream);
+/* Record this collider's launches in the event trace of `plan` (ld_profile); NULL stops. */
+LD_API int ld_collider_trace(ld_collider* collider, ld_plan* plan);
 /* Device pointers to the cell keys and droplet ids of the last ld_collide call, in cell order
  * (valid until the next call): the order that keeps droplet gathers local. */
 LD_API int ld_collider_sorted(ld_collider* collider, const uint32_t** keys, const uint32_t** ids);
+/* order[i] = the droplet that comes i-th in cell order (cell key of the wrapped position on the
+ * collider's grid, ties by index): the permutation that keeps droplet gathers local in memory. */
+LD_API int ld_cell_order(ld_collider* collider, const double* pos, int64_t n, double L, uint32_t* order,
+                         void* stream);
+/* dst row i = src row order[i] for n rows of row_bytes bytes (a multiple of 4); src != dst.  Applies
+ * a droplet permutation to every per-droplet array (the reference's send(), P:233-275, reorders the
+ * droplets the same way and tracks them by prtclid). */
+LD_API int ld_permute_rows(const void* src, void* dst, const uint32_t* order, int64_t n, int32_t row_bytes,
+                           void* stream);
 /* Stable LSD radix sort of n (key, value) pairs on the low `bits` bits of the keys, in place,
  * using the collider's workspace (n <= nmax). */
 LD_API int ld_radix_sort_u32(ld_collider* collider, uint32_t* keys, uint32_t* values, int64_t n, int bits,

@@ -56,12 +56,27 @@ SIGNATURES = {
                                ctypes.POINTER(_c_i32), _c_i]),
     "ld_kernel_name": (ctypes.c_char_p, [_c_i]),
     "ld_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),
+    "ld_exact_sum": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p]),
+    "ld_mlp_sizes": (_c_i, [ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i64), ctypes.POINTER(_c_i32),
+                            ctypes.POINTER(_c_i32)]),
+    "ld_mlp_pack": (_c_i, [_c_p, _c_p, _c_p]),
+    "ld_mlp_infer": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p]),
+    "ld_phase_shift": (_c_i, [_c_p, _c_p, _c_p, _c_d, _c_d, _c_d, _c_p]),
+    "ld_mlp_samples": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_d, _c_p, _c_p, _c_p, _c_p]),
+    "ld_interleave3": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
+    "ld_gather4": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
+    "ld_mlp_partial_floats": (_c_i64, [_c_i64]),
+    "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),
+    "ld_mlp_adam": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_float, _c_p, _c_p]),
     "ld_collider_create": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32]),
     "ld_collider_destroy": (_c_i, [_c_p]),
     "ld_collide": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_i64, _c_p, _c_p]),
     "ld_collider_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),
+    "ld_collider_trace": (_c_i, [_c_p, _c_p]),
     "ld_collider_sorted": (_c_i, [_c_p, ctypes.POINTER(_c_p), ctypes.POINTER(_c_p)]),
     "ld_radix_sort_u32": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p]),
+    "ld_cell_order": (_c_i, [_c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),
+    "ld_permute_rows": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i32, _c_p]),
 }
 
 

@@ -56,6 +56,15 @@ class Collider:
             raise RuntimeError(f"pair capacity {cap} exceeded ({m} colliding pairs)")
         return pairs[:m]
 
+    def cell_order(self, pos, order=None, stream=None):
+        """Permutation (int32) into cell order of the wrapped positions."""
+        torch = _torch()
+        n = int(pos.shape[0])
+        if order is None:
+            order = torch.empty(n, dtype=torch.int32, device=self.device)
+        check(_lib.lib().ld_cell_order(self._h, ptr(pos), n, self.L, ptr(order), stream_ptr(stream)))
+        return order
+
     def status(self, clear=True, stream=None):
         v = ctypes.c_uint32()
         check(_lib.lib().ld_collider_status(self._h, ctypes.byref(v), int(bool(clear)), stream_ptr(stream)))

@@ -26,6 +26,11 @@ enum LdKernelId : int {
   KID_CONVERT,       // cube <-> reference layout
   KID_SHELL,         // shell spectrum
   KID_IFAC,          // integrating-factor table
+  KID_EXACT,         // exact spectral sum at points
+  KID_COLL_SORT,     // collision cell keys + radix sort
+  KID_COLL_PAIRS,    // collision ranges, count, scan, emit
+  KID_CELL_ORDER,    // droplet cell-order permutation
+  KID_MLP_INFER,     // fused gather + tricubic + MLP
   KID_COUNT_BASE     // further ids are defined by later units
 };
 

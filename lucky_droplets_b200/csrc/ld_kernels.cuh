@@ -13,6 +13,7 @@
 #pragma once
 #include <type_traits>
 
+#include "ld_async.cuh"
 #include "ld_fft.cuh"
 
 namespace ld {
@@ -28,6 +29,15 @@ __device__ __forceinline__ int crow(int n, int N, int kc) {
 __device__ __forceinline__ int cfreq(int i, int kc) { return i <= kc ? i : i - (2 * kc + 1); }
 // logical FFT index -> signed frequency (fftfreq convention: N/2 -> -N/2)
 __device__ __forceinline__ int nfreq(int n, int N) { return n < N / 2 ? n : n - N; }
+
+// 4-vectors for interleaved physical fields (u, v, w, 0)
+template <typename T> struct V4T;
+template <> struct V4T<float> { using type = float4; };
+template <> struct V4T<double> { using type = double4; };
+template <typename T> using vec4 = typename V4T<T>::type;
+template <typename T> __device__ __forceinline__ vec4<T> mk4(T a, T b, T c, T d) {
+  vec4<T> v; v.x = a; v.y = b; v.z = c; v.w = d; return v;
+}
 
 template <int N> struct Cfg {
   // column passes: E elements per thread, TB columns per CTA
@@ -429,36 +439,27 @@ k_z_r2c(const T* __restrict__ x, cplx<T>* __restrict__ X, long long nrows, int s
   zstore_pair<T, N>(a, sb, A, hasb ? A + ss : nullptr, Kout, Kval, j, ok, ZSync<N>());
 }
 
-// Fused z pass of the nonlinear term: for each (x, y) row, C2R of the six y-transformed fields
-// [u, w] (cube kz rows), optional store of physical u, u x w (F:299-301), R2C of the three
-// products (kz < Mzp kept, zero beyond kc).  W: (6, N*N, Mzp) in; P: (3, N*N, Mzp) out.
+// One row of the fused z pass: C2R of the six y-transformed fields [u, w] (kz < Kin of each row
+// pointer in[f]), optional store of physical u, u x w (F:299-301), R2C of the three products
+// (kz < Mzp stored, zero beyond Kin) into P + f*fs + row*Mzp.
 template <typename T, int N>
-__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
-k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int Mzp,
-          int kc, T s, const cplx<T>* __restrict__ tw) {
+__device__ __forceinline__ void zcross_row(const cplx<T>* const* in, cplx<T>* sb, cplx<T>* P, long long fs,
+                                           long long row, T* uphys, int ulayout, int Mzp, int Kin, T s, int j,
+                                           const cplx<T>* __restrict__ tw) {
   constexpr int E = Cfg<N>::EZ, NT = Cfg<N>::NTZ;
   constexpr long long NR = (long long)N * N;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
-  cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
-  const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR exactly
-  const long long fs = NR * Mzp;
-  const int Kin = kc + 1;
+  using Sy = ZSync<N>;
   cplx<T> p0[E], p1[E], p2[E];
-  // pair (u_x, u_y)
-  zload_pair<T, N>(p0, W + row * Mzp, W + fs + row * Mzp, Kin, j, s);
-  fft_run<T, N, E, true, true>(p0, sb, 1, j, tw, ZSync<N>());
-  ZSync<N>()();
-  // pair (u_z, w_x)
-  zload_pair<T, N>(p1, W + 2 * fs + row * Mzp, W + 3 * fs + row * Mzp, Kin, j, s);
-  fft_run<T, N, E, true, true>(p1, sb, 1, j, tw, ZSync<N>());
-  ZSync<N>()();
-  // pair (w_y, w_z)
-  zload_pair<T, N>(p2, W + 4 * fs + row * Mzp, W + 5 * fs + row * Mzp, Kin, j, s);
-  fft_run<T, N, E, true, true>(p2, sb, 1, j, tw, ZSync<N>());
-  ZSync<N>()();
-  if (uphys) {
+  zload_pair<T, N>(p0, in[0], in[1], Kin, j, s);  // pair (u_x, u_y)
+  fft_run<T, N, E, true, true>(p0, sb, 1, j, tw, Sy());
+  Sy()();
+  zload_pair<T, N>(p1, in[2], in[3], Kin, j, s);  // pair (u_z, w_x)
+  fft_run<T, N, E, true, true>(p1, sb, 1, j, tw, Sy());
+  Sy()();
+  zload_pair<T, N>(p2, in[4], in[5], Kin, j, s);  // pair (w_y, w_z)
+  fft_run<T, N, E, true, true>(p2, sb, 1, j, tw, Sy());
+  Sy()();
+  if (uphys && ulayout == 0) {  // planar (3, N, N, N)
     const long long NN3 = NR * N;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
@@ -466,6 +467,13 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
       uphys[row * N + n] = p0[m].x;
       uphys[NN3 + row * N + n] = p0[m].y;
       uphys[2 * NN3 + row * N + n] = p1[m].x;
+    }
+  } else if (uphys) {  // interleaved (N, N, N, 4): (u, v, w, 0) per grid point
+    vec4<T>* u4 = reinterpret_cast<vec4<T>*>(uphys);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int n = j + NT * m;
+      u4[row * N + n] = mk4<T>(p0[m].x, p0[m].y, p1[m].x, T(0));
     }
   }
   // products: (u x w) = (uy wz - uz wy, uz wx - ux wz, ux wy - uy wx)
@@ -475,12 +483,95 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
     p0[m] = cmk(wz * uy - wy * uz, wx * uz - wz * ux);
     p1[m] = cmk(wy * ux - wx * uy, T(0));
   }
-  fft_run<T, N, E, false, true>(p0, sb, 1, j, tw, ZSync<N>());
-  ZSync<N>()();
-  zstore_pair<T, N>(p0, sb, P + row * Mzp, P + fs + row * Mzp, Mzp, Kin, j, true, ZSync<N>());
-  ZSync<N>()();
-  fft_run<T, N, E, false, true>(p1, sb, 1, j, tw, ZSync<N>());
-  zstore_pair<T, N>(p1, sb, P + 2 * fs + row * Mzp, (cplx<T>*)nullptr, Mzp, Kin, j, true, ZSync<N>());
+  fft_run<T, N, E, false, true>(p0, sb, 1, j, tw, Sy());
+  Sy()();
+  zstore_pair<T, N>(p0, sb, P + row * Mzp, P + fs + row * Mzp, Mzp, Kin, j, true, Sy());
+  Sy()();
+  fft_run<T, N, E, false, true>(p1, sb, 1, j, tw, Sy());
+  zstore_pair<T, N>(p1, sb, P + 2 * fs + row * Mzp, (cplx<T>*)nullptr, Mzp, Kin, j, true, Sy());
+}
+
+// Fused z pass, one row unit per NTZ threads, rows read straight from global memory.
+// W: (6, N*N, Mzp) in; P: (3, N*N, Mzp) out.
+template <typename T, int N>
+__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
+k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
+          int kc, T s, const cplx<T>* __restrict__ tw) {
+  constexpr int NT = Cfg<N>::NTZ;
+  constexpr long long NR = (long long)N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
+  cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
+  const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR exactly
+  const long long fs = NR * Mzp;
+  const cplx<T>* in[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) in[f] = W + f * fs + row * Mzp;
+  zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, Mzp, kc + 1, s, j, tw);
+}
+
+// Pipelined fused z pass for one warp per row (N >= 256): persistent warps walk the rows with a
+// stride; lane 0 of each warp prefetches the next row's six field rows into a double-buffered
+// shared staging area with bulk asynchronous copies (the TMA engine), completed on per-buffer
+// mbarriers, while the warp transforms the current row.  Waits are bounded: on time-out the
+// warp raises LD_STATUS_WAIT_TIMEOUT, drains its copies in flight (again bounded) and returns.
+// Shared memory per warp: 2 x 6 x Mzp staging + ZBUF exchange elements, then 2 mbarriers.
+constexpr unsigned kWaitLimit = 1u << 24;
+
+template <typename T, int N>
+__global__ void __launch_bounds__(256)
+k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
+               int kc, T s, const cplx<T>* __restrict__ tw, unsigned* status) {
+  static_assert(Cfg<N>::NTZ == 32, "one warp per row");
+  constexpr long long NR = (long long)N * N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const long long stage_elems = 12LL * Mzp;
+  cplx<T>* base = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* stage = base + warp * stage_elems;
+  cplx<T>* sb = base + nwarps * stage_elems + warp * Cfg<N>::ZBUF;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + nwarps * (stage_elems + Cfg<N>::ZBUF)) + 2 * warp;
+  const long long fs = NR * Mzp;
+  const unsigned rowbytes = (unsigned)(Mzp * sizeof(cplx<T>));
+  const long long stride = (long long)gridDim.x * nwarps;
+  long long row = (long long)blockIdx.x * nwarps + warp;
+  if (lane == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init_fence();
+  }
+  __syncwarp();
+  auto issue = [&](long long r, int b) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bars[b], 6u * rowbytes);
+#pragma unroll
+      for (int f = 0; f < 6; ++f) bulk_g2s(stage + (6 * b + f) * (long long)Mzp, W + f * fs + r * Mzp, rowbytes, &bars[b]);
+    }
+  };
+  unsigned ph[2] = {0u, 0u};
+  bool pend[2] = {false, false};
+  if (row < NR) { issue(row, 0); pend[0] = true; }
+  int b = 0;
+  for (; row < NR; row += stride, b ^= 1) {
+    const long long next = row + stride;
+    if (next < NR) { issue(next, b ^ 1); pend[b ^ 1] = true; }
+    if (!mbar_wait_bounded(&bars[b], ph[b], kWaitLimit)) {
+      if (lane == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
+      for (int q = 0; q < 2; ++q)
+        if (pend[q]) mbar_wait_bounded(&bars[q], ph[q], kWaitLimit);
+      return;
+    }
+    ph[b] ^= 1u;
+    pend[b] = false;
+    const cplx<T>* st = stage + 6 * b * (long long)Mzp;
+    const cplx<T>* in[6];
+#pragma unroll
+    for (int f = 0; f < 6; ++f) in[f] = st + f * Mzp;
+    zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, Mzp, kc + 1, s, lane, tw);
+    __syncwarp();  // every lane is done with staging buffer b and the exchange buffer
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -745,18 +836,70 @@ __global__ void k_gather(const T* __restrict__ f, int ncomp, int N, double L, co
   }
 }
 
+// Interpolation of an interleaved (N, N, N, 4) velocity: one 16/32-byte load per stencil point.
+template <typename T, int METHOD>
+__device__ __forceinline__ void gather_point4(const vec4<T>* __restrict__ f, int N, double L, double px, double py,
+                                              double pz, T* out) {
+  using A = AxisW<T, METHOD>;
+  constexpr int W = A::W, LO = A::LO;
+  int ix, iy, iz;
+  T wx[W], wy[W], wz[W];
+  A::get(px, N, L, ix, wx);
+  A::get(py, N, L, iy, wy);
+  A::get(pz, N, L, iz, wz);
+  int jz[W];
+#pragma unroll
+  for (int c = 0; c < W; ++c) jz[c] = (iz + LO + c + N) & (N - 1);
+  T o0 = 0, o1 = 0, o2 = 0;
+#pragma unroll
+  for (int a = 0; a < W; ++a) {
+    const int jx = (ix + LO + a + N) & (N - 1);
+#pragma unroll
+    for (int b = 0; b < W; ++b) {
+      const int jy = (iy + LO + b + N) & (N - 1);
+      const vec4<T>* row = f + ((long long)jx * N + jy) * N;
+      T s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        const vec4<T> v = row[jz[q]];
+        s0 += wz[q] * v.x;
+        s1 += wz[q] * v.y;
+        s2 += wz[q] * v.z;
+      }
+      const T wab = wx[a] * wy[b];
+      o0 += wab * s0;
+      o1 += wab * s1;
+      o2 += wab * s2;
+    }
+  }
+  out[0] = o0;
+  out[1] = o1;
+  out[2] = o2;
+}
+
+template <typename T, int METHOD>
+__global__ void k_gather4(const vec4<T>* __restrict__ f, int N, double L, const double* __restrict__ pos, long long n,
+                          T* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    T v[3];
+    gather_point4<T, METHOD>(f, N, L, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], v);
+    out[3 * i] = v[0];
+    out[3 * i + 1] = v[1];
+    out[3 * i + 2] = v[2];
+  }
+}
+
 template <typename T, int METHOD, int STAGE>
-__global__ void k_droplet_stage(const T* __restrict__ u, int N, double L, double* __restrict__ pos,
+__global__ void k_droplet_stage(const vec4<T>* __restrict__ u, int N, double L, double* __restrict__ pos,
                                 T* __restrict__ vel, const T* __restrict__ tau, T* __restrict__ a1,
                                 long long n, double h, T g) {
-  const long long fs = (long long)N * N * N;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
     const T vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
     const T it = T(1) / tau[i];
     T up[3];
     if (STAGE == 1) {
-      gather_point<T, METHOD>(u, 3, fs, N, L, px, py, pz, up);
+      gather_point4<T, METHOD>(u, N, L, px, py, pz, up);
       a1[3 * i] = (up[0] - vx) * it;
       a1[3 * i + 1] = (up[1] - vy) * it;
       a1[3 * i + 2] = (up[2] - vz) * it - g;
@@ -765,7 +908,7 @@ __global__ void k_droplet_stage(const T* __restrict__ u, int N, double L, double
       const T hh = T(h);
       const T sx = vx + hh * ax, sy = vy + hh * ay, sz = vz + hh * az;  // vs = v + h a1
       const double qx = px + h * double(vx), qy = py + h * double(vy), qz = pz + h * double(vz);
-      gather_point<T, METHOD>(u, 3, fs, N, L, qx, qy, qz, up);
+      gather_point4<T, METHOD>(u, N, L, qx, qy, qz, up);
       const T bx = (up[0] - sx) * it, by = (up[1] - sy) * it, bz = (up[2] - sz) * it - g;
       pos[3 * i] = px + 0.5 * h * (double(vx) + double(sx));
       pos[3 * i + 1] = py + 0.5 * h * (double(vy) + double(sy));

@@ -1,0 +1,679 @@
+// Learned interpolation: an MLP that predicts the correction from tricubic interpolation to the
+// exact spectral velocity at a droplet, from the droplet's 4x4x4 stencil of (u, v, w) and its
+// fractional cell offset.  No counterpart in the reference.
+//
+// Network: 195 inputs -> 128 SiLU -> 128 SiLU -> 3.  Operands are BF16 on the tensor cores
+// (mma.sync m16n8k16, FP32 accumulation); master weights, biases and the optimiser are FP32.
+//
+// Features of a point with stencil values s (192 = 3 components x 64 taps, tap order
+// c*64 + a*16 + b*4 + q for offsets a, b, q in -1..2 along x, y, z) and cell offsets t (3):
+//   scale   = sqrt(mean(s^2)) + 1e-30
+//   x[0:192] = s / scale,  x[192:195] = t - 0.5,  x[195:208] = 0
+//   u(point) = tricubic(s, t) + scale * MLP(x)
+// Per-point normalisation keeps the inputs O(1) and makes the prediction scale with the field,
+// as the exact correction (a linear functional of the field) does.
+//
+// Parameter vector (FP32, contiguous), "params":
+//   W1 [208][128] (input-major; rows 195..207 stay zero)  b1 [128]
+//   W2 [128][128]                                          b2 [128]
+//   W3 [128][8]   (columns 3..7 stay zero)                 b3 [8]
+// Packed BF16 copies for the tensor cores ("packed"), output-major with padded rows:
+//   W1t [128][KP1]   W2t [128][KP2]   W2n [128][KP2] (= W2, input-major)   W3t [8][KP2]   W3n [128][8]
+#include <cmath>
+
+#include <cuda_bf16.h>
+
+#include "ld_internal.cuh"
+#include "ld_kernels.cuh"
+
+namespace {
+
+using namespace ld;
+
+constexpr int D_IN = 195, K1 = 208, H = 128, D_OUT = 3, N3 = 8;
+constexpr int KP1 = 216;  // padded row stride (bf16) of 208-long rows: conflict-free fragment loads
+constexpr int KP2 = 136;  // padded row stride of 128-long rows
+constexpr int XP = 216;   // feature rows in shared memory
+
+constexpr int OFF_W1 = 0;
+constexpr int OFF_B1 = OFF_W1 + K1 * H;
+constexpr int OFF_W2 = OFF_B1 + H;
+constexpr int OFF_B2 = OFF_W2 + H * H;
+constexpr int OFF_W3 = OFF_B2 + H;
+constexpr int OFF_B3 = OFF_W3 + H * N3;
+constexpr int N_PARAMS = OFF_B3 + N3;
+
+constexpr int P_W1T = 0;
+constexpr int P_W2T = P_W1T + H * KP1;
+constexpr int P_W2N = P_W2T + H * KP2;
+constexpr int P_W3T = P_W2N + H * KP2;
+constexpr int P_W3N = P_W3T + N3 * KP2;
+constexpr int N_PACKED = P_W3N + H * N3;
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ unsigned pack2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const unsigned*>(&v);
+}
+
+__device__ __forceinline__ void mma16816(float* d, const unsigned* a, const unsigned* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+__device__ __forceinline__ float dsilu(float z) {
+  const float s = 1.f / (1.f + __expf(-z));
+  return s * (1.f + z * (1.f - s));
+}
+
+// Warp tile: 16 rows of A (row-major, stride lda bf16) times B^T given output-major (Bt[n][k],
+// stride ldb): acc[nt][4] for NT n8 tiles over K (multiple of 16).
+template <int NT, int K>
+__device__ __forceinline__ void warp_gemm(float (*acc)[4], const bf16* A, int lda, const bf16* Bt, int ldb, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    unsigned a[4];
+    a[0] = *reinterpret_cast<const unsigned*>(A + g * lda + k0 + 2 * t);
+    a[1] = *reinterpret_cast<const unsigned*>(A + (g + 8) * lda + k0 + 2 * t);
+    a[2] = *reinterpret_cast<const unsigned*>(A + g * lda + k0 + 8 + 2 * t);
+    a[3] = *reinterpret_cast<const unsigned*>(A + (g + 8) * lda + k0 + 8 + 2 * t);
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      unsigned b[2];
+      const bf16* bp = Bt + (nt * 8 + g) * ldb + k0 + 2 * t;
+      b[0] = *reinterpret_cast<const unsigned*>(bp);
+      b[1] = *reinterpret_cast<const unsigned*>(bp + 8);
+      mma16816(acc[nt], a, b);
+    }
+  }
+}
+
+// Tricubic stencil of one point from the interleaved field: writes 192 stencil values (fp32) and
+// returns the tricubic velocity and the fractional offsets.
+template <typename T>
+__device__ __forceinline__ void stencil_point(const vec4<T>* __restrict__ f, int N, double L, double px, double py,
+                                              double pz, float* st, float* tric, float* toff) {
+  using A = AxisW<T, LD_INTERP_TRICUBIC>;
+  int ix, iy, iz;
+  T wx[4], wy[4], wz[4];
+  A::get(px, N, L, ix, wx);
+  A::get(py, N, L, iy, wy);
+  A::get(pz, N, L, iz, wz);
+  const double sc = double(N) / L;
+  double tx = px * sc, ty = py * sc, tz = pz * sc;
+  toff[0] = float(tx - floor(tx));
+  toff[1] = float(ty - floor(ty));
+  toff[2] = float(tz - floor(tz));
+  float o0 = 0, o1 = 0, o2 = 0;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int jx = (ix - 1 + a + N) & (N - 1);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int jy = (iy - 1 + b + N) & (N - 1);
+      const vec4<T>* row = f + ((long long)jx * N + jy) * N;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int jz = (iz - 1 + q + N) & (N - 1);
+        const vec4<T> v = row[jz];
+        const int tap = a * 16 + b * 4 + q;
+        st[tap] = float(v.x);
+        st[64 + tap] = float(v.y);
+        st[128 + tap] = float(v.z);
+        const float w = float(wx[a] * wy[b] * wz[q]);
+        o0 += w * float(v.x);
+        o1 += w * float(v.y);
+        o2 += w * float(v.z);
+      }
+    }
+  }
+  tric[0] = o0;
+  tric[1] = o1;
+  tric[2] = o2;
+}
+
+// Features of one point into a bf16 row of K1 (+ scale); st = 192 stencil values.
+__device__ __forceinline__ float features_row(const float* st, const float* toff, bf16* row) {
+  float ss = 0.f;
+  for (int i = 0; i < 192; ++i) ss += st[i] * st[i];
+  const float scale = sqrtf(ss / 192.f) + 1e-30f;
+  const float inv = 1.f / scale;
+  for (int i = 0; i < 192; ++i) row[i] = __float2bfloat16_rn(st[i] * inv);
+  for (int i = 0; i < 3; ++i) row[192 + i] = __float2bfloat16_rn(toff[i] - 0.5f);
+  for (int i = D_IN; i < K1; ++i) row[i] = __float2bfloat16_rn(0.f);
+  return scale;
+}
+
+// ---- packing -----------------------------------------------------------------------------------
+__global__ void k_mlp_pack(const float* __restrict__ p, bf16* __restrict__ q) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PACKED; e += gridDim.x * blockDim.x) {
+    float v = 0.f;
+    if (e < P_W2T) {  // W1t[o][k] = W1[k][o]
+      const int o = (e - P_W1T) / KP1, k = (e - P_W1T) % KP1;
+      v = k < K1 ? p[OFF_W1 + k * H + o] : 0.f;
+    } else if (e < P_W2N) {  // W2t[o][i] = W2[i][o]
+      const int o = (e - P_W2T) / KP2, i = (e - P_W2T) % KP2;
+      v = i < H ? p[OFF_W2 + i * H + o] : 0.f;
+    } else if (e < P_W3T) {  // W2n[i][o] = W2[i][o]
+      const int i = (e - P_W2N) / KP2, o = (e - P_W2N) % KP2;
+      v = o < H ? p[OFF_W2 + i * H + o] : 0.f;
+    } else if (e < P_W3N) {  // W3t[o][i] = W3[i][o]
+      const int o = (e - P_W3T) / KP2, i = (e - P_W3T) % KP2;
+      v = i < H ? p[OFF_W3 + i * N3 + o] : 0.f;
+    } else {  // W3n[i][o] = W3[i][o]
+      const int r = e - P_W3N;
+      v = p[OFF_W3 + r];
+    }
+    q[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// ---- shared forward of one 16-row warp tile ------------------------------------------------------
+// X (16 x XP bf16) -> h1, h2 (16 x KP2 bf16, activations), z1, z2 (pre-activations, fp32, optional),
+// y (16 x 3 fp32 in registers, held by lanes with (lane&3) < 2 as in the C fragment layout).
+struct MlpSmemW {
+  bf16* W1t;
+  bf16* W2t;
+  bf16* W3t;
+  const float* b;  // params (biases read from global/L1)
+};
+
+__device__ __forceinline__ void tile_forward(const bf16* X, bf16* h1, bf16* h2, float* z1s, float* z2s,
+                                             const MlpSmemW& w, const float* __restrict__ params, float (&y)[4],
+                                             int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  float acc[16][4];
+  warp_gemm<16, K1>(acc, X, XP, w.W1t, KP1, lane);
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const int c = nt * 8 + 2 * t;
+    const float b0 = params[OFF_B1 + c], b1v = params[OFF_B1 + c + 1];
+    const float z00 = acc[nt][0] + b0, z01 = acc[nt][1] + b1v, z10 = acc[nt][2] + b0, z11 = acc[nt][3] + b1v;
+    if (z1s) {
+      z1s[g * H + c] = z00; z1s[g * H + c + 1] = z01;
+      z1s[(g + 8) * H + c] = z10; z1s[(g + 8) * H + c + 1] = z11;
+    }
+    *reinterpret_cast<unsigned*>(h1 + g * KP2 + c) = pack2(silu(z00), silu(z01));
+    *reinterpret_cast<unsigned*>(h1 + (g + 8) * KP2 + c) = pack2(silu(z10), silu(z11));
+  }
+  __syncwarp();
+  warp_gemm<16, H>(acc, h1, KP2, w.W2t, KP2, lane);
+#pragma unroll
+  for (int nt = 0; nt < 16; ++nt) {
+    const int c = nt * 8 + 2 * t;
+    const float b0 = params[OFF_B2 + c], b1v = params[OFF_B2 + c + 1];
+    const float z00 = acc[nt][0] + b0, z01 = acc[nt][1] + b1v, z10 = acc[nt][2] + b0, z11 = acc[nt][3] + b1v;
+    if (z2s) {
+      z2s[g * H + c] = z00; z2s[g * H + c + 1] = z01;
+      z2s[(g + 8) * H + c] = z10; z2s[(g + 8) * H + c + 1] = z11;
+    }
+    *reinterpret_cast<unsigned*>(h2 + g * KP2 + c) = pack2(silu(z00), silu(z01));
+    *reinterpret_cast<unsigned*>(h2 + (g + 8) * KP2 + c) = pack2(silu(z10), silu(z11));
+  }
+  __syncwarp();
+  float a3[1][4];
+  warp_gemm<1, H>(a3, h2, KP2, w.W3t, KP2, lane);
+  // C fragment: rows g, g+8; cols 2t, 2t+1 (only cols < 3 are outputs)
+  const int c = 2 * t;
+  y[0] = a3[0][0] + (c < N3 ? params[OFF_B3 + c] : 0.f);
+  y[1] = a3[0][1] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
+  y[2] = a3[0][2] + (c < N3 ? params[OFF_B3 + c] : 0.f);
+  y[3] = a3[0][3] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
+}
+
+// Loads the packed forward weights into shared memory (whole CTA).
+__device__ __forceinline__ void load_weights(const bf16* __restrict__ packed, bf16* s_w1t, bf16* s_w2t, bf16* s_w3t) {
+  const unsigned* src1 = reinterpret_cast<const unsigned*>(packed + P_W1T);
+  unsigned* d1 = reinterpret_cast<unsigned*>(s_w1t);
+  for (int i = threadIdx.x; i < H * KP1 / 2; i += blockDim.x) d1[i] = src1[i];
+  const unsigned* src2 = reinterpret_cast<const unsigned*>(packed + P_W2T);
+  unsigned* d2 = reinterpret_cast<unsigned*>(s_w2t);
+  for (int i = threadIdx.x; i < H * KP2 / 2; i += blockDim.x) d2[i] = src2[i];
+  const unsigned* src3 = reinterpret_cast<const unsigned*>(packed + P_W3T);
+  unsigned* d3 = reinterpret_cast<unsigned*>(s_w3t);
+  for (int i = threadIdx.x; i < N3 * KP2 / 2; i += blockDim.x) d3[i] = src3[i];
+}
+
+constexpr int WARPS = 8;
+constexpr size_t SMEM_W = sizeof(bf16) * ((size_t)H * KP1 + (size_t)H * KP2 + (size_t)N3 * KP2);
+constexpr size_t SMEM_TILE_INFER = sizeof(bf16) * (16 * XP + 2 * 16 * KP2) + sizeof(float) * (16 * 4);
+constexpr size_t SMEM_INFER = SMEM_W + WARPS * SMEM_TILE_INFER;
+
+// ---- fused inference: gather + tricubic + MLP ---------------------------------------------------
+// u4: interleaved (N,N,N,4) velocity; pos (n,3) -> out (n,3) = tricubic + scale * MLP.
+template <typename T>
+__global__ void __launch_bounds__(WARPS * 32)
+k_mlp_infer(const vec4<T>* __restrict__ u4, int N, double L, const double* __restrict__ pos, long long n,
+            const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  bf16* s_w1t = reinterpret_cast<bf16*>(smem_raw);
+  bf16* s_w2t = s_w1t + H * KP1;
+  bf16* s_w3t = s_w2t + H * KP2;
+  unsigned char* tiles = smem_raw + SMEM_W;
+  load_weights(packed, s_w1t, s_w2t, s_w3t);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* mine = tiles + warp * SMEM_TILE_INFER;
+  bf16* X = reinterpret_cast<bf16*>(mine);
+  bf16* h1 = X + 16 * XP;
+  bf16* h2 = h1 + 16 * KP2;
+  float* aux = reinterpret_cast<float*>(h2 + 16 * KP2);  // [16][4]: tricubic xyz, scale
+  MlpSmemW w{s_w1t, s_w2t, s_w3t, params};
+  const long long ntiles = (n + 15) / 16;
+  for (long long tile = (long long)blockIdx.x * WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * WARPS) {
+    // gather: lanes 0..15 build one row each
+    if (lane < 16) {
+      const long long i = tile * 16 + lane;
+      float st[192], tric[3], toff[3];
+      if (i < n) {
+        stencil_point<T>(u4, N, L, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], st, tric, toff);
+      } else {
+        for (int q = 0; q < 192; ++q) st[q] = 0.f;
+        tric[0] = tric[1] = tric[2] = 0.f;
+        toff[0] = toff[1] = toff[2] = 0.5f;
+      }
+      const float scale = features_row(st, toff, X + lane * XP);
+      aux[lane * 4 + 0] = tric[0];
+      aux[lane * 4 + 1] = tric[1];
+      aux[lane * 4 + 2] = tric[2];
+      aux[lane * 4 + 3] = scale;
+    }
+    __syncwarp();
+    float y[4];
+    tile_forward(X, h1, h2, nullptr, nullptr, w, params, y, lane);
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = g + 8 * h;
+      const long long i = tile * 16 + r;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int c = 2 * t + q;
+        if (i < n && c < D_OUT) out[3 * i + c] = T(aux[r * 4 + c] + aux[r * 4 + 3] * y[2 * h + q]);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---- training samples ------------------------------------------------------------------------------
+// For sample s: point = grid point idx[s] + shift (in grid units), exact velocity = ue (planar
+// (3, N^3)) at idx[s] (ue is the field phase-shifted by `shift`), features from the unshifted
+// interleaved field u4.  Writes X row, target T = (exact - tricubic)/scale, tricubic and scale.
+template <typename T>
+__global__ void k_mlp_samples(const vec4<T>* __restrict__ u4, const T* __restrict__ ue, int N, double L,
+                              const long long* __restrict__ idx, long long ns, double sx, double sy, double sz,
+                              bf16* __restrict__ X, float* __restrict__ Tg, float* __restrict__ aux) {
+  const long long N3g = (long long)N * N * N;
+  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < ns; s += (long long)gridDim.x * blockDim.x) {
+    const long long j = idx[s];
+    const long long jx = j / ((long long)N * N), jy = (j / N) % N, jz = j % N;
+    const double dx = L / N;
+    const double px = (jx + sx) * dx, py = (jy + sy) * dx, pz = (jz + sz) * dx;
+    float st[192], tric[3], toff[3];
+    stencil_point<T>(u4, N, L, px, py, pz, st, tric, toff);
+    const float scale = features_row(st, toff, X + s * K1);
+    for (int c = 0; c < 3; ++c) {
+      const float ex = float(ue[c * N3g + j]);
+      Tg[s * 3 + c] = (ex - tric[c]) / scale;
+      aux[s * 4 + c] = tric[c];
+    }
+    aux[s * 4 + 3] = scale;
+  }
+}
+
+// uk * exp(i k . shift dx): the spectrum of the field translated by -shift (its values at grid
+// point j are the field's values at x_j + shift).
+template <typename T>
+__global__ void k_phase_shift(const ld::cplx<T>* __restrict__ in, ld::cplx<T>* __restrict__ out, long long cs, int kc,
+                              int My, int Mzp, double ax, double ay, double az) {
+  const long long total = 3 * cs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e % cs;
+    const int ix = (int)(r / ((long long)My * Mzp));
+    const int iy = (int)((r / Mzp) % My);
+    const int kz = (int)(r % Mzp);
+    const int kx = ix <= kc ? ix : ix - My, ky = iy <= kc ? iy : iy - My;
+    double sn, cn;
+    sincos(ax * kx + ay * ky + az * kz, &sn, &cn);
+    const ld::cplx<T> v = in[e];
+    out[e] = ld::cmk(T(v.x * cn - v.y * sn), T(v.x * sn + v.y * cn));
+  }
+}
+
+// ---- training: forward + backward of a batch, per-CTA gradient partials ---------------------------
+// CTA = 4 warps = 64 samples.  B operands come straight from the packed weights in global memory
+// (L1/L2 resident); shared memory holds the CTA's X, H1, H2 (bf16), Z1, Z2 (fp32, overwritten by
+// dZ1, dZ2) and dY.  Weight gradients are fixed-order sums over the 64 rows (deterministic).
+constexpr int TWARPS = 4;
+constexpr int TB = TWARPS * 16;
+constexpr size_t SMEM_TRAIN = sizeof(bf16) * ((size_t)TB * XP + 2 * (size_t)TB * KP2) +
+                              sizeof(float) * (2 * (size_t)TB * H + (size_t)TB * 4);
+
+__global__ void __launch_bounds__(TWARPS * 32)
+k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, long long nb, float inv_norm,
+            const bf16* __restrict__ packed, const float* __restrict__ params, float* __restrict__ gpart,
+            float* __restrict__ lpart) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  bf16* X = reinterpret_cast<bf16*>(smem_raw);
+  bf16* h1 = X + TB * XP;
+  bf16* h2 = h1 + TB * KP2;
+  float* z1 = reinterpret_cast<float*>(h2 + TB * KP2);
+  float* z2 = z1 + TB * H;
+  float* dy = z2 + TB * H;  // [TB][4]
+  __shared__ float lw[TWARPS];
+  const long long r0 = (long long)blockIdx.x * TB;
+  for (int e = threadIdx.x; e < TB * K1 / 2; e += blockDim.x) {
+    const int r = e / (K1 / 2), k2 = e % (K1 / 2);
+    unsigned v = 0u;
+    if (r0 + r < nb) v = reinterpret_cast<const unsigned*>(Xg + (r0 + r) * K1)[k2];
+    reinterpret_cast<unsigned*>(X + r * XP)[k2] = v;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const bf16* W1t = packed + P_W1T;
+  const bf16* W2t = packed + P_W2T;
+  const bf16* W2n = packed + P_W2N;
+  const bf16* W3t = packed + P_W3T;
+  const bf16* W3n = packed + P_W3N;
+  MlpSmemW w{const_cast<bf16*>(W1t), const_cast<bf16*>(W2t), const_cast<bf16*>(W3t), params};
+  float y[4];
+  const int rw = warp * 16;
+  tile_forward(X + rw * XP, h1 + rw * KP2, h2 + rw * KP2, z1 + rw * H, z2 + rw * H, w, params, y, lane);
+  // dY = 2 (Y - T) / B on valid rows (zero elsewhere); loss partial
+  float lsum = 0.f;
+#pragma unroll
+  for (int hh = 0; hh < 2; ++hh) {
+    const int r = rw + g + 8 * hh;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = 2 * t + q;
+      float d = 0.f;
+      if (c < D_OUT && r0 + r < nb) {
+        const float e = y[2 * hh + q] - Tg[(r0 + r) * 3 + c];
+        lsum += e * e;
+        d = 2.f * e * inv_norm;
+      }
+      if (c < 4) dy[r * 4 + c] = d;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+  if (lane == 0) lw[warp] = lsum;
+  __syncthreads();
+  float* G = gpart + (long long)blockIdx.x * N_PARAMS;
+  // dW3[i][c] = sum_r H2[r][i] dY[r][c];  db3[c] = sum_r dY[r][c]
+  for (int e = threadIdx.x; e < H * N3; e += blockDim.x) {
+    const int i = e / N3, c = e % N3;
+    float s = 0.f;
+    if (c < D_OUT)
+      for (int r = 0; r < TB; ++r) s += __bfloat162float(h2[r * KP2 + i]) * dy[r * 4 + c];
+    G[OFF_W3 + e] = s;
+  }
+  for (int c = threadIdx.x; c < N3; c += blockDim.x) {
+    float s = 0.f;
+    if (c < D_OUT)
+      for (int r = 0; r < TB; ++r) s += dy[r * 4 + c];
+    G[OFF_B3 + c] = s;
+  }
+  __syncthreads();
+  // dZ2 = (dY W3^T) * silu'(Z2)  (fp32, in z2) and as bf16 rows in h2 (A operand of dH1)
+  for (int e = threadIdx.x; e < TB * H; e += blockDim.x) {
+    const int r = e / H, i = e % H;
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < D_OUT; ++c) s += dy[r * 4 + c] * __bfloat162float(W3n[i * N3 + c]);
+    const float d = s * dsilu(z2[r * H + i]);
+    z2[r * H + i] = d;
+  }
+  __syncthreads();
+  // dW2[i][o] = sum_r H1[r][i] dZ2[r][o];  db2[o] = sum_r dZ2[r][o]
+  for (int e = threadIdx.x; e < H * H; e += blockDim.x) {
+    const int i = e / H, o = e % H;
+    float s = 0.f;
+    for (int r = 0; r < TB; ++r) s += __bfloat162float(h1[r * KP2 + i]) * z2[r * H + o];
+    G[OFF_W2 + e] = s;
+  }
+  for (int o = threadIdx.x; o < H; o += blockDim.x) {
+    float s = 0.f;
+    for (int r = 0; r < TB; ++r) s += z2[r * H + o];
+    G[OFF_B2 + o] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < TB * H; e += blockDim.x) {
+    const int r = e / H, i = e % H;
+    h2[r * KP2 + i] = __float2bfloat16_rn(z2[r * H + i]);
+  }
+  __syncthreads();
+  // dH1 = dZ2 W2^T on the tensor cores (B^T[n=i][k=o] = W2[i][o] = W2n), then dZ1 = dH1 * silu'(Z1)
+  {
+    float acc[16][4];
+    warp_gemm<16, H>(acc, h2 + rw * KP2, KP2, W2n, KP2, lane);
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) {
+      const int c = nt * 8 + 2 * t;
+      const int ra = rw + g, rb = rw + g + 8;
+      z1[ra * H + c] = acc[nt][0] * dsilu(z1[ra * H + c]);
+      z1[ra * H + c + 1] = acc[nt][1] * dsilu(z1[ra * H + c + 1]);
+      z1[rb * H + c] = acc[nt][2] * dsilu(z1[rb * H + c]);
+      z1[rb * H + c + 1] = acc[nt][3] * dsilu(z1[rb * H + c + 1]);
+    }
+  }
+  __syncthreads();
+  // dW1[k][o] = sum_r X[r][k] dZ1[r][o];  db1[o] = sum_r dZ1[r][o]
+  for (int e = threadIdx.x; e < K1 * H; e += blockDim.x) {
+    const int k = e / H, o = e % H;
+    float s = 0.f;
+    if (k < D_IN)
+      for (int r = 0; r < TB; ++r) s += __bfloat162float(X[r * XP + k]) * z1[r * H + o];
+    G[OFF_W1 + e] = s;
+  }
+  for (int o = threadIdx.x; o < H; o += blockDim.x) {
+    float s = 0.f;
+    for (int r = 0; r < TB; ++r) s += z1[r * H + o];
+    G[OFF_B1 + o] = s;
+  }
+  if (threadIdx.x == 0) {
+    float l = 0.f;
+    for (int q = 0; q < TWARPS; ++q) l += lw[q];
+    lpart[blockIdx.x] = l;
+  }
+}
+
+// Fixed-order sum of the per-CTA partials: grad[e] = sum_b gpart[b][e]; loss = sum_b lpart[b] / norm.
+__global__ void k_mlp_reduce(const float* __restrict__ gpart, const float* __restrict__ lpart, int nblk,
+                             float* __restrict__ grad, float* __restrict__ loss, float inv_norm) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int b = 0; b < nblk; ++b) s += gpart[(long long)b * N_PARAMS + e];
+    grad[e] = s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    float l = 0.f;
+    for (int b = 0; b < nblk; ++b) l += lpart[b];
+    *loss = l * inv_norm;
+  }
+}
+
+// Adam on the FP32 master weights; padded rows/columns stay zero.
+__global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                           float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x) {
+    bool pad = false;
+    if (e < OFF_B1) pad = (e - OFF_W1) / H >= D_IN;
+    else if (e >= OFF_W3 && e < OFF_B3) pad = (e - OFF_W3) % N3 >= D_OUT;
+    else if (e >= OFF_B3) pad = (e - OFF_B3) >= D_OUT;
+    if (pad) { p[e] = 0.f; continue; }
+    const float gg = g[e];
+    const float mm = b1 * m[e] + (1.f - b1) * gg;
+    const float vv = b2 * v[e] + (1.f - b2) * gg * gg;
+    m[e] = mm;
+    v[e] = vv;
+    p[e] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  }
+}
+
+// planar (3, M) -> interleaved (M, 4) with a zero fourth component
+template <typename T>
+__global__ void k_interleave3(const T* __restrict__ in, vec4<T>* __restrict__ out, long long m) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    out[i] = mk4<T>(in[i], in[m + i], in[2 * m + i], T(0));
+}
+
+inline int gridn(long long n, int th) {
+  long long b = (n + th - 1) / th;
+  if (b > 148LL * 16) b = 148LL * 16;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ld_mlp_sizes(int64_t* n_params, int64_t* n_packed, int32_t* k_in, int32_t* batch_tile) {
+  if (n_params) *n_params = N_PARAMS;
+  if (n_packed) *n_packed = N_PACKED;
+  if (k_in) *k_in = K1;
+  if (batch_tile) *batch_tile = TB;
+  return LD_OK;
+}
+
+int ld_mlp_pack(const float* params, void* packed, void* stream) {
+  if (!params || !packed) return ld_fail(LD_ERR_ARG, "ld_mlp_pack: bad arguments");
+  k_mlp_pack<<<gridn(N_PACKED, 256), 256, 0, (cudaStream_t)stream>>>(params, (bf16*)packed);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const void* packed, const float* params,
+                 void* out, void* stream) {
+  if (!p || !u4 || !packed || !params || n < 0 || (n > 0 && (!pos || !out)))
+    return ld_fail(LD_ERR_ARG, "ld_mlp_infer: bad arguments");
+  if (n == 0) return LD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  ProfScope ps(p, KID_MLP_INFER, s);
+  const double L = 2.0 * M_PI;
+  long long tiles = (n + 15) / 16;
+  long long grid = (tiles + WARPS - 1) / WARPS;
+  if (grid > 148 * 2) grid = 148 * 2;
+  static_assert(SMEM_INFER <= 227 * 1024, "inference tile exceeds shared memory");
+  if (p->prec == LD_F32) {
+    auto k = k_mlp_infer<float>;
+    LD_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_INFER));
+    k<<<(unsigned)grid, WARPS * 32, SMEM_INFER, s>>>((const float4*)u4, p->N, L, pos, n, (const bf16*)packed,
+                                                       params, (float*)out);
+  } else {
+    auto k = k_mlp_infer<double>;
+    LD_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_INFER));
+    k<<<(unsigned)grid, WARPS * 32, SMEM_INFER, s>>>((const double4*)u4, p->N, L, pos, n, (const bf16*)packed,
+                                                       params, (double*)out);
+  }
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_phase_shift(ld_plan* p, const void* uk, void* out, double sx, double sy, double sz, void* stream) {
+  if (!p || !uk || !out) return ld_fail(LD_ERR_ARG, "ld_phase_shift: bad arguments");
+  const double dx = 2.0 * M_PI / p->N;
+  const long long cs = p->cube_elems();
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->prec == LD_F32)
+    k_phase_shift<float><<<gridn(3 * cs, 256), 256, 0, s>>>((const float2*)uk, (float2*)out, cs, p->kc, p->My,
+                                                             p->Mzp, sx * dx, sy * dx, sz * dx);
+  else
+    k_phase_shift<double><<<gridn(3 * cs, 256), 256, 0, s>>>((const double2*)uk, (double2*)out, cs, p->kc, p->My,
+                                                              p->Mzp, sx * dx, sy * dx, sz * dx);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_mlp_samples(ld_plan* p, const void* u4, const void* ue, const int64_t* idx, int64_t ns, double sx, double sy,
+                   double sz, void* X, float* T, float* aux, void* stream) {
+  if (!p || !u4 || !ue || ns < 0 || (ns > 0 && (!idx || !X || !T || !aux)))
+    return ld_fail(LD_ERR_ARG, "ld_mlp_samples: bad arguments");
+  if (ns == 0) return LD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const double L = 2.0 * M_PI;
+  if (p->prec == LD_F32)
+    k_mlp_samples<float><<<gridn(ns, 128), 128, 0, s>>>((const float4*)u4, (const float*)ue, p->N, L,
+                                                        (const long long*)idx, ns, sx, sy, sz, (bf16*)X, T, aux);
+  else
+    k_mlp_samples<double><<<gridn(ns, 128), 128, 0, s>>>((const double4*)u4, (const double*)ue, p->N, L,
+                                                         (const long long*)idx, ns, sx, sy, sz, (bf16*)X, T, aux);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_interleave3(ld_plan* p, const void* planar, void* out, void* stream) {
+  if (!p || !planar || !out) return ld_fail(LD_ERR_ARG, "ld_interleave3: bad arguments");
+  const long long m = (long long)p->N * p->N * p->N;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->prec == LD_F32) k_interleave3<float><<<gridn(m, 256), 256, 0, s>>>((const float*)planar, (float4*)out, m);
+  else k_interleave3<double><<<gridn(m, 256), 256, 0, s>>>((const double*)planar, (double4*)out, m);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_gather4(ld_plan* p, const void* u4, const double* pos, int64_t n, int method, void* out, void* stream) {
+  if (!p || !u4 || n < 0 || method < 0 || method > 2 || (n > 0 && (!pos || !out)))
+    return ld_fail(LD_ERR_ARG, "ld_gather4: bad arguments");
+  if (n == 0) return LD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const double L = 2.0 * M_PI;
+  const int g = gridn(n, 256);
+#define LD_G4(TT, V4, M) k_gather4<TT, M><<<g, 256, 0, s>>>((const V4*)u4, p->N, L, pos, n, (TT*)out)
+  if (p->prec == LD_F32) {
+    if (method == LD_INTERP_TRILINEAR) LD_G4(float, float4, LD_INTERP_TRILINEAR);
+    else if (method == LD_INTERP_TRICUBIC) LD_G4(float, float4, LD_INTERP_TRICUBIC);
+    else LD_G4(float, float4, LD_INTERP_COSINE);
+  } else {
+    if (method == LD_INTERP_TRILINEAR) LD_G4(double, double4, LD_INTERP_TRILINEAR);
+    else if (method == LD_INTERP_TRICUBIC) LD_G4(double, double4, LD_INTERP_TRICUBIC);
+    else LD_G4(double, double4, LD_INTERP_COSINE);
+  }
+#undef LD_G4
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int64_t ld_mlp_partial_floats(int64_t nb) { return ((nb + TB - 1) / TB) * (int64_t)(N_PARAMS + 1); }
+
+int ld_mlp_grad(const void* X, const float* T, int64_t nb, const float* params, const void* packed, float* work,
+                float* grad, float* loss, void* stream) {
+  if (!X || !T || nb < 1 || !params || !packed || !work || !grad || !loss)
+    return ld_fail(LD_ERR_ARG, "ld_mlp_grad: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nblk = (int)((nb + TB - 1) / TB);
+  float* gpart = work;
+  float* lpart = work + (long long)nblk * N_PARAMS;
+  const float inv_norm = 1.f / (float)nb;
+  LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN));
+  k_mlp_train<<<nblk, TWARPS * 32, SMEM_TRAIN, s>>>((const bf16*)X, T, nb, inv_norm, (const bf16*)packed, params,
+                                                    gpart, lpart);
+  k_mlp_reduce<<<gridn(N_PARAMS, 256), 256, 0, s>>>(gpart, lpart, nblk, grad, loss, inv_norm);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t step, float lr, void* packed,
+                void* stream) {
+  if (!params || !grad || !m || !v || step < 1 || !packed) return ld_fail(LD_ERR_ARG, "ld_mlp_adam: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_mlp_adam<<<gridn(N_PARAMS, 256), 256, 0, s>>>(params, grad, m, v, lr, b1, b2, 1e-8f, c1, c2);
+  k_mlp_pack<<<gridn(N_PACKED, 256), 256, 0, s>>>(params, (bf16*)packed);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+}  // extern "C"

@@ -174,6 +174,31 @@ template <typename T, int N> struct Ops {
     return LD_OK;
   }
 
+  // ---- pipelined fused z pass (one warp per row) -------------------------------------------------
+  static int zcross_pipe(ld_plan* p, const C* W2, C* W1, T* uout, int ulayout, T sc, cudaStream_t s) {
+    constexpr int WARPS = sizeof(T) == 4 ? 8 : 4;
+    const long long NN = (long long)N * N;
+    const size_t smem = (size_t)WARPS * ((size_t)12 * p->Mzp + Cfg<N>::ZBUF) * sizeof(C) + 16 * WARPS;
+    auto k = k_z_cross_pipe<T, N>;
+    if (int rc = set_smem(k, smem)) return rc;
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+      int b = 0;
+      cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, WARPS * 32, smem);
+      if (e != cudaSuccess) { ld_set_last_error(e); return LD_ERR_CUDA; }
+      blocks_per_sm = b > 0 ? b : 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long grid = (long long)sms * blocks_per_sm;
+    const long long need = (NN + WARPS - 1) / WARPS;
+    if (grid > need) grid = need;
+    k<<<(unsigned)grid, WARPS * 32, smem, s>>>(W2, W1, uout, ulayout, p->Mzp, p->kc, sc, (const C*)p->tw, p->status);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
+  }
+
   // ---- RHS pipeline: y (stage input) -> update epilogue ------------------------------------------
   template <int MODE>
   static int rhs(ld_plan* p, C* s0, C* s1, C* s2, T* uout, const ld_flow_params* prm, double visc,
@@ -198,11 +223,16 @@ template <typename T, int N> struct Ops {
     // fused z pass: u, w -> u x w  (W2 -> W1 as (3, N*N, Mzp))
     {
       ProfScope ps(p, KID_ZCROSS, s);
-      auto k = k_z_cross<T, N>;
-      if (int rc = set_smem(k, Z_SMEM)) return rc;
       const T sc = T(1.0 / (double(N) * N * N));
-      k<<<(unsigned)(NN / Cfg<N>::ZROWS), Cfg<N>::ZTHREADS, Z_SMEM, s>>>(W2, W1, uout, Mzp, kc, sc, tw);
-      LD_LAUNCH_CHECK();
+      const int ulayout = (MODE == UPD_RHS) ? 0 : 1;  // the time steppers feed droplets: interleaved
+      if constexpr (Cfg<N>::NTZ == 32) {
+        if (int rc = zcross_pipe(p, W2, W1, uout, ulayout, sc, s)) return rc;
+      } else {
+        auto k = k_z_cross<T, N>;
+        if (int rc = set_smem(k, Z_SMEM)) return rc;
+        k<<<(unsigned)(NN / Cfg<N>::ZROWS), Cfg<N>::ZTHREADS, Z_SMEM, s>>>(W2, W1, uout, ulayout, Mzp, kc, sc, tw);
+        LD_LAUNCH_CHECK();
+      }
     }
     // forward y pass (W1 -> W2 as (3, N, My, Mzp))
     auto fyin = io(W1, w2s, (long long)N * Mzp, Mzp, -1);
@@ -244,8 +274,9 @@ template <typename T, int N> struct Ops {
     const int th = 256;
     const int gr = grid1d(n, th);
     const double L = 2.0 * M_PI;
-    if (stage == 1) k_droplet_stage<T, M, 1><<<gr, th, 0, s>>>(u, N, L, pos, vel, tau, a1, n, h, T(g));
-    else k_droplet_stage<T, M, 2><<<gr, th, 0, s>>>(u, N, L, pos, vel, tau, a1, n, h, T(g));
+    const vec4<T>* u4 = reinterpret_cast<const vec4<T>*>(u);
+    if (stage == 1) k_droplet_stage<T, M, 1><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g));
+    else k_droplet_stage<T, M, 2><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g));
     LD_LAUNCH_CHECK();
     return LD_OK;
   }

@@ -47,6 +47,8 @@ class ForcedDNS:
         self.acc = p.empty_cube(3)
         self.u_phys = None
         self.droplets = None
+        self.collider = None
+        self.sort_every = 0
         self.t = 0.0
         self.nstep = 0
 
@@ -97,11 +99,32 @@ class ForcedDNS:
         """Shell spectrum ek_arr of F:423, F:431 (FP64 numpy)."""
         return self.plan.e3d_to_e1d(self.uk).cpu().numpy()
 
-    def attach(self, droplets):
-        """Advance ``droplets`` with the flow; allocates the physical-velocity buffer."""
+    def attach(self, droplets, collider=None, sort_every=0, pair_capacity=None):
+        """Advance ``droplets`` with the flow.
+
+        Allocates the interleaved (N, N, N, 4) physical-velocity buffer the droplet stages read.
+        With a ``collider`` the colliding pairs are found after every step (``self.pairs`` /
+        ``collider.count`` on the device); with ``sort_every`` > 0 the droplets are re-sorted into
+        cell order every that many steps, which keeps their stencil loads local in memory."""
+        torch = _torch()
         self.droplets = droplets
         if self.u_phys is None:
-            self.u_phys = self.plan.empty_phys(3)
+            p = self.plan
+            self.u_phys = torch.empty((p.N, p.N, p.N, 4), dtype=p.rdtype, device=p.device)
+        self.collider = collider
+        self.sort_every = int(sort_every)
+        if collider is not None:
+            check(_lib.lib().ld_collider_trace(collider._h, self.plan.handle))
+        if collider is not None:
+            cap = pair_capacity or max(1024, 4 * droplets.n)
+            self.pairs = torch.empty((cap, 2), dtype=torch.int32, device=self.plan.device)
+        if self.sort_every > 0:
+            self._sorter = collider
+            if self._sorter is None:
+                from .collide import Collider
+                self._sorter = Collider(droplets.n, 4 * self.plan.dx, device=self.plan.device)
+                check(_lib.lib().ld_collider_trace(self._sorter._h, self.plan.handle))
+            droplets.sort(self._sorter)
         return self
 
     # ---- stepping ---------------------------------------------------------------------------------
@@ -127,6 +150,10 @@ class ForcedDNS:
                 check(L.ld_step_epilogue(h, ptr(self.uk), st))
             self.t += self.dt
             self.nstep += 1
+            if d is not None and self.sort_every > 0 and self.nstep % self.sort_every == 0:
+                d.sort(self._sorter, stream)
+            if d is not None and self.collider is not None:
+                d.collide(self.collider, self.pairs, stream)
 
     def step_host(self, uk_host, pos_host=None, vel_host=None, nsteps=1, stream=None):
         """Drop-in for one call of the reference's time-loop body with host state (F:582-610):
@@ -158,9 +185,12 @@ class ForcedDNS:
 
 
 class Droplets:
-    """One-way-coupled inertial droplets: pos (n,3) FP64, vel (n,3), tau (n) on the device."""
+    """One-way-coupled inertial droplets: pos (n,3) FP64, vel (n,3), tau (n) on the device.
 
-    def __init__(self, plan, pos, vel, tau, method="tricubic", g=0.0):
+    ``ids`` (int64) follows every droplet through re-sorting, like the reference's prtclid
+    (particles.py:92-93); ``radius`` (FP64, optional) is used by the collision search."""
+
+    def __init__(self, plan, pos, vel, tau, method="tricubic", g=0.0, radius=None, ids=None):
         torch = _torch()
         self.plan = plan
         dev = plan.device
@@ -169,6 +199,11 @@ class Droplets:
         self.tau = torch.as_tensor(tau).to(device=dev, dtype=plan.rdtype).contiguous()
         self.a1 = torch.zeros_like(self.vel)
         self.n = int(self.pos.shape[0])
+        self.ids = (torch.arange(self.n, dtype=torch.int64, device=dev) if ids is None
+                    else torch.as_tensor(ids).to(device=dev, dtype=torch.int64).contiguous())
+        self.radius = (None if radius is None
+                       else torch.as_tensor(radius).to(device=dev, dtype=torch.float64).contiguous())
+        self._order = torch.empty(self.n, dtype=torch.int32, device=dev)
         if self.pos.shape != (self.n, 3) or self.vel.shape != (self.n, 3) or self.tau.shape != (self.n,):
             raise ValueError("pos (n,3), vel (n,3), tau (n,) expected")
         self.method = method
@@ -185,6 +220,36 @@ class Droplets:
         check(_lib.lib().ld_gather(self.plan.handle, ptr(field), C, ptr(pos), int(pos.shape[0]), self.m,
                                    ptr(out), stream_ptr(stream)))
         return out
+
+    def arrays(self):
+        """Every per-droplet array, in the order they are permuted together."""
+        out = [("pos", self.pos), ("vel", self.vel), ("tau", self.tau), ("a1", self.a1), ("ids", self.ids)]
+        if self.radius is not None:
+            out.append(("radius", self.radius))
+        return out
+
+    def sort(self, collider, stream=None):
+        """Re-order every per-droplet array into the collider's cell order."""
+        L = _lib.lib()
+        st = stream_ptr(stream)
+        check(L.ld_cell_order(collider._h, ptr(self.pos), self.n, collider.L, ptr(self._order), st))
+        for name, t in self.arrays():
+            tmp = _torch().empty_like(t)
+            row = t.element_size() * (t.shape[1] if t.dim() > 1 else 1)
+            check(L.ld_permute_rows(ptr(t), ptr(tmp), ptr(self._order), self.n, row, st))
+            setattr(self, name, tmp)
+
+    def collide(self, collider, pairs, stream=None):
+        """Colliding pairs (array indices, i < j) into ``pairs``; the count stays on the device."""
+        if self.radius is None:
+            raise ValueError("droplet radii are needed for the collision search")
+        check(_lib.lib().ld_collide(collider._h, ptr(self.pos), ptr(self.radius), self.n, collider.L, ptr(pairs),
+                                    int(pairs.shape[0]), ptr(collider.count), stream_ptr(stream)))
+
+    def by_id(self, t):
+        """Rows of a per-droplet tensor in droplet-id order (host numpy)."""
+        order = _torch().argsort(self.ids)
+        return t[order].cpu().numpy()
 
     def stage(self, s, u_phys, h, stream=None):
         check(_lib.lib().ld_droplet_stage(self.plan.handle, int(s), ptr(u_phys), ptr(self.pos), ptr(self.vel),

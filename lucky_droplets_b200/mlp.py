@@ -1,0 +1,219 @@
+"""Learned interpolation of the fluid velocity at droplets (no counterpart in the reference).
+
+``LearnedInterp`` owns the MLP parameters (FP32) and their packed BF16 copy on the device and
+drives the kernels of csrc/ld_mlp.cu:
+
+* ``make_samples``: training pairs from a DNS state.  For a random sub-grid shift s, the spectrum
+  is phase-shifted by exp(i k.s dx) and inverse-transformed: the result at grid point j is the
+  exact spectral velocity at x_j + s dx.  Random grid points j of that field give exact targets at
+  uniformly distributed points; features come from the unshifted grid.
+* ``train``: Adam on mini-batches with the project's forward/backward kernels.
+* ``infer``: fused stencil gather + tricubic + MLP correction at droplet positions.
+* ``judge``: relative L2 error against the exact direct Fourier sum (``Plan.exact_sum``) on a
+  sample of droplets, with tricubic as the comparison; ``enabled`` turns off when the learned
+  error exceeds the tolerance or loses to tricubic.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, ptr, stream_ptr
+
+TWO_PI = 2.0 * np.pi
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def sizes():
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    k, t = ctypes.c_int32(), ctypes.c_int32()
+    check(_lib.lib().ld_mlp_sizes(ctypes.byref(a), ctypes.byref(b), ctypes.byref(k), ctypes.byref(t)))
+    return a.value, b.value, k.value, t.value
+
+
+D_IN, H, D_OUT, K1, N3 = 195, 128, 3, 208, 8
+OFF_W1 = 0
+OFF_B1 = OFF_W1 + K1 * H
+OFF_W2 = OFF_B1 + H
+OFF_B2 = OFF_W2 + H * H
+OFF_W3 = OFF_B2 + H
+OFF_B3 = OFF_W3 + H * N3
+N_PARAMS = OFF_B3 + N3
+
+
+def flat_from_mats(W1, b1, W2, b2, W3, b3):
+    """(195,128),(128),(128,128),(128),(128,3),(3) -> the flat padded parameter vector."""
+    p = np.zeros(N_PARAMS, np.float32)
+    p[OFF_W1:OFF_B1].reshape(K1, H)[:D_IN] = W1
+    p[OFF_B1:OFF_W2] = b1
+    p[OFF_W2:OFF_B2] = np.asarray(W2).reshape(-1)
+    p[OFF_B2:OFF_W3] = b2
+    p[OFF_W3:OFF_B3].reshape(H, N3)[:, :D_OUT] = W3
+    p[OFF_B3:OFF_B3 + D_OUT] = b3
+    return p
+
+
+def mats_from_flat(p):
+    p = np.asarray(p, np.float32)
+    return dict(W1=p[OFF_W1:OFF_B1].reshape(K1, H)[:D_IN].copy(), b1=p[OFF_B1:OFF_W2].copy(),
+                W2=p[OFF_W2:OFF_B2].reshape(H, H).copy(), b2=p[OFF_B2:OFF_W3].copy(),
+                W3=p[OFF_W3:OFF_B3].reshape(H, N3)[:, :D_OUT].copy(), b3=p[OFF_B3:OFF_B3 + D_OUT].copy())
+
+
+def init_flat(seed=0):
+    """He-uniform initial weights, zero biases, a small last layer."""
+    rng = np.random.default_rng(seed)
+
+    def lin(i, o):
+        lim = np.sqrt(6.0 / i)
+        return rng.uniform(-lim, lim, (i, o)).astype(np.float32), np.zeros(o, np.float32)
+
+    W1, b1 = lin(D_IN, H)
+    W2, b2 = lin(H, H)
+    W3, b3 = lin(H, D_OUT)
+    return flat_from_mats(W1, b1, W2, b2, 0.1 * W3, b3)
+
+
+class LearnedInterp:
+    """MLP parameters, optimiser state and packed weights on one device."""
+
+    def __init__(self, plan, seed=0, params=None, tol=1e-4):
+        torch = _torch()
+        n_params, n_packed, k_in, tile = sizes()
+        assert n_params == N_PARAMS and k_in == K1
+        self.plan = plan
+        dev = plan.device
+        flat = init_flat(seed) if params is None else np.asarray(params, np.float32)
+        self.params = torch.as_tensor(flat).to(dev).contiguous()
+        self.packed = torch.empty(n_packed, dtype=torch.bfloat16, device=dev)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grad = torch.zeros_like(self.params)
+        self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.step_count = 0
+        self.tol = tol
+        self.enabled = True
+        self.history = []
+        check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
+
+    def set_params(self, flat):
+        self.params.copy_(_torch().as_tensor(np.asarray(flat, np.float32)))
+        check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
+
+    # ---- inference ------------------------------------------------------------------------------
+    def infer(self, u4, pos, out=None, stream=None):
+        torch = _torch()
+        n = int(pos.shape[0])
+        if out is None:
+            out = torch.empty((n, 3), dtype=self.plan.rdtype, device=self.plan.device)
+        check(_lib.lib().ld_mlp_infer(self.plan.handle, ptr(u4), ptr(pos), n, ptr(self.packed), ptr(self.params),
+                                      ptr(out), stream_ptr(stream)))
+        return out
+
+    # ---- data -------------------------------------------------------------------------------------
+    def interleaved(self, uk):
+        """Interleaved (N,N,N,4) physical velocity of a cube-layout spectrum."""
+        torch = _torch()
+        p = self.plan
+        u = p.irfft_cube(uk)
+        u4 = torch.empty((p.N, p.N, p.N, 4), dtype=p.rdtype, device=p.device)
+        check(_lib.lib().ld_interleave3(p.handle, ptr(u), ptr(u4), stream_ptr()))
+        return u4
+
+    def make_samples(self, uk, n_shifts, per_shift, seed=0, X=None, T=None, offset=0):
+        """Training pairs from a cube-layout spectrum: n_shifts random sub-grid shifts, per_shift
+        random grid points each.  Returns (X bf16 (ns, 208), T (ns,3), aux (ns,4))."""
+        torch = _torch()
+        p = self.plan
+        ns = n_shifts * per_shift
+        rng = np.random.default_rng(seed)
+        if X is None:
+            X = torch.empty((ns, K1), dtype=torch.bfloat16, device=p.device)
+            T = torch.empty((ns, 3), dtype=torch.float32, device=p.device)
+            offset = 0
+        aux = torch.empty((ns, 4), dtype=torch.float32, device=p.device)
+        u4 = self.interleaved(uk)
+        shifted = p.empty_cube(3)
+        L = _lib.lib()
+        for i in range(n_shifts):
+            s = rng.uniform(0.0, 1.0, 3)
+            check(L.ld_phase_shift(p.handle, ptr(uk), ptr(shifted), float(s[0]), float(s[1]), float(s[2]),
+                                   stream_ptr()))
+            ue = p.irfft_cube(shifted)
+            idx = torch.as_tensor(rng.integers(0, p.N ** 3, per_shift, dtype=np.int64)).to(p.device)
+            a = offset + i * per_shift
+            check(L.ld_mlp_samples(p.handle, ptr(u4), ptr(ue), ptr(idx), per_shift, float(s[0]), float(s[1]),
+                                   float(s[2]), ptr(X[a:a + per_shift]), ptr(T[a:a + per_shift]),
+                                   ptr(aux[i * per_shift:(i + 1) * per_shift]), stream_ptr()))
+        return X, T, aux
+
+    # ---- training ---------------------------------------------------------------------------------
+    def loss_and_grad(self, X, T, work=None):
+        """Exact batch loss and gradient (device tensors); deterministic."""
+        torch = _torch()
+        nb = int(X.shape[0])
+        L = _lib.lib()
+        if work is None:
+            work = torch.empty(int(L.ld_mlp_partial_floats(nb)), dtype=torch.float32, device=self.plan.device)
+        check(L.ld_mlp_grad(ptr(X), ptr(T), nb, ptr(self.params), ptr(self.packed), ptr(work), ptr(self.grad),
+                            ptr(self.loss), stream_ptr()))
+        return self.loss, self.grad
+
+    def train(self, X, T, epochs=1, batch=4096, lr=1e-3, lr_final=None, seed=0, log_every=0):
+        """Adam over shuffled mini-batches; returns the per-epoch mean loss (host floats)."""
+        torch = _torch()
+        n = int(X.shape[0])
+        L = _lib.lib()
+        work = torch.empty(int(L.ld_mlp_partial_floats(batch)), dtype=torch.float32, device=self.plan.device)
+        xb = torch.empty((batch, K1), dtype=torch.bfloat16, device=self.plan.device)
+        tb = torch.empty((batch, 3), dtype=torch.float32, device=self.plan.device)
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        nbatch = max(1, n // batch)
+        total = epochs * nbatch
+        out = []
+        for ep in range(epochs):
+            perm = torch.randperm(n, generator=g).to(torch.int32).to(self.plan.device)
+            acc = torch.zeros(1, dtype=torch.float32, device=self.plan.device)
+            for b in range(nbatch):
+                idx = perm[b * batch:(b + 1) * batch]
+                check(L.ld_permute_rows(ptr(X), ptr(xb), ptr(idx), batch, K1 * 2, stream_ptr()))
+                check(L.ld_permute_rows(ptr(T), ptr(tb), ptr(idx), batch, 12, stream_ptr()))
+                self.loss_and_grad(xb, tb, work)
+                acc += self.loss
+                self.step_count += 1
+                k = self.step_count
+                lr_k = lr if lr_final is None else lr * (lr_final / lr) ** (min(k, total) / total)
+                check(L.ld_mlp_adam(ptr(self.params), ptr(self.grad), ptr(self.m), ptr(self.v), k, float(lr_k),
+                                    ptr(self.packed), stream_ptr()))
+            out.append(float(acc.item()) / nbatch)
+            if log_every and (ep + 1) % log_every == 0:
+                print(f"epoch {ep + 1}: loss {out[-1]:.4e}")
+        return out
+
+    # ---- judge ------------------------------------------------------------------------------------
+    def judge(self, uk, u4, pos, n_sample=None, seed=0):
+        """Relative L2 errors (learned, tricubic) against the exact Fourier sum on a sample of
+        positions; disables the network when it misses the tolerance and loses to tricubic."""
+        torch = _torch()
+        p = self.plan
+        n = int(pos.shape[0])
+        if n_sample is not None and n_sample < n:
+            g = torch.Generator(device="cpu").manual_seed(seed)
+            sel = torch.randperm(n, generator=g)[:n_sample].to(p.device)
+            pos = pos[sel].contiguous()
+        exact = p.exact_sum(uk, pos)
+        learned = self.infer(u4, pos).to(torch.float64)
+        tric = torch.empty((pos.shape[0], 3), dtype=p.rdtype, device=p.device)
+        check(_lib.lib().ld_gather4(p.handle, ptr(u4), ptr(pos), int(pos.shape[0]), _lib.LD_INTERP["tricubic"],
+                                    ptr(tric), stream_ptr()))
+        den = torch.linalg.norm(exact)
+        e_l = float(torch.linalg.norm(learned - exact) / den)
+        e_t = float(torch.linalg.norm(tric.to(torch.float64) - exact) / den)
+        self.enabled = (e_l <= self.tol) or (e_l < e_t)
+        self.history.append((e_l, e_t, self.enabled))
+        return e_l, e_t
+

@@ -164,6 +164,16 @@ class Plan:
                                          stream_ptr(stream)))
         return ku
 
+    def exact_sum(self, uk, pos, out=None, stream=None):
+        """Direct Fourier-sum velocity (FP64) of a cube-layout 3-vector at pos (n, 3) double."""
+        torch = _torch()
+        self._chk(uk, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        n = int(pos.shape[0])
+        if out is None:
+            out = torch.empty((n, 3), dtype=torch.float64, device=self.device)
+        check(_lib.lib().ld_exact_sum(self._h, ptr(uk), ptr(pos), n, ptr(out), stream_ptr(stream)))
+        return out
+
     def profile(self, enable=True):
         """Start/stop bracketing every kernel launch of this plan with CUDA events."""
         check(_lib.lib().ld_profile(self._h, int(bool(enable))))

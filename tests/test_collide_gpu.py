@@ -1,0 +1,137 @@
+"""Cell-list collision detection on the GPU against the bit-exact FP64 CPU rule
+(oracle/collide_np.py), and the project's radix sort against a stable argsort.  Also checks that
+two calls on the same input give the identical pair list (deterministic order)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import collide_np as K
+
+pytestmark = pytest.mark.gpu
+TWO_PI = 2 * np.pi
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def gpu_pairs(torch, pos, rad, cell, cap=200000):
+    from lucky_droplets_b200.collide import Collider
+    c = Collider(max(1, pos.shape[0]), cell)
+    p = torch.as_tensor(pos).cuda().contiguous()
+    r = torch.as_tensor(rad).cuda().contiguous()
+    out = c.collide(p, r, cap=cap).cpu().numpy().astype(np.int64)
+    # the device order is deterministic (by cell); compare as a canonical (i, j)-sorted list
+    assert (out[:, 0] < out[:, 1]).all() if len(out) else True
+    out = out[np.lexsort((out[:, 1], out[:, 0]))] if len(out) else out
+    return out, c
+
+
+@pytest.mark.parametrize("n,scale,seed", [(20000, 1.0, 0), (50000, 0.5, 1), (5000, 3.0, 2)])
+def test_pairs_bit_exact(torch, n, scale, seed):
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(-2.0, TWO_PI + 2.0, (n, 3))  # unwrapped positions, as the reference keeps them
+    rad = 0.01 * scale * np.exp(0.3 * rng.standard_normal(n))
+    cell = 2 * rad.max()
+    got, _ = gpu_pairs(torch, pos, rad, cell)
+    ref = K.collide(pos, rad, cell)
+    assert got.shape == ref.shape and np.array_equal(got, ref)
+
+
+def test_edge_cases(torch):
+    rng = np.random.default_rng(5)
+    # empty and single droplet
+    got, _ = gpu_pairs(torch, np.zeros((0, 3)), np.zeros(0), 0.1)
+    assert got.shape == (0, 2)
+    got, _ = gpu_pairs(torch, np.ones((1, 3)), np.ones(1) * 0.1, 0.2)
+    assert got.shape == (0, 2)
+    # everything in one cell, and fewer than three cells per side (neighbour cells repeat)
+    pos = rng.uniform(0, 0.3, (400, 3))
+    rad = np.full(400, 0.05)
+    for cell in (2.5, 4.0, 10.0):
+        got, _ = gpu_pairs(torch, pos, rad, cell)
+        ref = K.collide_bruteforce(pos, rad)
+        assert np.array_equal(got, ref)
+    # periodic images across the box faces
+    pos = np.array([[0.001, 3.0, 3.0], [TWO_PI - 0.001, 3.0, 3.0], [3.0, 3.0, TWO_PI - 1e-4], [3.0, 3.0, 1e-4]])
+    rad = np.full(4, 0.01)
+    got, _ = gpu_pairs(torch, pos, rad, 0.5)
+    assert np.array_equal(got, K.collide_bruteforce(pos, rad))
+
+
+def test_capacity_overflow_reported(torch):
+    from lucky_droplets_b200 import _lib
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(0, 0.5, (300, 3))
+    rad = np.full(300, 0.05)
+    ref = K.collide(pos, rad, 0.2)
+    c = Collider(300, 0.2)
+    with pytest.raises(RuntimeError, match="capacity"):
+        c.collide(torch.as_tensor(pos).cuda(), torch.as_tensor(rad).cuda(), cap=len(ref) // 2)
+    assert c.status() & _lib.STATUS_PAIR_OVERFLOW
+    assert int(c.count.item()) == len(ref)
+
+
+@pytest.mark.parametrize("n,bits", [(1, 8), (4095, 12), (100000, 18), (300001, 24)])
+def test_radix_sort_stable(torch, n, bits):
+    from lucky_droplets_b200 import _lib
+    from lucky_droplets_b200._lib import check, ptr, stream_ptr
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 1 << bits, n, dtype=np.uint32)
+    keys[: n // 3] = keys[0]  # many equal keys: stability matters
+    vals = np.arange(n, dtype=np.uint32)
+    c = Collider(n, 1.0)
+    k = torch.as_tensor(keys.astype(np.int64)).to(torch.int32).cuda().contiguous()
+    v = torch.as_tensor(vals.astype(np.int64)).to(torch.int32).cuda().contiguous()
+    check(_lib.lib().ld_radix_sort_u32(c._h, ptr(k), ptr(v), n, bits, stream_ptr()))
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(k.cpu().numpy().astype(np.uint32), keys[order])
+    assert np.array_equal(v.cpu().numpy().astype(np.uint32), vals[order])
+
+
+def test_cell_keys_match_cpu(torch):
+    from lucky_droplets_b200 import _lib
+    rng = np.random.default_rng(3)
+    n = 30000
+    pos = rng.uniform(-1, 7, (n, 3))
+    rad = np.full(n, 0.02)
+    _, c = gpu_pairs(torch, pos, rad, 0.04)
+    kp = ctypes.c_void_p()
+    ip = ctypes.c_void_p()
+    assert _lib.lib().ld_collider_sorted(c._h, ctypes.byref(kp), ctypes.byref(ip)) == 0
+    import torch as T
+    keys = np.empty(n, np.uint32)
+    ids = np.empty(n, np.uint32)
+    # copy device arrays through torch (no host pointer access needed)
+    kt = T.empty(n, dtype=T.int32, device="cuda")
+    it = T.empty(n, dtype=T.int32, device="cuda")
+    cudart = ctypes.CDLL("libcudart.so.12")
+    cudart.cudaMemcpy.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    T.cuda.synchronize()
+    assert cudart.cudaMemcpy(kt.data_ptr(), kp.value, 4 * n, 3) == 0  # device to device
+    assert cudart.cudaMemcpy(it.data_ptr(), ip.value, 4 * n, 3) == 0
+    keys[:] = kt.cpu().numpy().astype(np.uint32)
+    ids[:] = it.cpu().numpy().astype(np.uint32)
+    _, ref_keys = K.cell_keys(pos, K.cell_count(TWO_PI, 0.04))
+    order = np.argsort(ref_keys, kind="stable")
+    assert np.array_equal(ids, order.astype(np.uint32))
+    assert np.array_equal(keys, ref_keys[order].astype(np.uint32))
+
+
+def test_pair_order_is_deterministic(torch):
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng(21)
+    n = 40000
+    pos = rng.uniform(0, TWO_PI, (n, 3))
+    rad = 0.02 * np.exp(0.3 * rng.standard_normal(n))
+    c = Collider(n, 2 * rad.max())
+    p, r = torch.as_tensor(pos).cuda(), torch.as_tensor(rad).cuda()
+    a = c.collide(p, r, cap=100000).cpu().numpy()
+    b = c.collide(p, r, cap=100000).cpu().numpy()
+    assert np.array_equal(a, b)

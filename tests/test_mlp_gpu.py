@@ -1,0 +1,124 @@
+"""Learned interpolation on the GPU: gradients and inference against the CPU oracle
+(oracle/mlp_np.py), the exact training targets against the direct Fourier sum, and a short
+training run that must beat tricubic interpolation."""
+import numpy as np
+import pytest
+
+from oracle import config_np as C
+from oracle import mlp_np as M
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a - b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def test_gradients_match_oracle(torch):
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    rng = np.random.default_rng(0)
+    nb = 200  # not a multiple of the 64-sample tile: padded rows must not contribute
+    X = np.zeros((nb, G.K1), np.float32)
+    X[:, :M.D_IN] = M.bf16(rng.standard_normal((nb, M.D_IN)).astype(np.float32))
+    T = rng.standard_normal((nb, 3)).astype(np.float32) * 0.3
+    p = M.init_params(3)
+    p["b1"] = rng.standard_normal(128).astype(np.float32) * 0.1
+    p["b2"] = rng.standard_normal(128).astype(np.float32) * 0.1
+    p["b3"] = rng.standard_normal(3).astype(np.float32) * 0.1
+    plan = Plan(16, "f32")
+    li = G.LearnedInterp(plan, params=G.flat_from_mats(p["W1"], p["b1"], p["W2"], p["b2"], p["W3"], p["b3"]))
+    Xg = torch.as_tensor(X).to("cuda", torch.bfloat16)
+    Tg = torch.as_tensor(T).cuda()
+    loss, grad = li.loss_and_grad(Xg, Tg)
+    gm = G.mats_from_flat(grad.cpu().numpy())
+    ref_loss, ref = M.mse_loss_and_grads(p, X[:, :M.D_IN], T)
+    assert abs(float(loss.item()) - ref_loss) / ref_loss < 1e-4
+    for k in ("W3", "b3", "W2", "b2"):
+        assert rel(gm[k], ref[k]) < 2e-3, k
+    for k in ("W1", "b1"):  # dH1 uses the BF16 dZ2 on the tensor cores
+        assert rel(gm[k], ref[k]) < 2e-2, k
+
+
+def _oracle_infer(u, pos, p):
+    st, t = C.stencil_4x4x4(u, pos)
+    s = st.reshape(pos.shape[0], 192)
+    scale = np.sqrt((s ** 2).mean(axis=1)) + 1e-30
+    X = np.concatenate([s / scale[:, None], t - 0.5], axis=1)
+    y, _ = M.forward(p, X)
+    tric = C.gather(u, pos, "tricubic")
+    return tric + scale[:, None] * y, tric
+
+
+def test_inference_matches_oracle(torch):
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=1e-3)
+    grid = C.ConfigGrid(N)
+    uk, u = C.init_flow(grid, prm, seed=8)
+    plan = Plan(N, "f32")
+    p = M.init_params(5)
+    li = G.LearnedInterp(plan, params=G.flat_from_mats(**p))
+    cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
+    u4 = li.interleaved(cube)
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(-1, 7.5, (3001, 3))
+    got = li.infer(u4, torch.as_tensor(pos).cuda()).cpu().numpy()
+    ref, tric = _oracle_infer(u, pos, p)
+    # the correction part agrees to FP32/BF16-input accuracy
+    assert rel(got - tric, ref - tric) < 5e-3
+    assert rel(got, ref) < 1e-4
+
+
+def test_training_targets_are_exact(torch):
+    """T * scale + tricubic at the shifted sample points equals the direct Fourier sum."""
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=1e-3)
+    grid = C.ConfigGrid(N)
+    uk, _ = C.init_flow(grid, prm, seed=9)
+    plan = Plan(N, "f64")
+    li = G.LearnedInterp(plan)
+    cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
+    rng = np.random.default_rng(4)
+    s = rng.uniform(0, 1, 3)
+    import ctypes
+    from lucky_droplets_b200 import _lib
+    from lucky_droplets_b200._lib import check, ptr, stream_ptr
+    shifted = plan.empty_cube(3)
+    check(_lib.lib().ld_phase_shift(plan.handle, ptr(cube), ptr(shifted), *map(float, s), stream_ptr()))
+    ue = plan.irfft_cube(shifted).cpu().numpy()
+    idx = rng.integers(0, N ** 3, 200)
+    j = np.stack([idx // (N * N), (idx // N) % N, idx % N], axis=1)
+    pos = (j + s) * (2 * np.pi / N)
+    exact = plan.exact_sum(cube, torch.as_tensor(pos).cuda()).cpu().numpy()
+    assert np.abs(ue.reshape(3, -1)[:, idx].T - exact).max() / np.abs(exact).max() < 1e-12
+
+
+def test_training_beats_tricubic(torch):
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=1e-3)
+    grid = C.ConfigGrid(N)
+    uk, _ = C.init_flow(grid, prm, seed=10)
+    plan = Plan(N, "f32")
+    li = G.LearnedInterp(plan, seed=1, tol=1e-12)
+    cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
+    X, T, _ = li.make_samples(cube, n_shifts=400, per_shift=1024, seed=1)
+    losses = li.train(X, T, epochs=12, batch=4096, lr=2e-3, lr_final=2e-4, seed=0)
+    assert losses[-1] < 0.5 * losses[0]
+    rng = np.random.default_rng(77)
+    pos = torch.as_tensor(rng.uniform(0, 2 * np.pi, (4000, 3))).cuda()
+    e_learned, e_tric = li.judge(cube, li.interleaved(cube), pos)
+    assert e_learned < e_tric, (e_learned, e_tric)
+    assert li.enabled
