@@ -190,6 +190,12 @@ LD_API int ld_gather4(ld_plan* plan, const void* u4, const double* pos, int64_t 
                       void* stream);
 /* planar (3, N^3) -> interleaved (N^3, 4) in the plan precision. */
 LD_API int ld_interleave3(ld_plan* plan, const void* planar, void* out, void* stream);
+/* Heun stage-2 positions xs = pos + h vel (n,3), and the droplet stage of ld_droplet_stage with the
+ * fluid velocity at the stage position given in up (n,3) (the learned interpolation supplies it). */
+LD_API int ld_droplet_predict(ld_plan* plan, const double* pos, const void* vel, int64_t n, double h, double* xs,
+                              void* stream);
+LD_API int ld_droplet_update(ld_plan* plan, int stage, const void* up, double* pos, void* vel, const void* tau,
+                             void* a1, int64_t n, double h, double g, void* stream);
 /* Floats of workspace ld_mlp_grad needs for a batch of nb samples. */
 LD_API int64_t ld_mlp_partial_floats(int64_t nb);
 /* Mean-squared-error loss and its exact gradient over a batch of nb samples (X bf16 (nb, k_in),

@@ -3,11 +3,11 @@
 // Pipeline (one call of ld_collide):
 //   keys      key[i] = cell of the wrapped position of droplet i, val[i] = i
 //   sort      stable LSD radix sort of (key, val), 8-bit digits
-//   ranges    cell_start / cell_end of every cell in the sorted order
-//   reorder   sorted copies of wrapped positions and radii (candidate loads become contiguous)
-//   count     per droplet i: partners j > i among the 27 neighbour cells that overlap
-//   scan      exclusive scan of the counts in droplet-id order -> offsets, total
-//   emit      pairs (i, j) at offset[i] + t, each droplet's run sorted by j
+//   starts    cs[k] = first sorted index of cell k (k = 0..ncell; cs[ncell] = n)
+//   reorder   sorted copies of wrapped positions and radii (FP64, and an FP32 copy for the filter)
+//   count     per sorted droplet: partners among the cell itself and its 13 forward neighbours
+//   scan      exclusive scan of the counts in sorted order -> offsets, total
+//   emit      pairs at offset + t in a fixed visiting order, then mapped to droplet ids (i < j)
 // The FP64 arithmetic (wrap, cell index, minimum image, squared distance) is done with explicit
 // round-to-nearest operations and no fused multiply-add, in the same order as the CPU rule, so
 // the pair list is bit-exact given identical inputs.
@@ -148,18 +148,23 @@ k_rs_scatter(const unsigned* __restrict__ kin, const unsigned* __restrict__ vin,
   }
 }
 
-// ---- cell ranges and sorted copies ------------------------------------------------------------
-__global__ void k_cell_ranges(const unsigned* __restrict__ skey, long long n, int* __restrict__ start,
-                              int* __restrict__ end) {
-  for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
-    const unsigned k = skey[s];
-    if (s == 0 || skey[s - 1] != k) start[k] = (int)s;
-    if (s == n - 1 || skey[s + 1] != k) end[k] = (int)(s + 1);
+// ---- cell starts and sorted copies ------------------------------------------------------------
+// cs[k] = number of sorted keys < k, for k = 0..ncell (binary search; cells are balanced work).
+__global__ void k_cell_starts(const unsigned* __restrict__ skey, long long n, long long ncell, int* __restrict__ cs) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k <= ncell; k += (long long)gridDim.x * blockDim.x) {
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+      const long long mid = (lo + hi) >> 1;
+      if ((long long)skey[mid] < k) lo = mid + 1;
+      else hi = mid;
+    }
+    cs[k] = (int)lo;
   }
 }
 
 __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __restrict__ rad,
-                              const unsigned* __restrict__ sval, long long n, double L, double4* __restrict__ sp) {
+                              const unsigned* __restrict__ sval, long long n, double L, double4* __restrict__ sp,
+                              float4* __restrict__ spf) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const unsigned i = sval[s];
     double4 q;
@@ -168,6 +173,7 @@ __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __re
     q.z = wrapL(pos[3 * (long long)i + 2], L);
     q.w = rad[i];
     sp[s] = q;
+    spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
   }
 }
 
@@ -245,62 +251,105 @@ __global__ void k_pairs(const double4* __restrict__ sp, const unsigned* __restri
   }
 }
 
-// Warp per cell (nc >= 3): the cell against itself and its 13 forward neighbours (offsets after
-// (0,0,0) in lexicographic order), so every unordered droplet pair is tested exactly once.  Pairs
-// are visited in a fixed order (neighbour, then i-major pair index in chunks of 32) and hits are
-// ranked inside each chunk by ballot, so the emitted order is deterministic.
-// MODE 0: cnt[cell] = hits; MODE 1: emit at off[cell] + rank as (min index, max index).
+// FP32 pre-test of the FP64 rule: true whenever overlap() is.  Coordinates in [0, L) rounded
+// to FP32 are off by at most L 2^-24 each, so every float difference is within 1.2e-7 L of the
+// FP64 one and the distance within 2.1e-7 L (plus relative roundoff of 1e-7 of the distance);
+// the margin of 1e-6 (L + rs) covers both several times over.
+__device__ __forceinline__ bool near_f(const float4 a, const float4 b, float L, float h, float margin) {
+  float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  if (dx > h) dx -= L;
+  if (dx < -h) dx += L;
+  if (dy > h) dy -= L;
+  if (dy < -h) dy += L;
+  if (dz > h) dz -= L;
+  if (dz < -h) dz += L;
+  const float r = a.w + b.w + margin;
+  return dx * dx + dy * dy + dz * dz < r * r;
+}
+
+// Block per (column, part), nc >= 3.  Column (cx, cy) holds cells (cx, cy, 0..nc-1), contiguous
+// in the sorted order.  Its droplets are tested against its own column (the same cell, partners
+// after them; the cell z+1) and the four forward columns (0,+1), (+1,-1), (+1,0), (+1,+1) at
+// cells z-1, z, z+1: the cell itself and its 13 forward neighbours, so every unordered pair is
+// tested exactly once.  The FP32 copies of the five columns are staged in shared memory (read
+// from global memory when they exceed cap_smem).  Each droplet visits its partners in a fixed
+// order; MODE 0 stores the count per sorted index, MODE 1 writes the pairs (sorted indices)
+// from off[i].
+constexpr int COL_THREADS = 256;
+constexpr int kColSmemRows = 12288;  // 192 KB of staged FP32 rows per block at most
+
 template <int MODE>
-__global__ void __launch_bounds__(256)
-k_cell_pairs(const double4* __restrict__ sp, const int* __restrict__ start, const int* __restrict__ end, int nc,
-             double L, unsigned* __restrict__ cnt, const unsigned* __restrict__ off, int* __restrict__ pairs,
-             long long cap) {
-  const int lane = threadIdx.x & 31;
-  const long long ncell = (long long)nc * nc * nc;
-  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-  for (long long c = blockIdx.x * (long long)(blockDim.x >> 5) + (threadIdx.x >> 5); c < ncell; c += warps) {
-    const int cz = (int)(c % nc), cy = (int)((c / nc) % nc), cx = (int)(c / ((long long)nc * nc));
-    const int a0 = start[c], a1 = end[c];
-    const int na = a1 - a0;
-    unsigned hits = 0;
-    long long o = MODE == 1 ? (long long)off[c] : 0;
-    if (na > 0) {
-      for (int q = 0; q < 14; ++q) {
-        // q = 0: the cell itself; q = 1..13: forward offsets
-        int dx = 0, dy = 0, dz = 0;
-        if (q > 0) {
-          const int r = q + 13;  // offsets -1..1 enumerated as r = (dx+1)*9 + (dy+1)*3 + (dz+1), r > 13
-          dx = r / 9 - 1;
-          dy = (r / 3) % 3 - 1;
-          dz = r % 3 - 1;
-        }
-        const long long nb = ((long long)((cx + dx + nc) % nc) * nc + (cy + dy + nc) % nc) * nc + (cz + dz + nc) % nc;
-        const int b0 = start[nb], b1 = end[nb];
-        const int nbb = b1 - b0;
-        const long long npair = (long long)na * nbb;
-        for (long long base = 0; base < npair; base += 32) {
-          const long long pidx = base + lane;
-          bool hit = false;
-          int ia = 0, ib = 0;
-          if (pidx < npair) {
-            ia = a0 + (int)(pidx / nbb);
-            ib = b0 + (int)(pidx % nbb);
-            if (q > 0 || ib > ia) hit = overlap(sp[ia], sp[ib], L);
-          }
-          const unsigned m = __ballot_sync(0xffffffffu, hit);
-          if (MODE == 1 && hit) {
-            const long long dst = o + __popc(m & ((1u << lane) - 1u));
-            if (dst < cap) {
-              pairs[2 * dst] = ia < ib ? ia : ib;
-              pairs[2 * dst + 1] = ia < ib ? ib : ia;
-            }
-          }
-          o += __popc(m);
-          hits += __popc(m);
+__global__ void __launch_bounds__(COL_THREADS)
+k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
+            const int* __restrict__ cs, int nc, int parts, double L, int cap_smem, unsigned* __restrict__ cnt,
+            const unsigned* __restrict__ off, int* __restrict__ pairs, long long cap) {
+  extern __shared__ float4 colbuf[];
+  __shared__ int lo[5], len[5], so[6];
+  const long long col = blockIdx.x / parts;
+  const int part = (int)(blockIdx.x % parts);
+  const int cx = (int)(col / nc), cy = (int)(col % nc);
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int q = 0; q < 5; ++q) {
+      const int ox = q < 2 ? 0 : 1;
+      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+      const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
+      lo[q] = cs[k];
+      len[q] = cs[k + nc] - cs[k];
+      so[q] = acc;
+      acc += len[q];
+    }
+    so[5] = acc;
+  }
+  __syncthreads();
+  const bool staged = so[5] <= cap_smem;
+  if (staged) {
+    for (int q = 0; q < 5; ++q)
+      for (int t = threadIdx.x; t < len[q]; t += COL_THREADS) colbuf[so[q] + t] = spf[lo[q] + t];
+  }
+  __syncthreads();
+  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
+  const long long ncol_cells = (long long)nc;
+  for (int t = part * COL_THREADS + threadIdx.x; t < len[0]; t += parts * COL_THREADS) {
+    const int i = lo[0] + t;
+    const float4 mf = staged ? colbuf[t] : spf[i];
+    const float mar = margin + 1e-6f * mf.w;
+    const int cz = (int)(skey[i] % (unsigned)nc);
+    unsigned c = 0;
+    long long o = MODE == 1 ? (long long)off[i] : 0;
+    double4 me;
+    bool have_me = false;
+    // target q, cell z: the sorted range [g0, g1)
+    for (int r = 0; r < 14; ++r) {
+      int q, dz;
+      if (r < 2) { q = 0; dz = r; }
+      else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
+      const int z = (cz + dz + nc) % nc;
+      const int base_cell = lo[q];
+      // cell start within column q: cs of the cell (column q, z)
+      int g0, g1;
+      {
+        const int ox = q < 2 ? 0 : 1;
+        const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+        const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * ncol_cells + z;
+        g0 = cs[k];
+        g1 = cs[k + 1];
+      }
+      if (r == 0) g0 = i + 1;
+      for (int g = g0; g < g1; ++g) {
+        const float4 b = staged ? colbuf[so[q] + (g - base_cell)] : spf[g];
+        if (!near_f(mf, b, Lf, hf, mar)) continue;
+        if (!have_me) { me = sp[i]; have_me = true; }
+        if (!overlap(me, sp[g], L)) continue;
+        if (MODE == 0) {
+          ++c;
+        } else {
+          if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
+          ++o;
         }
       }
     }
-    if (MODE == 0 && lane == 0) cnt[c] = hits;
+    if (MODE == 0) cnt[i] = c;
   }
 }
 
@@ -345,8 +394,9 @@ struct ld_collider {
   long long nmax = 0;
   int nc = 0;
   unsigned *key = nullptr, *val = nullptr, *key2 = nullptr, *val2 = nullptr, *hist = nullptr, *cnt = nullptr;
-  int *start = nullptr, *end = nullptr;
+  int* start = nullptr;  // cell starts, ncell + 1 entries
   double4* sp = nullptr;
+  float4* spf = nullptr;
   unsigned* status = nullptr;
   unsigned* sums = nullptr;  // scan tile totals
   int nblocks = 0;
@@ -389,9 +439,9 @@ int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
   A((void**)&c->val2, 4 * nmax);
   A((void**)&c->hist, 4 * (size_t)RADIX * c->nblocks);
   A((void**)&c->cnt, 4 * ((nmax > ncell ? nmax : ncell) + 1));
-  A((void**)&c->start, 4 * ncell);
-  A((void**)&c->end, 4 * ncell);
+  A((void**)&c->start, 4 * (ncell + 1));
   A((void**)&c->sp, sizeof(double4) * nmax);
+  A((void**)&c->spf, sizeof(float4) * nmax);
   A((void**)&c->status, sizeof(unsigned));
   {
     long long m = (nmax + 1) > (long long)RADIX * c->nblocks ? (nmax + 1) : (long long)RADIX * c->nblocks;
@@ -411,7 +461,7 @@ int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
 int ld_collider_destroy(ld_collider* c) {
   if (!c) return LD_OK;
   cudaFree(c->key); cudaFree(c->val); cudaFree(c->key2); cudaFree(c->val2); cudaFree(c->hist);
-  cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->end); cudaFree(c->sp); cudaFree(c->status);
+  cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->status);
   cudaFree(c->sums);
   delete c;
   return LD_OK;
@@ -462,29 +512,38 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
     if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
   }
   ProfScope ps(c->trace, KID_COLL_PAIRS, s);
-  LD_CUDA_CHECK(cudaMemsetAsync(c->start, 0, 4 * ncell, s));
-  LD_CUDA_CHECK(cudaMemsetAsync(c->end, 0, 4 * ncell, s));
-  k_cell_ranges<<<gridn(n, 256), 256, 0, s>>>(c->key, n, c->start, c->end);
-  k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp);
+  k_cell_starts<<<gridn(ncell + 1, 256), 256, 0, s>>>(c->key, n, ncell, c->start);
+  k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf);
+  LD_CUDA_CHECK(cudaMemsetAsync(c->cnt + n, 0, 4, s));
   if (nc >= 3) {
-    // cell-pair search over sorted positions; pairs come out as sorted-array indices and are
-    // mapped back to droplet indices by k_map_pairs
-    const int gw = gridn(ncell * 32, 256);
-    k_cell_pairs<0><<<gw, 256, 0, s>>>(c->sp, c->start, c->end, nc, L, c->cnt, nullptr, nullptr, 0);
-    LD_CUDA_CHECK(cudaMemsetAsync(c->cnt + ncell, 0, 4, s));
-    if (int rc = scan_u32(c, c->cnt, ncell + 1, s)) return rc;
-    k_cell_pairs<1><<<gw, 256, 0, s>>>(c->sp, c->start, c->end, nc, L, nullptr, c->cnt, pairs, cap);
-    k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + ncell, cap, c->val, pairs);
-    k_finish<<<1, 1, 0, s>>>(c->cnt, ncell, cap, count, c->status);
-  } else {
-    k_pairs<0, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, c->end, n, nc, L, c->cnt,
-                                                   nullptr, nullptr, 0);
-    LD_CUDA_CHECK(cudaMemsetAsync(c->cnt + n, 0, 4, s));
+    // block per cell column; pairs come out as sorted-array indices and are mapped back to
+    // droplet indices by k_map_pairs
+    const long long ncol = (long long)nc * nc;
+    const long long per_col = (n + ncol - 1) / ncol;
+    const long long parts = per_col > 512 ? (per_col + 511) / 512 : 1;
+    long long want = 5 * per_col + (5 * per_col) / 4 + 256;  // typical staged rows, with headroom
+    if (want > kColSmemRows) want = kColSmemRows;
+    const int cap_smem = (int)want;
+    const size_t smem = sizeof(float4) * (size_t)cap_smem;
+    if (ncol * parts > 0x7fffffffLL) return ld_fail(LD_ERR_UNSUPPORTED, "ld_collide: too many cell columns");
+    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const unsigned gb = (unsigned)(ncol * parts);
+    k_col_pairs<0><<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem,
+                                                 c->cnt, nullptr, nullptr, 0);
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
-    k_pairs<1, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, c->end, n, nc, L, nullptr,
+    k_col_pairs<1><<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem,
+                                                 nullptr, c->cnt, pairs, cap);
+    k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + n, cap, c->val, pairs);
+  } else {
+    const int* end = c->start + 1;  // end of cell k = start of cell k + 1
+    k_pairs<0, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, end, n, nc, L, c->cnt,
+                                                   nullptr, nullptr, 0);
+    if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
+    k_pairs<1, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, end, n, nc, L, nullptr,
                                                    c->cnt, pairs, cap);
-    k_finish<<<1, 1, 0, s>>>(c->cnt, n, cap, count, c->status);
   }
+  k_finish<<<1, 1, 0, s>>>(c->cnt, n, cap, count, c->status);
   LD_LAUNCH_CHECK();
   return LD_OK;
 }

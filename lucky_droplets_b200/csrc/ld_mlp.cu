@@ -522,6 +522,41 @@ __global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, f
   }
 }
 
+// Droplet stage with the fluid velocity at the stage position given (the learned interpolation
+// evaluates it in a separate launch): the arithmetic of k_droplet_stage without the gather.
+template <typename T>
+__global__ void k_droplet_given(int stage, const T* __restrict__ up, double* __restrict__ pos, T* __restrict__ vel,
+                                const T* __restrict__ tau, T* __restrict__ a1, long long n, double h, T g) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
+    const T it = T(1) / tau[i];
+    if (stage == 1) {
+      a1[3 * i] = (up[3 * i] - vx) * it;
+      a1[3 * i + 1] = (up[3 * i + 1] - vy) * it;
+      a1[3 * i + 2] = (up[3 * i + 2] - vz) * it - g;
+    } else {
+      const T ax = a1[3 * i], ay = a1[3 * i + 1], az = a1[3 * i + 2];
+      const T hh = T(h);
+      const T sx = vx + hh * ax, sy = vy + hh * ay, sz = vz + hh * az;
+      const T bx = (up[3 * i] - sx) * it, by = (up[3 * i + 1] - sy) * it, bz = (up[3 * i + 2] - sz) * it - g;
+      pos[3 * i] += 0.5 * h * (double(vx) + double(sx));
+      pos[3 * i + 1] += 0.5 * h * (double(vy) + double(sy));
+      pos[3 * i + 2] += 0.5 * h * (double(vz) + double(sz));
+      vel[3 * i] = vx + T(0.5) * hh * (ax + bx);
+      vel[3 * i + 1] = vy + T(0.5) * hh * (ay + by);
+      vel[3 * i + 2] = vz + T(0.5) * hh * (az + bz);
+    }
+  }
+}
+
+// xs = x + h v (the stage-2 position of the Heun step)
+template <typename T>
+__global__ void k_droplet_predict(const double* __restrict__ pos, const T* __restrict__ vel, long long n, double h,
+                                  double* __restrict__ xs) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * n; e += (long long)gridDim.x * blockDim.x)
+    xs[e] = pos[e] + h * double(vel[e]);
+}
+
 // planar (3, M) -> interleaved (M, 4) with a zero fourth component
 template <typename T>
 __global__ void k_interleave3(const T* __restrict__ in, vec4<T>* __restrict__ out, long long m) {
@@ -641,6 +676,34 @@ int ld_gather4(ld_plan* p, const void* u4, const double* pos, int64_t n, int met
     else LD_G4(double, double4, LD_INTERP_COSINE);
   }
 #undef LD_G4
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_droplet_predict(ld_plan* p, const double* pos, const void* vel, int64_t n, double h, double* xs,
+                       void* stream) {
+  if (!p || n < 0 || (n > 0 && (!pos || !vel || !xs))) return ld_fail(LD_ERR_ARG, "ld_droplet_predict: bad arguments");
+  if (n == 0) return LD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->prec == LD_F32) k_droplet_predict<float><<<gridn(3 * n, 256), 256, 0, s>>>(pos, (const float*)vel, n, h, xs);
+  else k_droplet_predict<double><<<gridn(3 * n, 256), 256, 0, s>>>(pos, (const double*)vel, n, h, xs);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_droplet_update(ld_plan* p, int stage, const void* up, double* pos, void* vel, const void* tau, void* a1,
+                      int64_t n, double h, double g, void* stream) {
+  if (!p || (stage != 1 && stage != 2) || n < 0 || (n > 0 && (!up || !pos || !vel || !tau || !a1)))
+    return ld_fail(LD_ERR_ARG, "ld_droplet_update: bad arguments");
+  if (n == 0) return LD_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  ProfScope ps(p, stage == 1 ? KID_DROPLET1 : KID_DROPLET2, s);
+  if (p->prec == LD_F32)
+    k_droplet_given<float><<<gridn(n, 256), 256, 0, s>>>(stage, (const float*)up, pos, (float*)vel, (const float*)tau,
+                                                         (float*)a1, n, h, (float)g);
+  else
+    k_droplet_given<double><<<gridn(n, 256), 256, 0, s>>>(stage, (const double*)up, pos, (double*)vel,
+                                                          (const double*)tau, (double*)a1, n, h, g);
   LD_LAUNCH_CHECK();
   return LD_OK;
 }

@@ -251,7 +251,28 @@ class Droplets:
         order = _torch().argsort(self.ids)
         return t[order].cpu().numpy()
 
+    def use_learned(self, learned):
+        """Interpolate with a trained LearnedInterp (tricubic + learned correction); the judge of
+        the LearnedInterp switches back to tricubic when it fails."""
+        torch = _torch()
+        self.learned = learned
+        self._up = torch.empty((self.n, 3), dtype=self.plan.rdtype, device=self.plan.device)
+        self._xs = torch.empty((self.n, 3), dtype=torch.float64, device=self.plan.device)
+
     def stage(self, s, u_phys, h, stream=None):
+        li = getattr(self, "learned", None)
+        if li is not None and li.enabled:
+            L = _lib.lib()
+            st = stream_ptr(stream)
+            if s == 1:
+                li.infer(u_phys, self.pos, out=self._up, stream=stream)
+            else:
+                check(L.ld_droplet_predict(self.plan.handle, ptr(self.pos), ptr(self.vel), self.n, float(h),
+                                           ptr(self._xs), st))
+                li.infer(u_phys, self._xs, out=self._up, stream=stream)
+            check(L.ld_droplet_update(self.plan.handle, int(s), ptr(self._up), ptr(self.pos), ptr(self.vel),
+                                      ptr(self.tau), ptr(self.a1), self.n, float(h), self.g, st))
+            return
         check(_lib.lib().ld_droplet_stage(self.plan.handle, int(s), ptr(u_phys), ptr(self.pos), ptr(self.vel),
                                           ptr(self.tau), ptr(self.a1), self.n, self.m, float(h), self.g,
                                           stream_ptr(stream)))

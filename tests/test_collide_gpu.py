@@ -135,3 +135,33 @@ def test_pair_order_is_deterministic(torch):
     a = c.collide(p, r, cap=100000).cpu().numpy()
     b = c.collide(p, r, cap=100000).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def _contact_pairs(rng, m, rel_gap):
+    r = rng.uniform(0.005, 0.02, (m, 2))
+    rs = r.sum(axis=1)
+    d = rng.standard_normal((m, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    sign = np.where(np.arange(m) % 2 == 0, -1.0, 1.0)  # inside / outside by rel_gap
+    sep = rs * (1.0 + sign * rel_gap)
+    a = rng.uniform(0, TWO_PI, (m, 3))
+    a[: m // 4, 0] = rng.uniform(-1e-3, 1e-3, m // 4)  # straddle the x = 0 face
+    b = a + d * sep[:, None]
+    pos = np.empty((2 * m, 3))
+    pos[0::2], pos[1::2] = a, b
+    rad = np.empty(2 * m)
+    rad[0::2], rad[1::2] = r[:, 0], r[:, 1]
+    return pos, rad
+
+
+@pytest.mark.parametrize("rel_gap", [1e-7, 1e-10, 1e-13])
+def test_contact_distance_boundary(torch, rel_gap):
+    """Pairs placed at the contact distance (1 -/+ rel_gap) rs, a quarter across the x = 0 face:
+    the FP32 pre-test keeps every pair the FP64 rule accepts (the list is bit-exact)."""
+    rng = np.random.default_rng(int(-np.log10(rel_gap)))
+    pos, rad = _contact_pairs(rng, 20000, rel_gap)
+    cell = 2 * rad.max()
+    got, _ = gpu_pairs(torch, pos, rad, cell)
+    ref = K.collide(pos, rad, cell)
+    assert len(ref) >= 5000  # the inside half, mostly
+    assert got.shape == ref.shape and np.array_equal(got, ref)
