@@ -168,23 +168,26 @@ LD_API int ld_exact_sum(ld_plan* plan, const void* uk, const double* pos, int64_
 
 /* ---- learned interpolation (no counterpart in the reference) ------------------------------ */
 /* MLP 195 -> 128 SiLU -> 128 SiLU -> 3 on BF16 tensor-core tiles with FP32 accumulation, predicting
- * (exact spectral - tricubic) / scale from the 4x4x4 stencil of (u, v, w) divided by its RMS
- * `scale` and the fractional cell offsets minus 1/2.  Parameters: one FP32 vector of n_params
- * (layout in csrc/ld_mlp.cu); the kernels read a packed BF16 copy (n_packed) made by ld_mlp_pack. */
+ * (exact spectral - tricubic) / (scale * os) from the 4x4x4 stencil of (u, v, w) in an orthonormal
+ * polynomial basis, divided by its RMS `scale` and multiplied by per-coefficient feature scales,
+ * and the fractional cell offsets minus 1/2.  Parameters: one FP32 vector of n_params (layout,
+ * feature scales and output scale os in csrc/ld_mlp.cu); the kernels read a packed BF16 copy
+ * (n_packed) made by ld_mlp_pack. */
 LD_API int ld_mlp_sizes(int64_t* n_params, int64_t* n_packed, int32_t* k_in, int32_t* batch_tile);
 LD_API int ld_mlp_pack(const float* params, void* packed, void* stream);
 /* Fused gather + tricubic + MLP at n droplets from the interleaved (N,N,N,4) velocity:
- * out (n,3) = tricubic + scale * MLP(features). */
+ * out (n,3) = tricubic + scale * os * MLP(features). */
 LD_API int ld_mlp_infer(ld_plan* plan, const void* u4, const double* pos, int64_t n, const void* packed,
                         const float* params, void* out, void* stream);
 /* uk * exp(i k.(s dx)) for a cube-layout 3-vector: the field translated so that its grid values are
  * the original field's values at x_j + s dx (s in grid units). */
 LD_API int ld_phase_shift(ld_plan* plan, const void* uk, void* out, double sx, double sy, double sz, void* stream);
 /* Training samples at grid points idx[i] + s (grid units): X (ns, k_in) bf16 features from the
- * interleaved field u4, T (ns,3) = (exact - tricubic)/scale with exact = ue (planar (3,N^3), the
- * field phase-shifted by s) at idx[i], aux (ns,4) = tricubic xyz and scale. */
+ * interleaved field u4 with the feature scales of params, T (ns,3) = (exact - tricubic)/(scale * os)
+ * with exact = ue (planar (3,N^3), the field phase-shifted by s) at idx[i], aux (ns,4) = tricubic xyz
+ * and scale. */
 LD_API int ld_mlp_samples(ld_plan* plan, const void* u4, const void* ue, const int64_t* idx, int64_t ns, double sx,
-                          double sy, double sz, void* X, float* T, float* aux, void* stream);
+                          double sy, double sz, const float* params, void* X, float* T, float* aux, void* stream);
 /* Interpolation of an interleaved (N,N,N,4) velocity at n positions -> out (n,3). */
 LD_API int ld_gather4(ld_plan* plan, const void* u4, const double* pos, int64_t n, int method, void* out,
                       void* stream);
@@ -198,10 +201,11 @@ LD_API int ld_droplet_update(ld_plan* plan, int stage, const void* up, double* p
                              void* a1, int64_t n, double h, double g, void* stream);
 /* Floats of workspace ld_mlp_grad needs for a batch of nb samples. */
 LD_API int64_t ld_mlp_partial_floats(int64_t nb);
-/* Mean-squared-error loss and its exact gradient over a batch of nb samples (X bf16 (nb, k_in),
- * T (nb,3)): deterministic fixed-order reductions.  grad: n_params floats; loss: 1 float. */
-LD_API int ld_mlp_grad(const void* X, const float* T, int64_t nb, const float* params, const void* packed,
-                       float* work, float* grad, float* loss, void* stream);
+/* Weighted mean-squared-error loss sum_r w_r |Y_r - T_r|^2 / nb and its exact gradient over a batch
+ * of nb samples (X bf16 (nb, k_in), T (nb,3), W (nb) or null for unit weights): deterministic
+ * fixed-order reductions.  grad: n_params floats; loss: 1 float. */
+LD_API int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb, const float* params,
+                       const void* packed, float* work, float* grad, float* loss, void* stream);
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on the FP32 parameters, then re-packs the BF16 copy. */
 LD_API int ld_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t step, float lr, void* packed,
                        void* stream);

@@ -62,13 +62,13 @@ SIGNATURES = {
     "ld_mlp_pack": (_c_i, [_c_p, _c_p, _c_p]),
     "ld_mlp_infer": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p]),
     "ld_phase_shift": (_c_i, [_c_p, _c_p, _c_p, _c_d, _c_d, _c_d, _c_p]),
-    "ld_mlp_samples": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_d, _c_p, _c_p, _c_p, _c_p]),
+    "ld_mlp_samples": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_d, _c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_interleave3": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_gather4": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
     "ld_mlp_partial_floats": (_c_i64, [_c_i64]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),
     "ld_droplet_update": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_p]),
-    "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),
+    "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_mlp_adam": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_float, _c_p, _c_p]),
     "ld_collider_create": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32]),
     "ld_collider_destroy": (_c_i, [_c_p]),

@@ -6,9 +6,11 @@
 // also drops the imaginary part of the kz = 0 coefficients).  Only the modes of the spherical
 // mask round(|k|) <= kc are summed: they are the only non-zero modes of a dealiased field.
 //
-// One thread per point.  Every thread of a warp walks the same (kx, ky, kz) sequence, so the
-// spectrum loads are warp-uniform (one broadcast transaction per warp); the phases come from
-// FP64 recurrences seeded by sincos once per row.
+// Thread per point and block per (tile of 128 points, chunk of kx planes): the kx planes are
+// split across blocks so that even 1e4 points fill the GPU, and the per-chunk partial sums are
+// added in chunk order afterwards (deterministic).  Every thread of a warp walks the same
+// (kx, ky, kz) sequence, so the spectrum loads are warp-uniform (one broadcast transaction per
+// warp); the phases come from FP64 recurrences seeded by sincos once per row.
 #include "ld_internal.cuh"
 
 namespace {
@@ -16,8 +18,10 @@ namespace {
 template <typename T>
 __global__ void __launch_bounds__(128)
 k_exact_sum(const ld::cplx<T>* __restrict__ uk, long long cs, int N, int kc, int My, int Mzp,
-            const double* __restrict__ pos, long long n, double* __restrict__ out) {
+            const double* __restrict__ pos, long long n, int per_chunk, double* __restrict__ part) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int ix0 = blockIdx.y * per_chunk;
+  const int ix1 = ix0 + per_chunk < My ? ix0 + per_chunk : My;
   const bool ok = i < n;
   const double x = ok ? pos[3 * i] : 0.0, y = ok ? pos[3 * i + 1] : 0.0, z = ok ? pos[3 * i + 2] : 0.0;
   const int lim = kc * kc + kc;  // round(|k|) <= kc  <=>  k^2 <= kc^2 + kc
@@ -26,7 +30,7 @@ k_exact_sum(const ld::cplx<T>* __restrict__ uk, long long cs, int N, int kc, int
   sincos(y, &syi, &syr);
   sincos(z, &szi, &szr);
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int ix = 0; ix < My; ++ix) {
+  for (int ix = ix0; ix < ix1; ++ix) {
     const int kx = ix <= kc ? ix : ix - My;
     double exr, exi;
     sincos((double)kx * x, &exi, &exr);
@@ -68,9 +72,17 @@ k_exact_sum(const ld::cplx<T>* __restrict__ uk, long long cs, int N, int kc, int
 #pragma unroll
     for (int c = 0; c < 3; ++c) acc[c] += tx[c][0] * exr - tx[c][1] * exi;  // Re(ex * tx)
   }
-  if (ok) {
-    const double s = 1.0 / ((double)N * N * N);
-    for (int c = 0; c < 3; ++c) out[3 * i + c] = acc[c] * s;
+  if (ok)
+    for (int c = 0; c < 3; ++c) part[((long long)blockIdx.y * n + i) * 3 + c] = acc[c];
+}
+
+// out = (1/N^3) sum over chunks, in chunk order
+__global__ void k_exact_reduce(const double* __restrict__ part, int chunks, long long n, double scale,
+                               double* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < 3 * n; e += (long long)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int c = 0; c < chunks; ++c) s += part[(long long)c * 3 * n + e];
+    out[e] = s * scale;
   }
 }
 
@@ -82,13 +94,36 @@ extern "C" int ld_exact_sum(ld_plan* p, const void* uk, const double* pos, int64
   cudaStream_t s = (cudaStream_t)stream;
   ProfScope ps(p, KID_EXACT, s);
   const int th = 128;
-  const long long blocks = (n + th - 1) / th;
-  if (p->prec == LD_F32)
-    k_exact_sum<float><<<(unsigned)blocks, th, 0, s>>>((const float2*)uk, p->cube_elems(), p->N, p->kc, p->My,
-                                                       p->Mzp, pos, n, out);
-  else
-    k_exact_sum<double><<<(unsigned)blocks, th, 0, s>>>((const double2*)uk, p->cube_elems(), p->N, p->kc, p->My,
-                                                        p->Mzp, pos, n, out);
-  LD_LAUNCH_CHECK();
+  // partial sums live in the plan's transform workspace (free between steps): points are taken
+  // in batches that fit it
+  const long long cap = (long long)(p->work_bytes / sizeof(double));
+  double* part = (double*)p->work;
+  const double scale = 1.0 / ((double)p->N * p->N * p->N);
+  for (long long b0 = 0; b0 < n; ) {
+    long long nb = n - b0;
+    const long long tiles_all = (nb + th - 1) / th;
+    int chunks = (int)((148LL * 12 + tiles_all - 1) / tiles_all);
+    if (chunks > p->My) chunks = p->My;
+    if (chunks < 1) chunks = 1;
+    if ((long long)chunks * 3 * nb > cap) {
+      nb = cap / (3LL * chunks);
+      if (nb < 1) { chunks = 1; nb = cap / 3; }
+      if (nb < 1) return ld_fail(LD_ERR_CAPACITY, "ld_exact_sum: no workspace");
+    }
+    const int per_chunk = (p->My + chunks - 1) / chunks;
+    chunks = (p->My + per_chunk - 1) / per_chunk;
+    const dim3 grid((unsigned)((nb + th - 1) / th), (unsigned)chunks);
+    if (p->prec == LD_F32)
+      k_exact_sum<float><<<grid, th, 0, s>>>((const float2*)uk, p->cube_elems(), p->N, p->kc, p->My, p->Mzp,
+                                             pos + 3 * b0, nb, per_chunk, part);
+    else
+      k_exact_sum<double><<<grid, th, 0, s>>>((const double2*)uk, p->cube_elems(), p->N, p->kc, p->My, p->Mzp,
+                                              pos + 3 * b0, nb, per_chunk, part);
+    long long rb = (3 * nb + 255) / 256;
+    if (rb > 148LL * 16) rb = 148LL * 16;
+    k_exact_reduce<<<(unsigned)rb, 256, 0, s>>>(part, chunks, nb, scale, out + 3 * b0);
+    LD_LAUNCH_CHECK();
+    b0 += nb;
+  }
   return LD_OK;
 }

@@ -30,7 +30,8 @@ enum LdKernelId : int {
   KID_COLL_SORT,     // collision cell keys + radix sort
   KID_COLL_PAIRS,    // collision ranges, count, scan, emit
   KID_CELL_ORDER,    // droplet cell-order permutation
-  KID_MLP_INFER,     // fused gather + tricubic + MLP
+  KID_MLP_INFER,     // MLP forward of the feature rows (+ tricubic, back to the grid frame)
+  KID_MLP_FEAT,      // canonical stencil gather + polynomial features
   KID_COUNT_BASE     // further ids are defined by later units
 };
 

@@ -7,16 +7,31 @@
 //
 // Features of a point with stencil values s (192 = 3 components x 64 taps, tap order
 // c*64 + a*16 + b*4 + q for offsets a, b, q in -1..2 along x, y, z) and cell offsets t (3):
-//   scale   = sqrt(mean(s^2)) + 1e-30
-//   x[0:192] = s / scale,  x[192:195] = t - 0.5,  x[195:208] = 0
-//   u(point) = tricubic(s, t) + scale * MLP(x)
-// Per-point normalisation keeps the inputs O(1) and makes the prediction scale with the field,
-// as the exact correction (a linear functional of the field) does.
+//   D_c      = (P x P x P) s_c    per component: the orthonormal discrete polynomial basis of
+//              orders 0..3 on 4 points along each axis (FP32)
+//   scale    = RMS of all 192 coefficients (scale mode 0), or of the 162 coefficients of total
+//              order >= 3 (mode 1: tracks the small-scale content the correction depends on,
+//              so the normalised targets drift less while a flow develops), + 1e-30
+//   x[0:192] = D / scale * fs,  x[192:195] = t - 0.5,  x[195:208] = 0     (canonical frame)
+//   u(point) = tricubic(s, t) + scale * os * MLP(x)                     (back in the grid frame)
+// Canonical frame: the exact correction is equivariant under the 48 reflections and axis
+// permutations of the cube, and the flow is statistically isotropic.  Each axis whose offset
+// exceeds 1/2 is reflected (offset -> 1 - offset, that velocity component and the odd-order
+// coefficients along it change sign), then the axes are ordered by decreasing reflected offset
+// (stable).  Features, targets and outputs are expressed in that frame, which shrinks the input
+// domain 48-fold.
+// The correction lives in the high-order coefficients, which are 1e-2..1e-4 of the values: the
+// transform happens in FP32 before the BF16 rounding, and the per-coefficient feature scales fs
+// (64, shared by the components) bring every feature to O(1).  fs and the output scale os are
+// set from sample statistics before training and are not trained.  Per-point normalisation makes
+// the prediction scale with the field, as the exact correction (a linear functional of the
+// field) does.
 //
 // Parameter vector (FP32, contiguous), "params":
 //   W1 [208][128] (input-major; rows 195..207 stay zero)  b1 [128]
 //   W2 [128][128]                                          b2 [128]
 //   W3 [128][8]   (columns 3..7 stay zero)                 b3 [8]
+//   fs [64]       os [8] (os[0]: output scale, os[1]: scale mode)
 // Packed BF16 copies for the tensor cores ("packed"), output-major with padded rows:
 //   W1t [128][KP1]   W2t [128][KP2]   W2n [128][KP2] (= W2, input-major)   W3t [8][KP2]   W3n [128][8]
 #include <cmath>
@@ -41,7 +56,9 @@ constexpr int OFF_W2 = OFF_B1 + H;
 constexpr int OFF_B2 = OFF_W2 + H * H;
 constexpr int OFF_W3 = OFF_B2 + H;
 constexpr int OFF_B3 = OFF_W3 + H * N3;
-constexpr int N_PARAMS = OFF_B3 + N3;
+constexpr int OFF_FS = OFF_B3 + N3;
+constexpr int OFF_OS = OFF_FS + 64;
+constexpr int N_PARAMS = OFF_OS + 8;
 
 constexpr int P_W1T = 0;
 constexpr int P_W2T = P_W1T + H * KP1;
@@ -96,59 +113,204 @@ __device__ __forceinline__ void warp_gemm(float (*acc)[4], const bf16* A, int ld
   }
 }
 
-// Tricubic stencil of one point from the interleaved field: writes 192 stencil values (fp32) and
-// returns the tricubic velocity and the fractional offsets.
-template <typename T>
-__device__ __forceinline__ void stencil_point(const vec4<T>* __restrict__ f, int N, double L, double px, double py,
-                                              double pz, float* st, float* tric, float* toff) {
-  using A = AxisW<T, LD_INTERP_TRICUBIC>;
-  int ix, iy, iz;
-  T wx[4], wy[4], wz[4];
-  A::get(px, N, L, ix, wx);
-  A::get(py, N, L, iy, wy);
-  A::get(pz, N, L, iz, wz);
-  const double sc = double(N) / L;
-  double tx = px * sc, ty = py * sc, tz = pz * sc;
-  toff[0] = float(tx - floor(tx));
-  toff[1] = float(ty - floor(ty));
-  toff[2] = float(tz - floor(tz));
-  float o0 = 0, o1 = 0, o2 = 0;
-#pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int jx = (ix - 1 + a + N) & (N - 1);
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int jy = (iy - 1 + b + N) & (N - 1);
-      const vec4<T>* row = f + ((long long)jx * N + jy) * N;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int jz = (iz - 1 + q + N) & (N - 1);
-        const vec4<T> v = row[jz];
-        const int tap = a * 16 + b * 4 + q;
-        st[tap] = float(v.x);
-        st[64 + tap] = float(v.y);
-        st[128 + tap] = float(v.z);
-        const float w = float(wx[a] * wy[b] * wz[q]);
-        o0 += w * float(v.x);
-        o1 += w * float(v.y);
-        o2 += w * float(v.z);
-      }
-    }
-  }
-  tric[0] = o0;
-  tric[1] = o1;
-  tric[2] = o2;
+// ---- features of one point ------------------------------------------------------------------------
+// The building blocks below are shared by the thread-per-sample training kernel and the
+// warp-cooperative inference kernel; every element goes through the same arithmetic in both,
+// so training and inference features agree bit for bit.
+
+// Orthonormal discrete polynomial basis on 4 points (orders 0..3), in place.
+__device__ __forceinline__ void poly4(float* v, int stride) {
+  const float s0 = v[0], s1 = v[stride], s2 = v[2 * stride], s3 = v[3 * stride];
+  const float r20 = 0.22360679774997896f;  // 1/sqrt(20)
+  v[0] = 0.5f * ((s0 + s1) + (s2 + s3));
+  v[stride] = r20 * ((3.f * (s3 - s0)) + (s2 - s1));
+  v[2 * stride] = 0.5f * ((s0 - s1) - (s2 - s3));
+  v[3 * stride] = r20 * ((s3 - s0) + 3.f * (s1 - s2));
 }
 
-// Features of one point into a bf16 row of K1 (+ scale); st = 192 stencil values.
-__device__ __forceinline__ float features_row(const float* st, const float* toff, bf16* row) {
-  float ss = 0.f;
-  for (int i = 0; i < 192; ++i) ss += st[i] * st[i];
-  const float scale = sqrtf(ss / 192.f) + 1e-30f;
+// Frame code: bits 0-5 hold p[0..2] (canonical axis k <- grid axis p[k], 2 bits each), bits 6-8
+// the reflection of grid axes 0..2.
+__device__ __forceinline__ int frame_perm(int code, int k) { return (code >> (2 * k)) & 3; }
+__device__ __forceinline__ float frame_sign(int code, int d) { return (code >> (6 + d)) & 1 ? -1.f : 1.f; }
+
+__device__ __forceinline__ int make_frame(const float* toff, float* tc) {
+  float r[3];
+  int code = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const bool rf = toff[d] > 0.5f;
+    r[d] = rf ? 1.f - toff[d] : toff[d];
+    code |= (rf ? 1 : 0) << (6 + d);
+  }
+  int p0 = 0, p1 = 1, p2 = 2, x;
+  if (r[p1] > r[p0]) { x = p0; p0 = p1; p1 = x; }
+  if (r[p2] > r[p1]) { x = p1; p1 = p2; p2 = x; }
+  if (r[p1] > r[p0]) { x = p0; p0 = p1; p1 = x; }
+  tc[0] = r[p0];
+  tc[1] = r[p1];
+  tc[2] = r[p2];
+  return code | p0 | (p1 << 2) | (p2 << 4);
+}
+
+// Cell and canonical frame of a point: grid cell i (periodic), offsets t in grid units.
+struct PtFrame {
+  int i[3];
+  int code;
+  float tc[3];
+};
+
+__device__ __forceinline__ void point_frame(double px, double py, double pz, int N, double L, PtFrame& f) {
+  const double sc = double(N) / L;
+  const double q[3] = {px * sc, py * sc, pz * sc};
+  float toff[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double fl = floor(q[d]);
+    toff[d] = float(q[d] - fl);
+    long long ii = (long long)fl % N;
+    if (ii < 0) ii += N;
+    f.i[d] = int(ii);
+  }
+  f.code = make_frame(toff, f.tc);
+}
+
+// Tap `tap` (canonical j0*16 + j1*4 + j2, j in 0..3 <-> offsets -1..2) of the point's stencil (component
+// blocks CS floats apart) in
+// its canonical frame: along canonical axis k the taps run over grid axis p[k], reversed when that
+// axis is reflected; canonical component cc is grid component p[cc] with the reflection's sign.
+template <typename T, int CS>
+__device__ __forceinline__ void canon_tap(const vec4<T>* __restrict__ u4, int N, const int* ci, int code, int tap,
+                                          float* st) {
+  const int j[3] = {tap >> 4, (tap >> 2) & 3, tap & 3};
+  int g[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const int d = frame_perm(code, k);
+    const int o = (code >> (6 + d)) & 1 ? 3 - j[k] : j[k];
+    g[d] = (ci[d] - 1 + o + N) & (N - 1);
+  }
+  const vec4<T> v = u4[((long long)g[0] * N + g[1]) * N + g[2]];
+  const float comp[3] = {float(v.x), float(v.y), float(v.z)};
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    const int d = frame_perm(code, cc);
+    st[cc * CS + tap] = frame_sign(code, d) * comp[d];
+  }
+}
+
+// Tricubic weights of the canonical offsets in the polynomial basis (per canonical axis): the
+// tricubic value is sum_i D_i wh0[i0] wh1[i1] wh2[i2] (P orthonormal: w.s = (P w).(P s)).
+__device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float t = tc[k];
+    wh[k][0] = -t * (t - 1.f) * (t - 2.f) / 6.f;
+    wh[k][1] = (t + 1.f) * (t - 1.f) * (t - 2.f) / 2.f;
+    wh[k][2] = -(t + 1.f) * t * (t - 2.f) / 2.f;
+    wh[k][3] = (t + 1.f) * t * (t - 1.f) / 6.f;
+    poly4(wh[k], 1);
+  }
+}
+
+// One component's 64 taps (canonical order, in registers) -> its polynomial coefficients, then
+// the component's partial sums: squares, squares of total order >= 3, and its tricubic value.
+// The three components are combined as (c0 + c1) + c2 by every caller, so all paths round
+// identically; all indices are compile-time constants.
+__device__ __forceinline__ void comp_transform(float (&v)[64]) {
+#pragma unroll
+  for (int a = 0; a < 16; ++a) poly4(v + 4 * a, 1);                          // along axis 2
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) poly4(v + 16 * a + q, 4);                    // along axis 1
+#pragma unroll
+  for (int e = 0; e < 16; ++e) poly4(v + e, 16);                             // along axis 0
+}
+
+struct CompSums {
+  float ss, sh, tr;
+};
+
+__device__ __forceinline__ CompSums comp_sums(const float (&v)[64], const float (&wh)[3][4]) {
+  CompSums p{0.f, 0.f, 0.f};
+#pragma unroll
+  for (int j = 0; j < 64; ++j) {
+    const float v2 = v[j] * v[j];
+    p.ss += v2;
+    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh += v2;
+    p.tr += ((wh[0][j >> 4] * wh[1][(j >> 2) & 3]) * wh[2][j & 3]) * v[j];
+  }
+  return p;
+}
+
+__device__ __forceinline__ float scale_of(float ss0, float ss1, float ss2, float sh0, float sh1, float sh2,
+                                          float mode) {
+  const float ss = (ss0 + ss1) + ss2, sh = (sh0 + sh1) + sh2;
+  return (mode != 0.f ? sqrtf(sh / 162.f) : sqrtf(ss / 192.f)) + 1e-30f;
+}
+
+// The 64 features of one component as 32 packed bf16 pairs.
+__device__ __forceinline__ void comp_features(const float (&v)[64], const float* __restrict__ fs, float inv,
+                                              unsigned (&w)[32]) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    w[j] = pack2(v[2 * j] * inv * fs[2 * j], v[2 * j + 1] * inv * fs[2 * j + 1]);
+}
+
+// The offset part of a row (columns 192..207): t - 1/2 for the three canonical offsets, zeros.
+__device__ __forceinline__ void tail_features(const float* tc, unsigned (&w)[8]) {
+  w[0] = pack2(tc[0] - 0.5f, tc[1] - 0.5f);
+  w[1] = pack2(tc[2] - 0.5f, 0.f);
+#pragma unroll
+  for (int j = 2; j < 8; ++j) w[j] = 0u;
+}
+
+// Thread-per-point features (training samples): st is a 192-float scratch.  Returns the scale;
+// tric (grid frame), the canonical tricubic value and the frame code come back through the
+// arguments.
+template <typename T>
+__device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, int N, double L, double px, double py,
+                                                double pz, const float* __restrict__ params, float* st, bf16* row,
+                                                float* tric_grid, int& code, float* tric_can) {
+  PtFrame f;
+  point_frame(px, py, pz, N, L, f);
+  for (int tap = 0; tap < 64; ++tap) canon_tap<T, 64>(u4, N, f.i, f.code, tap, st);
+  float wh[3][4];
+  tric_weights(f.tc, wh);
+  CompSums cs[3];
+  for (int c = 0; c < 3; ++c) {
+    float v[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = st[64 * c + j];
+    comp_transform(v);
+    cs[c] = comp_sums(v, wh);
+#pragma unroll
+    for (int j = 0; j < 64; ++j) st[64 * c + j] = v[j];
+  }
+  const float scale = scale_of(cs[0].ss, cs[1].ss, cs[2].ss, cs[0].sh, cs[1].sh, cs[2].sh, params[OFF_OS + 1]);
   const float inv = 1.f / scale;
-  for (int i = 0; i < 192; ++i) row[i] = __float2bfloat16_rn(st[i] * inv);
-  for (int i = 0; i < 3; ++i) row[192 + i] = __float2bfloat16_rn(toff[i] - 0.5f);
-  for (int i = D_IN; i < K1; ++i) row[i] = __float2bfloat16_rn(0.f);
+  const float* fs = params + OFF_FS;
+  unsigned* rw = reinterpret_cast<unsigned*>(row);
+  for (int c = 0; c < 3; ++c) {
+    float v[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = st[64 * c + j];
+    unsigned w[32];
+    comp_features(v, fs, inv, w);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) rw[32 * c + j] = w[j];
+  }
+  unsigned wt[8];
+  tail_features(f.tc, wt);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) rw[96 + j] = wt[j];
+  code = f.code;
+#pragma unroll
+  for (int cc = 0; cc < 3; ++cc) {
+    tric_can[cc] = cs[cc].tr;
+    const int d = frame_perm(code, cc);
+    tric_grid[d] = frame_sign(code, d) * cs[cc].tr;
+  }
   return scale;
 }
 
@@ -242,64 +404,242 @@ __device__ __forceinline__ void load_weights(const bf16* __restrict__ packed, bf
   for (int i = threadIdx.x; i < N3 * KP2 / 2; i += blockDim.x) d3[i] = src3[i];
 }
 
-constexpr int WARPS = 8;
+// ---- fused-feature inference, in two kernels --------------------------------------------------
+// k_mlp_features: warp per 16 droplets, no weights in shared memory (16 warps per SM to hide the
+// gather latency): canonical-frame stencil gather into shared memory (2 taps per lane per
+// droplet), the three polynomial passes over all lines, one lane per droplet for the scale and
+// the tricubic value, then the feature rows (bf16, K1 per droplet) and the per-droplet aux
+// (tricubic xyz in the grid frame, scale, frame code) to global memory.
+constexpr int FWARPS = 8;
+constexpr int FROWS = 8;              // droplets per warp group; lanes 3r + c (r < 8, c < 3) transform
+constexpr int SCS = 65;               // component stride of the staged taps (= 1 mod 32)
+constexpr int SRS = 3 * SCS;          // droplet stride (= 3 mod 32): the 24 lanes hit distinct banks
+constexpr size_t SMEM_FEAT = sizeof(float) * FWARPS * FROWS * SRS;
+
+// Grid-memory offset of canonical index j along canonical axis k of a point (cell ci, frame code).
+__device__ __forceinline__ long long canon_offset(const int* ci, int code, int N, int k, int j) {
+  const int d = frame_perm(code, k);
+  const int o = (code >> (6 + d)) & 1 ? 3 - j : j;
+  const int cid = d == 0 ? ci[0] : (d == 1 ? ci[1] : ci[2]);
+  const long long g = (cid - 1 + o + N) & (N - 1);
+  return d == 0 ? g * N * N : (d == 1 ? g * N : g);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FWARPS * 32, 2)
+k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __restrict__ pos, long long n,
+               const float* __restrict__ params, bf16* __restrict__ Xg, float* __restrict__ auxg) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* st = reinterpret_cast<float*>(smem_raw) + warp * FROWS * SRS;
+  const float* fs = params + OFF_FS;
+  const float mode = params[OFF_OS + 1];
+  // this lane's taps: lane and lane + 32 (canonical j0 = lane>>4 and 2 + (lane>>4), shared j1, j2)
+  const int j0a = lane >> 4, j1 = (lane >> 2) & 3, j2 = lane & 3;
+  const long long ngroups = (n + FROWS - 1) / FROWS;
+  for (long long grp = (long long)blockIdx.x * FWARPS + warp; grp < ngroups; grp += (long long)gridDim.x * FWARPS) {
+    const long long i0 = grp * FROWS;
+    const int rows = (int)(n - i0 < FROWS ? n - i0 : FROWS);
+    // frame of droplet `lane` (lanes 0..7)
+    PtFrame f;
+    {
+      long long i = i0 + (lane & (FROWS - 1));
+      if (i >= n) i = n - 1;
+      point_frame(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], N, L, f);
+    }
+    // canonical taps of the 8 droplets into shared memory
+#pragma unroll 2
+    for (int r = 0; r < FROWS; ++r) {
+      int ci[3];
+      ci[0] = __shfl_sync(0xffffffffu, f.i[0], r);
+      ci[1] = __shfl_sync(0xffffffffu, f.i[1], r);
+      ci[2] = __shfl_sync(0xffffffffu, f.i[2], r);
+      const int code = __shfl_sync(0xffffffffu, f.code, r);
+      const long long o12 = canon_offset(ci, code, N, 1, j1) + canon_offset(ci, code, N, 2, j2);
+      const vec4<T> va = u4[canon_offset(ci, code, N, 0, j0a) + o12];
+      const vec4<T> vb = u4[canon_offset(ci, code, N, 0, j0a + 2) + o12];
+      float* sr = st + r * SRS;
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        const int d = frame_perm(code, cc);
+        const float sg = frame_sign(code, d);
+        const float xa = d == 0 ? float(va.x) : (d == 1 ? float(va.y) : float(va.z));
+        const float xb = d == 0 ? float(vb.x) : (d == 1 ? float(vb.y) : float(vb.z));
+        sr[cc * SCS + lane] = sg * xa;
+        sr[cc * SCS + lane + 32] = sg * xb;
+      }
+    }
+    __syncwarp();
+    // lane 3r + c: component c of droplet r
+    const int r = lane / 3, c = lane - 3 * (lane / 3);
+    const int rr = r < FROWS ? r : FROWS - 1;
+    float tc[3];
+    tc[0] = __shfl_sync(0xffffffffu, f.tc[0], rr);
+    tc[1] = __shfl_sync(0xffffffffu, f.tc[1], rr);
+    tc[2] = __shfl_sync(0xffffffffu, f.tc[2], rr);
+    const int code = __shfl_sync(0xffffffffu, f.code, rr);
+    float v[64];
+    const float* sv = st + rr * SRS + c * SCS;
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = sv[j];
+    comp_transform(v);
+    float wh[3][4];
+    tric_weights(tc, wh);
+    const CompSums cs = comp_sums(v, wh);
+    // the droplet's three components: lanes 3r, 3r+1, 3r+2
+    const int b0 = 3 * rr;
+    const float ss0 = __shfl_sync(0xffffffffu, cs.ss, b0), ss1 = __shfl_sync(0xffffffffu, cs.ss, b0 + 1),
+                ss2 = __shfl_sync(0xffffffffu, cs.ss, b0 + 2);
+    const float sh0 = __shfl_sync(0xffffffffu, cs.sh, b0), sh1 = __shfl_sync(0xffffffffu, cs.sh, b0 + 1),
+                sh2 = __shfl_sync(0xffffffffu, cs.sh, b0 + 2);
+    const float tr1 = __shfl_sync(0xffffffffu, cs.tr, b0 + 1), tr2 = __shfl_sync(0xffffffffu, cs.tr, b0 + 2);
+    const float scale = scale_of(ss0, ss1, ss2, sh0, sh1, sh2, mode);
+    if (r < rows) {
+      unsigned w[32];
+      comp_features(v, fs, 1.f / scale, w);
+      uint4* dst = reinterpret_cast<uint4*>(Xg + (i0 + r) * K1 + 64 * c);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+      if (c == 0) {
+        unsigned wt[8];
+        tail_features(tc, wt);
+        uint4* dt = reinterpret_cast<uint4*>(Xg + (i0 + r) * K1 + 192);
+        dt[0] = make_uint4(wt[0], wt[1], wt[2], wt[3]);
+        dt[1] = make_uint4(wt[4], wt[5], wt[6], wt[7]);
+        const float trc[3] = {cs.tr, tr1, tr2};
+        float* ax = auxg + (i0 + r) * 8;
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const int d = frame_perm(code, cc);
+          const float val = frame_sign(code, d) * trc[cc];
+          if (d == 0) ax[0] = val;
+          else if (d == 1) ax[1] = val;
+          else ax[2] = val;
+        }
+        ax[3] = scale;
+        ax[4] = __int_as_float(code);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Warp GEMM over RG row groups of 16 (rows 16*rg.. of A) sharing every B fragment load.
+template <int RG, int NT, int K>
+__device__ __forceinline__ void warp_gemm_rg(float (*acc)[NT][4], const bf16* A, int lda, const bf16* Bt, int ldb,
+                                             int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int r = 0; r < RG; ++r)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) acc[r][nt][0] = acc[r][nt][1] = acc[r][nt][2] = acc[r][nt][3] = 0.f;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    unsigned a[RG][4];
+#pragma unroll
+    for (int r = 0; r < RG; ++r) {
+      const bf16* Ar = A + 16 * r * lda;
+      a[r][0] = *reinterpret_cast<const unsigned*>(Ar + g * lda + k0 + 2 * t);
+      a[r][1] = *reinterpret_cast<const unsigned*>(Ar + (g + 8) * lda + k0 + 2 * t);
+      a[r][2] = *reinterpret_cast<const unsigned*>(Ar + g * lda + k0 + 8 + 2 * t);
+      a[r][3] = *reinterpret_cast<const unsigned*>(Ar + (g + 8) * lda + k0 + 8 + 2 * t);
+    }
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      unsigned bb[2];
+      const bf16* bp = Bt + (nt * 8 + g) * ldb + k0 + 2 * t;
+      bb[0] = *reinterpret_cast<const unsigned*>(bp);
+      bb[1] = *reinterpret_cast<const unsigned*>(bp + 8);
+#pragma unroll
+      for (int r = 0; r < RG; ++r) mma16816(acc[r][nt], a[r], bb);
+    }
+  }
+}
+
+// bias + SiLU of a 2 x 16-row accumulator tile into bf16 rows of `h` (stride KP2)
+__device__ __forceinline__ void act_store(float (*acc)[16][4], const float* __restrict__ bias, bf16* h, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int nt = 0; nt < 16; ++nt) {
+      const int c = nt * 8 + 2 * t;
+      const float b0 = bias[c], b1v = bias[c + 1];
+      bf16* hr = h + 16 * r * KP2;
+      *reinterpret_cast<unsigned*>(hr + g * KP2 + c) = pack2(silu(acc[r][nt][0] + b0), silu(acc[r][nt][1] + b1v));
+      *reinterpret_cast<unsigned*>(hr + (g + 8) * KP2 + c) =
+          pack2(silu(acc[r][nt][2] + b0), silu(acc[r][nt][3] + b1v));
+    }
+}
+
+// k_mlp_forward: persistent CTAs (6 warps) with the packed weights in shared memory; each warp takes
+// tiles of 32 feature rows (copied in with 16-byte loads) and runs the three layers with every
+// weight fragment feeding both 16-row groups; out = tricubic + scale * os * MLP in the grid frame.
+constexpr int WARPS = 6;
+constexpr int IROWS = 32;
 constexpr size_t SMEM_W = sizeof(bf16) * ((size_t)H * KP1 + (size_t)H * KP2 + (size_t)N3 * KP2);
-constexpr size_t SMEM_TILE_INFER = sizeof(bf16) * (16 * XP + 2 * 16 * KP2) + sizeof(float) * (16 * 4);
+constexpr size_t SMEM_X = sizeof(bf16) * IROWS * XP;      // X rows, then h2 (layer 1 has consumed X)
+constexpr size_t SMEM_H = sizeof(bf16) * IROWS * KP2;     // h1
+constexpr size_t SMEM_TILE_INFER = SMEM_X + SMEM_H;
 constexpr size_t SMEM_INFER = SMEM_W + WARPS * SMEM_TILE_INFER;
 
-// ---- fused inference: gather + tricubic + MLP ---------------------------------------------------
-// u4: interleaved (N,N,N,4) velocity; pos (n,3) -> out (n,3) = tricubic + scale * MLP.
 template <typename T>
 __global__ void __launch_bounds__(WARPS * 32)
-k_mlp_infer(const vec4<T>* __restrict__ u4, int N, double L, const double* __restrict__ pos, long long n,
-            const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out) {
+k_mlp_forward(const bf16* __restrict__ Xg, const float* __restrict__ auxg, long long n,
+              const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   bf16* s_w1t = reinterpret_cast<bf16*>(smem_raw);
   bf16* s_w2t = s_w1t + H * KP1;
   bf16* s_w3t = s_w2t + H * KP2;
-  unsigned char* tiles = smem_raw + SMEM_W;
   load_weights(packed, s_w1t, s_w2t, s_w3t);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* mine = tiles + warp * SMEM_TILE_INFER;
+  unsigned char* mine = smem_raw + SMEM_W + warp * SMEM_TILE_INFER;
   bf16* X = reinterpret_cast<bf16*>(mine);
-  bf16* h1 = X + 16 * XP;
-  bf16* h2 = h1 + 16 * KP2;
-  float* aux = reinterpret_cast<float*>(h2 + 16 * KP2);  // [16][4]: tricubic xyz, scale
-  MlpSmemW w{s_w1t, s_w2t, s_w3t, params};
-  const long long ntiles = (n + 15) / 16;
+  bf16* h1 = reinterpret_cast<bf16*>(mine + SMEM_X);
+  bf16* h2 = X;
+  const float os = params[OFF_OS];
+  const long long ntiles = (n + IROWS - 1) / IROWS;
   for (long long tile = (long long)blockIdx.x * WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * WARPS) {
-    // gather: lanes 0..15 build one row each
-    if (lane < 16) {
-      const long long i = tile * 16 + lane;
-      float st[192], tric[3], toff[3];
-      if (i < n) {
-        stencil_point<T>(u4, N, L, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], st, tric, toff);
-      } else {
-        for (int q = 0; q < 192; ++q) st[q] = 0.f;
-        tric[0] = tric[1] = tric[2] = 0.f;
-        toff[0] = toff[1] = toff[2] = 0.5f;
-      }
-      const float scale = features_row(st, toff, X + lane * XP);
-      aux[lane * 4 + 0] = tric[0];
-      aux[lane * 4 + 1] = tric[1];
-      aux[lane * 4 + 2] = tric[2];
-      aux[lane * 4 + 3] = scale;
+    // 32 rows x 26 chunks of 16 bytes, all in flight at once (cp.async); rows past n repeat row n-1
+    for (int e = lane; e < IROWS * (K1 / 8); e += 32) {
+      const int r = e / (K1 / 8), q = e - r * (K1 / 8);
+      long long i = tile * IROWS + r;
+      if (i >= n) i = n - 1;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(X + r * XP + 8 * q);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(Xg + i * K1 + 8 * q) : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncwarp();
-    float y[4];
-    tile_forward(X, h1, h2, nullptr, nullptr, w, params, y, lane);
+    {
+      float acc[2][16][4];
+      warp_gemm_rg<2, 16, K1>(acc, X, XP, s_w1t, KP1, lane);
+      act_store(acc, params + OFF_B1, h1, lane);
+      __syncwarp();
+      warp_gemm_rg<2, 16, H>(acc, h1, KP2, s_w2t, KP2, lane);
+      act_store(acc, params + OFF_B2, h2, lane);
+      __syncwarp();
+    }
+    float a3[2][1][4];
+    warp_gemm_rg<2, 1, H>(a3, h2, KP2, s_w3t, KP2, lane);
     const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = g + 8 * h;
-      const long long i = tile * 16 + r;
+    for (int r = 0; r < 2; ++r)
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const int c = 2 * t + q;
-        if (i < n && c < D_OUT) out[3 * i + c] = T(aux[r * 4 + c] + aux[r * 4 + 3] * y[2 * h + q]);
+      for (int hh = 0; hh < 2; ++hh) {
+        const long long i = tile * IROWS + 16 * r + g + 8 * hh;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int c = 2 * t + q;  // canonical component
+          if (i < n && c < D_OUT) {
+            const float* ax = auxg + i * 8;
+            const int code = __float_as_int(ax[4]);
+            const int cg = frame_perm(code, c);
+            const float y = a3[r][0][2 * hh + q] + params[OFF_B3 + c];
+            out[3 * i + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
+          }
+        }
       }
-    }
     __syncwarp();
   }
 }
@@ -307,25 +647,29 @@ k_mlp_infer(const vec4<T>* __restrict__ u4, int N, double L, const double* __res
 // ---- training samples ------------------------------------------------------------------------------
 // For sample s: point = grid point idx[s] + shift (in grid units), exact velocity = ue (planar
 // (3, N^3)) at idx[s] (ue is the field phase-shifted by `shift`), features from the unshifted
-// interleaved field u4.  Writes X row, target T = (exact - tricubic)/scale, tricubic and scale.
+// interleaved field u4.  Writes X row, target T = (exact - tricubic)/(scale os) in the point's
+// canonical frame, tricubic (grid frame) and scale.
 template <typename T>
 __global__ void k_mlp_samples(const vec4<T>* __restrict__ u4, const T* __restrict__ ue, int N, double L,
                               const long long* __restrict__ idx, long long ns, double sx, double sy, double sz,
-                              bf16* __restrict__ X, float* __restrict__ Tg, float* __restrict__ aux) {
+                              const float* __restrict__ params, bf16* __restrict__ X, float* __restrict__ Tg,
+                              float* __restrict__ aux) {
   const long long N3g = (long long)N * N * N;
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < ns; s += (long long)gridDim.x * blockDim.x) {
     const long long j = idx[s];
     const long long jx = j / ((long long)N * N), jy = (j / N) % N, jz = j % N;
     const double dx = L / N;
     const double px = (jx + sx) * dx, py = (jy + sy) * dx, pz = (jz + sz) * dx;
-    float st[192], tric[3], toff[3];
-    stencil_point<T>(u4, N, L, px, py, pz, st, tric, toff);
-    const float scale = features_row(st, toff, X + s * K1);
-    for (int c = 0; c < 3; ++c) {
-      const float ex = float(ue[c * N3g + j]);
-      Tg[s * 3 + c] = (ex - tric[c]) / scale;
-      aux[s * 4 + c] = tric[c];
+    float st[192], tric[3], tric_can[3];
+    int code;
+    const float scale = point_features<T>(u4, N, L, px, py, pz, params, st, X + s * K1, tric, code, tric_can);
+    const float os = params[OFF_OS];
+    for (int cc = 0; cc < 3; ++cc) {  // target in the canonical frame
+      const int cg = frame_perm(code, cc);
+      const float ex = frame_sign(code, cg) * float(ue[cg * N3g + j]);
+      Tg[s * 3 + cc] = (ex - tric_can[cc]) / (scale * os);
     }
+    for (int c = 0; c < 3; ++c) aux[s * 4 + c] = tric[c];
     aux[s * 4 + 3] = scale;
   }
 }
@@ -359,7 +703,8 @@ constexpr size_t SMEM_TRAIN = sizeof(bf16) * ((size_t)TB * XP + 2 * (size_t)TB *
                               sizeof(float) * (2 * (size_t)TB * H + (size_t)TB * 4);
 
 __global__ void __launch_bounds__(TWARPS * 32)
-k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, long long nb, float inv_norm,
+k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, const float* __restrict__ Wg, long long nb,
+            float inv_norm,
             const bf16* __restrict__ packed, const float* __restrict__ params, float* __restrict__ gpart,
             float* __restrict__ lpart) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -389,7 +734,7 @@ k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, long long
   float y[4];
   const int rw = warp * 16;
   tile_forward(X + rw * XP, h1 + rw * KP2, h2 + rw * KP2, z1 + rw * H, z2 + rw * H, w, params, y, lane);
-  // dY = 2 (Y - T) / B on valid rows (zero elsewhere); loss partial
+  // dY = 2 w (Y - T) / B on valid rows (zero elsewhere); loss partial
   float lsum = 0.f;
 #pragma unroll
   for (int hh = 0; hh < 2; ++hh) {
@@ -400,8 +745,9 @@ k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, long long
       float d = 0.f;
       if (c < D_OUT && r0 + r < nb) {
         const float e = y[2 * hh + q] - Tg[(r0 + r) * 3 + c];
-        lsum += e * e;
-        d = 2.f * e * inv_norm;
+        const float wr = Wg ? Wg[r0 + r] : 1.f;
+        lsum += wr * e * e;
+        d = 2.f * e * wr * inv_norm;
       }
       if (c < 4) dy[r * 4 + c] = d;
     }
@@ -482,6 +828,7 @@ k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, long long
     for (int r = 0; r < TB; ++r) s += z1[r * H + o];
     G[OFF_B1 + o] = s;
   }
+  for (int e = OFF_FS + threadIdx.x; e < N_PARAMS; e += blockDim.x) G[e] = 0.f;  // scales are not trained
   if (threadIdx.x == 0) {
     float l = 0.f;
     for (int q = 0; q < TWARPS; ++q) l += lw[q];
@@ -508,6 +855,7 @@ __global__ void k_mlp_reduce(const float* __restrict__ gpart, const float* __res
 __global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                            float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x) {
+    if (e >= OFF_FS) continue;  // feature and output scales: fixed
     bool pad = false;
     if (e < OFF_B1) pad = (e - OFF_W1) / H >= D_IN;
     else if (e >= OFF_W3 && e < OFF_B3) pad = (e - OFF_W3) % N3 >= D_OUT;
@@ -595,24 +943,53 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
     return ld_fail(LD_ERR_ARG, "ld_mlp_infer: bad arguments");
   if (n == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  ProfScope ps(p, KID_MLP_INFER, s);
   const double L = 2.0 * M_PI;
-  long long tiles = (n + 15) / 16;
-  long long grid = (tiles + WARPS - 1) / WARPS;
-  if (grid > 148 * 2) grid = 148 * 2;
   static_assert(SMEM_INFER <= 227 * 1024, "inference tile exceeds shared memory");
-  if (p->prec == LD_F32) {
-    auto k = k_mlp_infer<float>;
-    LD_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_INFER));
-    k<<<(unsigned)grid, WARPS * 32, SMEM_INFER, s>>>((const float4*)u4, p->N, L, pos, n, (const bf16*)packed,
-                                                       params, (float*)out);
-  } else {
-    auto k = k_mlp_infer<double>;
-    LD_CUDA_CHECK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_INFER));
-    k<<<(unsigned)grid, WARPS * 32, SMEM_INFER, s>>>((const double4*)u4, p->N, L, pos, n, (const bf16*)packed,
-                                                       params, (double*)out);
+  // feature rows and aux live in the plan's transform workspace (idle during droplet stages):
+  // droplets are taken in batches that fit it
+  const size_t per = sizeof(bf16) * K1 + sizeof(float) * 8;
+  long long cap = (long long)(p->work_bytes / per);
+  cap -= cap % 32;
+  if (cap < 32) return ld_fail(LD_ERR_CAPACITY, "ld_mlp_infer: no workspace");
+  bf16* X = (bf16*)p->work;
+  for (long long b0 = 0; b0 < n; b0 += cap) {
+    const long long nb = n - b0 < cap ? n - b0 : cap;
+    float* aux = (float*)((char*)p->work + sizeof(bf16) * K1 * nb);
+    const long long groups = (nb + FROWS - 1) / FROWS;
+    long long gf = (groups + FWARPS - 1) / FWARPS;
+    if (gf > 148LL * 4 * 4) gf = 148LL * 4 * 4;
+    const long long tiles = (nb + IROWS - 1) / IROWS;
+    long long gm = (tiles + WARPS - 1) / WARPS;
+    if (gm > 148) gm = 148;  // one CTA per SM (shared memory), persistent warps
+    if (p->prec == LD_F32) {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_FEAT));
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_INFER));
+      {
+        ProfScope ps(p, KID_MLP_FEAT, s);
+        k_mlp_features<float><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const float4*)u4, p->N, L,
+                                                                          pos + 3 * b0, nb, params, X, aux);
+      }
+      ProfScope ps(p, KID_MLP_INFER, s);
+      k_mlp_forward<float><<<(unsigned)gm, WARPS * 32, SMEM_INFER, s>>>(X, aux, nb, (const bf16*)packed, params,
+                                                                        (float*)out + 3 * b0);
+    } else {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_FEAT));
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_INFER));
+      {
+        ProfScope ps(p, KID_MLP_FEAT, s);
+        k_mlp_features<double><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const double4*)u4, p->N, L,
+                                                                            pos + 3 * b0, nb, params, X, aux);
+      }
+      ProfScope ps(p, KID_MLP_INFER, s);
+      k_mlp_forward<double><<<(unsigned)gm, WARPS * 32, SMEM_INFER, s>>>(X, aux, nb, (const bf16*)packed, params,
+                                                                         (double*)out + 3 * b0);
+    }
+    LD_LAUNCH_CHECK();
   }
-  LD_LAUNCH_CHECK();
   return LD_OK;
 }
 
@@ -632,18 +1009,19 @@ int ld_phase_shift(ld_plan* p, const void* uk, void* out, double sx, double sy, 
 }
 
 int ld_mlp_samples(ld_plan* p, const void* u4, const void* ue, const int64_t* idx, int64_t ns, double sx, double sy,
-                   double sz, void* X, float* T, float* aux, void* stream) {
-  if (!p || !u4 || !ue || ns < 0 || (ns > 0 && (!idx || !X || !T || !aux)))
+                   double sz, const float* params, void* X, float* T, float* aux, void* stream) {
+  if (!p || !u4 || !ue || ns < 0 || (ns > 0 && (!idx || !params || !X || !T || !aux)))
     return ld_fail(LD_ERR_ARG, "ld_mlp_samples: bad arguments");
   if (ns == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;
   if (p->prec == LD_F32)
     k_mlp_samples<float><<<gridn(ns, 128), 128, 0, s>>>((const float4*)u4, (const float*)ue, p->N, L,
-                                                        (const long long*)idx, ns, sx, sy, sz, (bf16*)X, T, aux);
+                                                        (const long long*)idx, ns, sx, sy, sz, params, (bf16*)X, T, aux);
   else
     k_mlp_samples<double><<<gridn(ns, 128), 128, 0, s>>>((const double4*)u4, (const double*)ue, p->N, L,
-                                                         (const long long*)idx, ns, sx, sy, sz, (bf16*)X, T, aux);
+                                                         (const long long*)idx, ns, sx, sy, sz, params, (bf16*)X, T,
+                                                         aux);
   LD_LAUNCH_CHECK();
   return LD_OK;
 }
@@ -710,8 +1088,8 @@ int ld_droplet_update(ld_plan* p, int stage, const void* up, double* pos, void* 
 
 int64_t ld_mlp_partial_floats(int64_t nb) { return ((nb + TB - 1) / TB) * (int64_t)(N_PARAMS + 1); }
 
-int ld_mlp_grad(const void* X, const float* T, int64_t nb, const float* params, const void* packed, float* work,
-                float* grad, float* loss, void* stream) {
+int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb, const float* params, const void* packed,
+                float* work, float* grad, float* loss, void* stream) {
   if (!X || !T || nb < 1 || !params || !packed || !work || !grad || !loss)
     return ld_fail(LD_ERR_ARG, "ld_mlp_grad: bad arguments");
   cudaStream_t s = (cudaStream_t)stream;
@@ -720,8 +1098,8 @@ int ld_mlp_grad(const void* X, const float* T, int64_t nb, const float* params, 
   float* lpart = work + (long long)nblk * N_PARAMS;
   const float inv_norm = 1.f / (float)nb;
   LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN));
-  k_mlp_train<<<nblk, TWARPS * 32, SMEM_TRAIN, s>>>((const bf16*)X, T, nb, inv_norm, (const bf16*)packed, params,
-                                                    gpart, lpart);
+  k_mlp_train<<<nblk, TWARPS * 32, SMEM_TRAIN, s>>>((const bf16*)X, T, W, nb, inv_norm, (const bf16*)packed,
+                                                    params, gpart, lpart);
   k_mlp_reduce<<<gridn(N_PARAMS, 256), 256, 0, s>>>(gpart, lpart, nblk, grad, loss, inv_norm);
   LD_LAUNCH_CHECK();
   return LD_OK;

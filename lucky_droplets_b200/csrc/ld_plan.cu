@@ -47,7 +47,7 @@ void ld_prof_end(ld_plan* p, cudaStream_t s) {
 
 static const char* const kKernelNames[] = {
     "xinv", "yinv", "zcross", "yfwd", "xfwd_update", "forcing", "epilogue", "droplet1", "droplet2", "gather",
-    "z_c2r", "z_r2c", "xpass", "ypass", "convert", "shell", "ifac", "exact_sum", "collide_sort", "collide_pairs", "cell_order", "mlp_infer"};
+    "z_c2r", "z_r2c", "xpass", "ypass", "convert", "shell", "ifac", "exact_sum", "collide_sort", "collide_pairs", "cell_order", "mlp_infer", "mlp_features"};
 
 namespace {
 

@@ -6,7 +6,10 @@ drives the kernels of csrc/ld_mlp.cu:
 * ``make_samples``: training pairs from a DNS state.  For a random sub-grid shift s, the spectrum
   is phase-shifted by exp(i k.s dx) and inverse-transformed: the result at grid point j is the
   exact spectral velocity at x_j + s dx.  Random grid points j of that field give exact targets at
-  uniformly distributed points; features come from the unshifted grid.
+  uniformly distributed points; features come from the unshifted grid.  Each sample carries the
+  weight scale^2, so that the weighted loss on normalised targets is the mean squared velocity
+  error the judge measures.
+* ``calibrate``: fixes the feature and output scales from samples (before training).
 * ``train``: Adam on mini-batches with the project's forward/backward kernels.
 * ``infer``: fused stencil gather + tricubic + MLP correction at droplet positions.
 * ``judge``: relative L2 error against the exact direct Fourier sum (``Plan.exact_sum``) on a
@@ -42,12 +45,18 @@ OFF_W2 = OFF_B1 + H
 OFF_B2 = OFF_W2 + H * H
 OFF_W3 = OFF_B2 + H
 OFF_B3 = OFF_W3 + H * N3
-N_PARAMS = OFF_B3 + N3
+OFF_FS = OFF_B3 + N3       # 64 feature scales (per polynomial coefficient, shared by components)
+OFF_OS = OFF_FS + 64       # output scale, then the scale mode (0: all coefficients, 1: order >= 3)
+N_PARAMS = OFF_OS + 8
 
 
-def flat_from_mats(W1, b1, W2, b2, W3, b3):
-    """(195,128),(128),(128,128),(128),(128,3),(3) -> the flat padded parameter vector."""
+def flat_from_mats(W1, b1, W2, b2, W3, b3, fs=None, os=1.0, scale_mode=1):
+    """(195,128),(128),(128,128),(128),(128,3),(3) [+ feature scales (64), output scale] -> the
+    flat padded parameter vector."""
     p = np.zeros(N_PARAMS, np.float32)
+    p[OFF_FS:OFF_FS + 64] = 1.0 if fs is None else fs
+    p[OFF_OS] = os
+    p[OFF_OS + 1] = scale_mode
     p[OFF_W1:OFF_B1].reshape(K1, H)[:D_IN] = W1
     p[OFF_B1:OFF_W2] = b1
     p[OFF_W2:OFF_B2] = np.asarray(W2).reshape(-1)
@@ -61,10 +70,11 @@ def mats_from_flat(p):
     p = np.asarray(p, np.float32)
     return dict(W1=p[OFF_W1:OFF_B1].reshape(K1, H)[:D_IN].copy(), b1=p[OFF_B1:OFF_W2].copy(),
                 W2=p[OFF_W2:OFF_B2].reshape(H, H).copy(), b2=p[OFF_B2:OFF_W3].copy(),
-                W3=p[OFF_W3:OFF_B3].reshape(H, N3)[:, :D_OUT].copy(), b3=p[OFF_B3:OFF_B3 + D_OUT].copy())
+                W3=p[OFF_W3:OFF_B3].reshape(H, N3)[:, :D_OUT].copy(), b3=p[OFF_B3:OFF_B3 + D_OUT].copy(),
+                fs=p[OFF_FS:OFF_FS + 64].copy(), os=float(p[OFF_OS]), scale_mode=int(p[OFF_OS + 1]))
 
 
-def init_flat(seed=0):
+def init_flat(seed=0, scale_mode=1):
     """He-uniform initial weights, zero biases, a small last layer."""
     rng = np.random.default_rng(seed)
 
@@ -75,19 +85,19 @@ def init_flat(seed=0):
     W1, b1 = lin(D_IN, H)
     W2, b2 = lin(H, H)
     W3, b3 = lin(H, D_OUT)
-    return flat_from_mats(W1, b1, W2, b2, 0.1 * W3, b3)
+    return flat_from_mats(W1, b1, W2, b2, 0.1 * W3, b3, scale_mode=scale_mode)
 
 
 class LearnedInterp:
     """MLP parameters, optimiser state and packed weights on one device."""
 
-    def __init__(self, plan, seed=0, params=None, tol=1e-4):
+    def __init__(self, plan, seed=0, params=None, tol=1e-4, scale_mode=1):
         torch = _torch()
         n_params, n_packed, k_in, tile = sizes()
         assert n_params == N_PARAMS and k_in == K1
         self.plan = plan
         dev = plan.device
-        flat = init_flat(seed) if params is None else np.asarray(params, np.float32)
+        flat = init_flat(seed, scale_mode) if params is None else np.asarray(params, np.float32)
         self.params = torch.as_tensor(flat).to(dev).contiguous()
         self.packed = torch.empty(n_packed, dtype=torch.bfloat16, device=dev)
         self.m = torch.zeros_like(self.params)
@@ -124,9 +134,10 @@ class LearnedInterp:
         check(_lib.lib().ld_interleave3(p.handle, ptr(u), ptr(u4), stream_ptr()))
         return u4
 
-    def make_samples(self, uk, n_shifts, per_shift, seed=0, X=None, T=None, offset=0):
+    def make_samples(self, uk, n_shifts, per_shift, seed=0, X=None, T=None, W=None, offset=0):
         """Training pairs from a cube-layout spectrum: n_shifts random sub-grid shifts, per_shift
-        random grid points each.  Returns (X bf16 (ns, 208), T (ns,3), aux (ns,4))."""
+        random grid points each, written at rows offset.. of X, T, W (allocated when X is None).
+        Returns (X bf16 (ns, 208), T (ns,3), W (ns) = scale^2, aux (ns,4) of this call)."""
         torch = _torch()
         p = self.plan
         ns = n_shifts * per_shift
@@ -134,6 +145,7 @@ class LearnedInterp:
         if X is None:
             X = torch.empty((ns, K1), dtype=torch.bfloat16, device=p.device)
             T = torch.empty((ns, 3), dtype=torch.float32, device=p.device)
+            W = torch.empty(ns, dtype=torch.float32, device=p.device)
             offset = 0
         aux = torch.empty((ns, 4), dtype=torch.float32, device=p.device)
         u4 = self.interleaved(uk)
@@ -147,30 +159,64 @@ class LearnedInterp:
             idx = torch.as_tensor(rng.integers(0, p.N ** 3, per_shift, dtype=np.int64)).to(p.device)
             a = offset + i * per_shift
             check(L.ld_mlp_samples(p.handle, ptr(u4), ptr(ue), ptr(idx), per_shift, float(s[0]), float(s[1]),
-                                   float(s[2]), ptr(X[a:a + per_shift]), ptr(T[a:a + per_shift]),
+                                   float(s[2]), ptr(self.params), ptr(X[a:a + per_shift]), ptr(T[a:a + per_shift]),
                                    ptr(aux[i * per_shift:(i + 1) * per_shift]), stream_ptr()))
-        return X, T, aux
+        if W is not None:
+            W[offset:offset + ns] = aux[:, 3].square()
+        return X, T, W, aux
+
+    def calibrate(self, uk, n_shifts=16, per_shift=8192, seed=12345):
+        """Set the feature scales (each polynomial coefficient to unit RMS) and the output scale
+        (targets to unit RMS) from samples of a cube-layout spectrum.  Call before generating the
+        training set; the scales are then fixed."""
+        torch = _torch()
+        X, T, W, _ = self.make_samples(uk, n_shifts, per_shift, seed=seed)
+        f = X[:, :192].float().view(-1, 3, 64)
+        rms = f.pow(2).mean(dim=(0, 1)).sqrt().clamp_min(1e-30)
+        # output scale: RMS of the targets with the training weights
+        t_rms = float(((T.square().sum(1) * W).sum() / (3 * W.sum())).sqrt().clamp_min(1e-30))
+        self.params[OFF_FS:OFF_FS + 64].div_(rms)
+        self.params[OFF_OS] *= t_rms
+        check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
+        del X, T, W, f
+        torch.cuda.synchronize(self.plan.device)
+        return rms.cpu().numpy(), t_rms
+
+    def normalise_targets(self, T, W):
+        """Rescale a generated training set so that its weighted target RMS is 1, moving the
+        factor into the output scale (targets drift while a flow develops)."""
+        r = float(((T.square().sum(1) * W).sum() / (3 * W.sum())).sqrt().clamp_min(1e-30))
+        T.div_(r)
+        self.params[OFF_OS] *= r
+        check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
+        return r
 
     # ---- training ---------------------------------------------------------------------------------
-    def loss_and_grad(self, X, T, work=None):
-        """Exact batch loss and gradient (device tensors); deterministic."""
+    def loss_and_grad(self, X, T, W=None, work=None):
+        """Exact batch loss and gradient (device tensors); deterministic.  W: per-sample weights
+        (None: unit weights)."""
         torch = _torch()
         nb = int(X.shape[0])
         L = _lib.lib()
         if work is None:
             work = torch.empty(int(L.ld_mlp_partial_floats(nb)), dtype=torch.float32, device=self.plan.device)
-        check(L.ld_mlp_grad(ptr(X), ptr(T), nb, ptr(self.params), ptr(self.packed), ptr(work), ptr(self.grad),
-                            ptr(self.loss), stream_ptr()))
+        check(L.ld_mlp_grad(ptr(X), ptr(T), ptr(W) if W is not None else None, nb, ptr(self.params),
+                            ptr(self.packed), ptr(work), ptr(self.grad), ptr(self.loss), stream_ptr()))
         return self.loss, self.grad
 
-    def train(self, X, T, epochs=1, batch=4096, lr=1e-3, lr_final=None, seed=0, log_every=0):
-        """Adam over shuffled mini-batches; returns the per-epoch mean loss (host floats)."""
+    def train(self, X, T, W=None, epochs=1, batch=4096, lr=1e-3, lr_final=None, seed=0, log_every=0):
+        """Adam over shuffled mini-batches; returns the per-epoch mean loss (host floats).  W: sample
+        weights, used normalised to mean 1."""
         torch = _torch()
         n = int(X.shape[0])
         L = _lib.lib()
         work = torch.empty(int(L.ld_mlp_partial_floats(batch)), dtype=torch.float32, device=self.plan.device)
         xb = torch.empty((batch, K1), dtype=torch.bfloat16, device=self.plan.device)
         tb = torch.empty((batch, 3), dtype=torch.float32, device=self.plan.device)
+        wn = wb = None
+        if W is not None:
+            wn = (W / W.mean()).contiguous()
+            wb = torch.empty(batch, dtype=torch.float32, device=self.plan.device)
         g = torch.Generator(device="cpu").manual_seed(seed)
         nbatch = max(1, n // batch)
         total = epochs * nbatch
@@ -182,7 +228,9 @@ class LearnedInterp:
                 idx = perm[b * batch:(b + 1) * batch]
                 check(L.ld_permute_rows(ptr(X), ptr(xb), ptr(idx), batch, K1 * 2, stream_ptr()))
                 check(L.ld_permute_rows(ptr(T), ptr(tb), ptr(idx), batch, 12, stream_ptr()))
-                self.loss_and_grad(xb, tb, work)
+                if wn is not None:
+                    check(L.ld_permute_rows(ptr(wn), ptr(wb), ptr(idx), batch, 4, stream_ptr()))
+                self.loss_and_grad(xb, tb, wb, work)
                 acc += self.loss
                 self.step_count += 1
                 k = self.step_count
@@ -193,6 +241,33 @@ class LearnedInterp:
             if log_every and (ep + 1) % log_every == 0:
                 print(f"epoch {ep + 1}: loss {out[-1]:.4e}")
         return out
+
+    def fit(self, snapshots, n_pairs=20_000_000, per_shift=40_000, epochs=16, batch=4096, lr=2e-3, decay=0.8,
+            seed=0, log=None):
+        """Train on DNS snapshots (cube-layout spectra, e.g. every 100 steps of a run): feature
+        scales from the latest snapshot, n_pairs exact-target pairs spread over the snapshots,
+        targets normalised, then ``epochs`` passes of Adam with the learning rate lr * decay^epoch.
+        Returns a summary dict (pairs, per-epoch losses)."""
+        torch = _torch()
+        p = self.plan
+        ns = len(snapshots)
+        n_shifts = max(1, int(n_pairs) // (ns * per_shift))
+        total = ns * n_shifts * per_shift
+        self.calibrate(snapshots[-1], seed=seed + 7)
+        X = torch.empty((total, K1), dtype=torch.bfloat16, device=p.device)
+        T = torch.empty((total, 3), dtype=torch.float32, device=p.device)
+        W = torch.empty(total, dtype=torch.float32, device=p.device)
+        for k, uk in enumerate(snapshots):
+            self.make_samples(uk, n_shifts, per_shift, seed=seed * 1009 + k, X=X, T=T, W=W,
+                              offset=k * n_shifts * per_shift)
+        self.normalise_targets(T, W)
+        losses = []
+        for ep in range(epochs):
+            losses += self.train(X, T, W, epochs=1, batch=batch, lr=lr * decay ** ep, seed=seed * 1009 + ep)
+            if log:
+                log(f"epoch {ep}: weighted loss {losses[-1]:.4e}")
+        del X, T, W
+        return {"pairs": total, "snapshots": ns, "epochs": epochs, "batch": batch, "losses": losses}
 
     # ---- judge ------------------------------------------------------------------------------------
     def judge(self, uk, u4, pos, n_sample=None, seed=0):

@@ -3,7 +3,10 @@
 TEST INFRASTRUCTURE ONLY.
 
 Network: 195 inputs (the 4x4x4 stencil of (u, v, w) in tap order (c, a, b, q) -> c*64 + a*16 + b*4
-+ q, then the three fractional cell offsets) -> 128 SiLU -> 128 SiLU -> 3.  The GPU kernels feed
++ q, transformed per component into the orthonormal discrete polynomial basis of orders 0..3 along
+each axis, divided by the stencil RMS and multiplied by fixed per-coefficient scales; then the
+three fractional cell offsets minus 1/2) -> 128 SiLU -> 128 SiLU -> 3, times a fixed output
+scale.  The GPU kernels feed
 BF16 operands to the tensor cores with FP32 accumulation; this oracle rounds the same operands to
 BF16 (round to nearest even) and accumulates in FP64, so the two agree to FP32 accumulation error.
 """
@@ -21,6 +24,79 @@ def bf16(x):
     out = rounded.astype(np.uint32).view(np.float32).copy()
     out[nan] = np.nan
     return out
+
+
+# orthonormal discrete polynomials on 4 points, orders 0..3 (rows)
+P4 = np.array([[1, 1, 1, 1], [-3, -1, 1, 3], [1, -1, -1, 1], [-1, 3, -3, 1]], np.float64)
+P4 /= np.linalg.norm(P4, axis=1)[:, None]
+
+
+def frames(t):
+    """Canonical frame of each point: reflect every axis whose offset exceeds 1/2, then order the
+    axes by decreasing reflected offset (stable).  Returns (perm (n,3): canonical axis k <- grid
+    axis perm[:, k], refl (n,3) bool per grid axis, tc (n,3) canonical offsets)."""
+    t = np.asarray(t, np.float32)
+    refl = t > np.float32(0.5)
+    r = np.where(refl, np.float32(1) - t, t)
+    n = t.shape[0]
+    perm = np.tile(np.arange(3), (n, 1))
+    for a, b in ((0, 1), (1, 2), (0, 1)):   # the same compare-exchange network as the kernels
+        ra = r[np.arange(n), perm[:, a]]
+        rb = r[np.arange(n), perm[:, b]]
+        sw = rb > ra
+        pa = perm[:, a].copy()
+        perm[sw, a] = perm[sw, b]
+        perm[sw, b] = pa[sw]
+    tc = np.take_along_axis(r, perm, axis=1)
+    return perm, refl, tc
+
+
+def to_canonical(v, perm, refl):
+    """Grid-frame vectors (n,3) -> canonical frame."""
+    sg = np.where(refl, -1.0, 1.0)
+    return np.take_along_axis(v * sg, perm, axis=1)
+
+
+def from_canonical(y, perm, refl):
+    """Canonical-frame vectors (n,3) -> grid frame."""
+    out = np.empty_like(y)
+    np.put_along_axis(out, perm, y, axis=1)
+    return out * np.where(refl, -1.0, 1.0)
+
+
+_ORDER = (np.arange(64) >> 4) + ((np.arange(64) >> 2) & 3) + (np.arange(64) & 3)
+
+
+def features(st, t, fs, scale_mode=1):
+    """Network inputs (n, 195) from stencils st (n, 192), offsets t (n, 3) and feature scales fs
+    (64): returns (X rounded to BF16, scale, perm, refl).  scale: RMS of all coefficients (mode 0)
+    or of those of total order >= 3 (mode 1)."""
+    n = st.shape[0]
+    v = st.reshape(n, 3, 4, 4, 4)
+    d = np.einsum("ia,jb,kq,ncabq->ncijk", P4, P4, P4, v, optimize=True)
+    d64 = d.reshape(n, 3, 64)
+    if scale_mode:
+        scale = np.sqrt((d64[:, :, _ORDER >= 3] ** 2).sum(axis=(1, 2)) / 162.0) + 1e-30
+    else:
+        scale = np.sqrt((st ** 2).mean(axis=1)) + 1e-30
+    perm, refl, tc = frames(t)
+    out = np.empty((n, 3, 4, 4, 4))
+    # reflection of grid axis g multiplies order-j coefficients along g by (-1)^j
+    par = np.array([1.0, -1.0, 1.0, -1.0])
+    for i in range(n):
+        p, rf = perm[i], refl[i]
+        di = d[i]
+        for g in range(3):
+            if rf[g]:
+                shp = [1, 1, 1, 1]
+                shp[1 + g] = 4
+                di = di * par.reshape(shp)
+        di = di * np.where(rf, -1.0, 1.0)[:, None, None, None]      # velocity components
+        di = di[p]                                                  # components to canonical order
+        out[i] = np.transpose(di, (0, 1 + p[0], 1 + p[1], 1 + p[2]))  # coefficient axes
+    dd = out.reshape(n, 3, 64) / scale[:, None, None] * np.asarray(fs, np.float64)[None, None, :]
+    X = np.concatenate([dd.reshape(n, 192), tc - 0.5], axis=1)
+    return bf16(X.astype(np.float32)), scale, perm, refl
 
 
 def silu(z):
@@ -76,13 +152,14 @@ def backward(p, cache, dy, emulate_bf16=True):
     return g
 
 
-def mse_loss_and_grads(p, X, T, emulate_bf16=True):
-    """mean over the batch of |Y - T|^2 and its gradients."""
+def mse_loss_and_grads(p, X, T, emulate_bf16=True, w=None):
+    """sum over the batch of w |Y - T|^2 / B (w = 1 by default) and its gradients."""
     y, cache = forward(p, X, emulate_bf16)
     d = y - T
     B = X.shape[0]
-    loss = float((d ** 2).sum() / B)
-    g = backward(p, cache, 2.0 * d / B, emulate_bf16)
+    w = np.ones(B) if w is None else np.asarray(w, np.float64)
+    loss = float((w[:, None] * d ** 2).sum() / B)
+    g = backward(p, cache, 2.0 * w[:, None] * d / B, emulate_bf16)
     return loss, g
 
 

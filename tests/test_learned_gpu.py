@@ -57,13 +57,11 @@ def test_zero_correction_equals_tricubic(torch, prec):
     assert np.abs(b.pos.cpu().numpy() - a.pos.cpu().numpy()).max() < tol
 
 
-def _oracle_learned(u, pos, p):
+def _oracle_learned(u, pos, p, fs, os):
     st, t = C.stencil_4x4x4(u, pos)
-    s = st.reshape(pos.shape[0], 192)
-    scale = np.sqrt((s ** 2).mean(axis=1)) + 1e-30
-    X = np.concatenate([s / scale[:, None], t - 0.5], axis=1)
+    X, scale, perm, refl = M.features(st.reshape(pos.shape[0], 192), t, fs)
     y, _ = M.forward(p, X)
-    return C.gather(u, pos, "tricubic") + scale[:, None] * y
+    return C.gather(u, pos, "tricubic") + scale[:, None] * os * M.from_canonical(y, perm, refl)
 
 
 def test_learned_step_matches_oracle(torch):
@@ -73,18 +71,19 @@ def test_learned_step_matches_oracle(torch):
     from lucky_droplets_b200 import mlp as G
     prm, grid, uk0, pos, tau, vel, dns = _setup(32, "f32", 4, 2000)
     p = M.init_params(2)
-    p["W3"] *= 0.05
+    fs = np.random.default_rng(5).uniform(0.5, 3.0, 64).astype(np.float32)
+    os = 0.05
     d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g)
-    d.use_learned(G.LearnedInterp(dns.plan, params=G.flat_from_mats(**p)))
+    d.use_learned(G.LearnedInterp(dns.plan, params=G.flat_from_mats(**p, fs=fs, os=os)))
     dns.attach(d)
     uk, x, v = uk0.copy(), pos.copy(), vel.copy()
     h = prm.dt
     for _ in range(2):
         uk_new, u_n, u_s = C.rk2if_step(grid, prm, uk)
-        up1 = _oracle_learned(u_n, x, p)
+        up1 = _oracle_learned(u_n, x, p, fs, os)
         k1x, k1v = C.droplet_rhs(v, up1, tau, prm.g)
         xs, vs = x + h * k1x, v + h * k1v
-        up2 = _oracle_learned(u_s, xs, p)
+        up2 = _oracle_learned(u_s, xs, p, fs, os)
         k2x, k2v = C.droplet_rhs(vs, up2, tau, prm.g)
         x, v = x + 0.5 * h * (k1x + k2x), v + 0.5 * h * (k1v + k2v)
         uk = grid.project(np.stack([grid.rfft(grid.irfft(uk_new[c])) for c in range(3)]))

@@ -35,11 +35,13 @@ def test_gradients_match_oracle(torch):
     p["b3"] = rng.standard_normal(3).astype(np.float32) * 0.1
     plan = Plan(16, "f32")
     li = G.LearnedInterp(plan, params=G.flat_from_mats(p["W1"], p["b1"], p["W2"], p["b2"], p["W3"], p["b3"]))
+    w = rng.uniform(0.1, 3.0, nb).astype(np.float32)
     Xg = torch.as_tensor(X).to("cuda", torch.bfloat16)
     Tg = torch.as_tensor(T).cuda()
-    loss, grad = li.loss_and_grad(Xg, Tg)
+    loss, grad = li.loss_and_grad(Xg, Tg, torch.as_tensor(w).cuda())
     gm = G.mats_from_flat(grad.cpu().numpy())
-    ref_loss, ref = M.mse_loss_and_grads(p, X[:, :M.D_IN], T)
+    assert np.all(gm["fs"] == 0) and gm["os"] == 0  # the scales get no gradient
+    ref_loss, ref = M.mse_loss_and_grads(p, X[:, :M.D_IN], T, w=w)
     assert abs(float(loss.item()) - ref_loss) / ref_loss < 1e-4
     for k in ("W3", "b3", "W2", "b2"):
         assert rel(gm[k], ref[k]) < 2e-3, k
@@ -47,14 +49,12 @@ def test_gradients_match_oracle(torch):
         assert rel(gm[k], ref[k]) < 2e-2, k
 
 
-def _oracle_infer(u, pos, p):
+def _oracle_infer(u, pos, p, fs, os):
     st, t = C.stencil_4x4x4(u, pos)
-    s = st.reshape(pos.shape[0], 192)
-    scale = np.sqrt((s ** 2).mean(axis=1)) + 1e-30
-    X = np.concatenate([s / scale[:, None], t - 0.5], axis=1)
+    X, scale, perm, refl = M.features(st.reshape(pos.shape[0], 192), t, fs)
     y, _ = M.forward(p, X)
     tric = C.gather(u, pos, "tricubic")
-    return tric + scale[:, None] * y, tric
+    return tric + scale[:, None] * os * M.from_canonical(y, perm, refl), tric
 
 
 def test_inference_matches_oracle(torch):
@@ -66,13 +66,15 @@ def test_inference_matches_oracle(torch):
     uk, u = C.init_flow(grid, prm, seed=8)
     plan = Plan(N, "f32")
     p = M.init_params(5)
-    li = G.LearnedInterp(plan, params=G.flat_from_mats(**p))
+    fs = np.random.default_rng(3).uniform(0.5, 3.0, 64).astype(np.float32)
+    os = 0.7
+    li = G.LearnedInterp(plan, params=G.flat_from_mats(**p, fs=fs, os=os))
     cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
     u4 = li.interleaved(cube)
     rng = np.random.default_rng(2)
     pos = rng.uniform(-1, 7.5, (3001, 3))
     got = li.infer(u4, torch.as_tensor(pos).cuda()).cpu().numpy()
-    ref, tric = _oracle_infer(u, pos, p)
+    ref, tric = _oracle_infer(u, pos, p, fs, os)
     # the correction part agrees to FP32/BF16-input accuracy
     assert rel(got - tric, ref - tric) < 5e-3
     assert rel(got, ref) < 1e-4
@@ -114,9 +116,10 @@ def test_training_beats_tricubic(torch):
     plan = Plan(N, "f32")
     li = G.LearnedInterp(plan, seed=1, tol=1e-12)
     cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
-    X, T, _ = li.make_samples(cube, n_shifts=400, per_shift=1024, seed=1)
-    losses = li.train(X, T, epochs=12, batch=4096, lr=2e-3, lr_final=2e-4, seed=0)
-    assert losses[-1] < 0.5 * losses[0]
+    li.calibrate(cube)
+    X, T, W, _ = li.make_samples(cube, n_shifts=400, per_shift=1024, seed=1)
+    losses = li.train(X, T, W, epochs=12, batch=4096, lr=2e-3, lr_final=2e-4, seed=0)
+    assert losses[-1] < 0.8 * losses[0]
     rng = np.random.default_rng(77)
     pos = torch.as_tensor(rng.uniform(0, 2 * np.pi, (4000, 3))).cuda()
     e_learned, e_tric = li.judge(cube, li.interleaved(cube), pos)
