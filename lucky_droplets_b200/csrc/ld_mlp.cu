@@ -391,25 +391,21 @@ __device__ __forceinline__ void tile_forward(const bf16* X, bf16* h1, bf16* h2, 
   y[3] = a3[0][3] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
 }
 
-// Loads the packed forward weights into shared memory (whole CTA).
-__device__ __forceinline__ void load_weights(const bf16* __restrict__ packed, bf16* s_w1t, bf16* s_w2t, bf16* s_w3t) {
-  const unsigned* src1 = reinterpret_cast<const unsigned*>(packed + P_W1T);
-  unsigned* d1 = reinterpret_cast<unsigned*>(s_w1t);
-  for (int i = threadIdx.x; i < H * KP1 / 2; i += blockDim.x) d1[i] = src1[i];
-  const unsigned* src2 = reinterpret_cast<const unsigned*>(packed + P_W2T);
-  unsigned* d2 = reinterpret_cast<unsigned*>(s_w2t);
-  for (int i = threadIdx.x; i < H * KP2 / 2; i += blockDim.x) d2[i] = src2[i];
-  const unsigned* src3 = reinterpret_cast<const unsigned*>(packed + P_W3T);
-  unsigned* d3 = reinterpret_cast<unsigned*>(s_w3t);
-  for (int i = threadIdx.x; i < N3 * KP2 / 2; i += blockDim.x) d3[i] = src3[i];
-}
-
 // ---- fused-feature inference, in two kernels --------------------------------------------------
-// k_mlp_features: warp per 16 droplets, no weights in shared memory (16 warps per SM to hide the
-// gather latency): canonical-frame stencil gather into shared memory (2 taps per lane per
-// droplet), the three polynomial passes over all lines, one lane per droplet for the scale and
-// the tricubic value, then the feature rows (bf16, K1 per droplet) and the per-droplet aux
-// (tricubic xyz in the grid frame, scale, frame code) to global memory.
+// k_mlp_features: warp per 8 droplets, no weights in shared memory: canonical-frame stencil
+// gather into shared memory (2 taps per lane per droplet), then lane 3r + c takes component c
+// of droplet r in registers (polynomial transform, partial sums, 64 features); the feature rows
+// (bf16, K1 per droplet) go to global memory in the tensor-core tile layout (tiles of TM rows,
+// 8x8 core matrices, see blk_off) and the per-droplet aux (tricubic xyz in the grid frame,
+// scale, frame code) as 8 floats.
+// Tensor-core tile layout of a K-major bf16 operand with `rows` rows: 8x8 core matrices (8 rows of
+// 16 bytes, 128 contiguous bytes), K-chunk major: byte offset of (row, 8-element K chunk kc).
+__host__ __device__ constexpr int blk_off(int row, int kc, int rows) {
+  return (kc * (rows / 8) + row / 8) * 128 + (row % 8) * 16;
+}
+constexpr int TM = 128;                             // droplets per tensor-core tile
+constexpr int TILE_X_BYTES = TM * K1 * 2;           // one tile of feature rows
+
 constexpr int FWARPS = 8;
 constexpr int FROWS = 8;              // droplets per warp group; lanes 3r + c (r < 8, c < 3) transform
 constexpr int SCS = 65;               // component stride of the staged taps (= 1 mod 32)
@@ -497,15 +493,18 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
     if (r < rows) {
       unsigned w[32];
       comp_features(v, fs, 1.f / scale, w);
-      uint4* dst = reinterpret_cast<uint4*>(Xg + (i0 + r) * K1 + 64 * c);
+      const long long i = i0 + r;
+      unsigned char* tb = reinterpret_cast<unsigned char*>(Xg) + (i / TM) * TILE_X_BYTES;
+      const int rr = (int)(i % TM);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) dst[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+      for (int q = 0; q < 8; ++q)
+        *reinterpret_cast<uint4*>(tb + blk_off(rr, 8 * c + q, TM)) =
+            make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
       if (c == 0) {
         unsigned wt[8];
         tail_features(tc, wt);
-        uint4* dt = reinterpret_cast<uint4*>(Xg + (i0 + r) * K1 + 192);
-        dt[0] = make_uint4(wt[0], wt[1], wt[2], wt[3]);
-        dt[1] = make_uint4(wt[4], wt[5], wt[6], wt[7]);
+        *reinterpret_cast<uint4*>(tb + blk_off(rr, 24, TM)) = make_uint4(wt[0], wt[1], wt[2], wt[3]);
+        *reinterpret_cast<uint4*>(tb + blk_off(rr, 25, TM)) = make_uint4(wt[4], wt[5], wt[6], wt[7]);
         const float trc[3] = {cs.tr, tr1, tr2};
         float* ax = auxg + (i0 + r) * 8;
 #pragma unroll
@@ -524,124 +523,179 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
   }
 }
 
-// Warp GEMM over RG row groups of 16 (rows 16*rg.. of A) sharing every B fragment load.
-template <int RG, int NT, int K>
-__device__ __forceinline__ void warp_gemm_rg(float (*acc)[NT][4], const bf16* A, int lda, const bf16* Bt, int ldb,
-                                             int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int r = 0; r < RG; ++r)
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) acc[r][nt][0] = acc[r][nt][1] = acc[r][nt][2] = acc[r][nt][3] = 0.f;
-#pragma unroll
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    unsigned a[RG][4];
-#pragma unroll
-    for (int r = 0; r < RG; ++r) {
-      const bf16* Ar = A + 16 * r * lda;
-      a[r][0] = *reinterpret_cast<const unsigned*>(Ar + g * lda + k0 + 2 * t);
-      a[r][1] = *reinterpret_cast<const unsigned*>(Ar + (g + 8) * lda + k0 + 2 * t);
-      a[r][2] = *reinterpret_cast<const unsigned*>(Ar + g * lda + k0 + 8 + 2 * t);
-      a[r][3] = *reinterpret_cast<const unsigned*>(Ar + (g + 8) * lda + k0 + 8 + 2 * t);
-    }
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      unsigned bb[2];
-      const bf16* bp = Bt + (nt * 8 + g) * ldb + k0 + 2 * t;
-      bb[0] = *reinterpret_cast<const unsigned*>(bp);
-      bb[1] = *reinterpret_cast<const unsigned*>(bp + 8);
-#pragma unroll
-      for (int r = 0; r < RG; ++r) mma16816(acc[r][nt], a[r], bb);
-    }
-  }
-}
-
-// bias + SiLU of a 2 x 16-row accumulator tile into bf16 rows of `h` (stride KP2)
-__device__ __forceinline__ void act_store(float (*acc)[16][4], const float* __restrict__ bias, bf16* h, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int r = 0; r < 2; ++r)
-#pragma unroll
-    for (int nt = 0; nt < 16; ++nt) {
-      const int c = nt * 8 + 2 * t;
-      const float b0 = bias[c], b1v = bias[c + 1];
-      bf16* hr = h + 16 * r * KP2;
-      *reinterpret_cast<unsigned*>(hr + g * KP2 + c) = pack2(silu(acc[r][nt][0] + b0), silu(acc[r][nt][1] + b1v));
-      *reinterpret_cast<unsigned*>(hr + (g + 8) * KP2 + c) =
-          pack2(silu(acc[r][nt][2] + b0), silu(acc[r][nt][3] + b1v));
-    }
-}
-
-// k_mlp_forward: persistent CTAs (6 warps) with the packed weights in shared memory; each warp takes
-// tiles of 32 feature rows (copied in with 16-byte loads) and runs the three layers with every
-// weight fragment feeding both 16-row groups; out = tricubic + scale * os * MLP in the grid frame.
-constexpr int WARPS = 6;
-constexpr int IROWS = 32;
-constexpr size_t SMEM_W = sizeof(bf16) * ((size_t)H * KP1 + (size_t)H * KP2 + (size_t)N3 * KP2);
-constexpr size_t SMEM_X = sizeof(bf16) * IROWS * XP;      // X rows, then h2 (layer 1 has consumed X)
-constexpr size_t SMEM_H = sizeof(bf16) * IROWS * KP2;     // h1
-constexpr size_t SMEM_TILE_INFER = SMEM_X + SMEM_H;
-constexpr size_t SMEM_INFER = SMEM_W + WARPS * SMEM_TILE_INFER;
+// ---- MLP forward on the 5th-generation tensor cores --------------------------------------------
+// Persistent CTA per SM, 8 warps.  Per tile of TM = 128 droplets:
+//   X tile (128 x 208 bf16, tile layout) arrives by one bulk asynchronous copy, double-buffered;
+//   layer 1: 13 tcgen05.mma (M 128, N 128, K 16) from X and W1 into TMEM columns 0..127;
+//   epilogue: 8 warps read the accumulators (tcgen05.ld), add b1, SiLU, bf16 -> H (tile layout);
+//   layer 2: 8 MMAs from H and W2 into TMEM 0..127; epilogue as above -> H;
+//   layer 3: 8 MMAs (N 16: W3 padded) into TMEM 128..143; warps 0..3 write
+//   out = tricubic + scale * os * MLP back in the grid frame.
+// One thread issues the MMAs and commits them to an mbarrier that all threads wait on (bounded:
+// a wait that runs out raises LD_STATUS_WAIT_TIMEOUT and the CTA frees its TMEM and returns).
+constexpr int FT_THREADS = 256;
+constexpr int N3P = 16;                               // layer-3 N padded for M = 128
+constexpr int SM_W1 = 0;
+constexpr int SM_W2 = SM_W1 + H * K1 * 2;             // 53248
+constexpr int SM_W3 = SM_W2 + H * H * 2;              // + 32768
+constexpr int SM_X0 = SM_W3 + N3P * H * 2;            // + 4096
+constexpr int SM_X1 = SM_X0 + TILE_X_BYTES;
+constexpr int SM_H = SM_X1 + TILE_X_BYTES;
+constexpr int SM_BIAS = SM_H + TM * H * 2;            // b1[128], b2[128], b3[16]
+constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma
+constexpr int SM_TMEM = SM_BAR + 3 * 8;
+constexpr size_t SMEM_FWD = SM_TMEM + 16;
+constexpr unsigned TMEM_COLS = 256;
+constexpr unsigned kWaitLimitMlp = 1u << 24;
 
 template <typename T>
-__global__ void __launch_bounds__(WARPS * 32)
-k_mlp_forward(const bf16* __restrict__ Xg, const float* __restrict__ auxg, long long n,
-              const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  bf16* s_w1t = reinterpret_cast<bf16*>(smem_raw);
-  bf16* s_w2t = s_w1t + H * KP1;
-  bf16* s_w3t = s_w2t + H * KP2;
-  load_weights(packed, s_w1t, s_w2t, s_w3t);
+__global__ void __launch_bounds__(FT_THREADS, 1)
+k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__ auxg, long long n,
+                 const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out,
+                 unsigned* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  float* bias = reinterpret_cast<float*>(sm + SM_BIAS);
+  uint64_t* bar_x = reinterpret_cast<uint64_t*>(sm + SM_BAR);
+  uint64_t* bar_mma = bar_x + 2;
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + SM_TMEM);
+  // weights into the tile layout (from the packed, row-padded copies)
+  for (int e = tid; e < H * (K1 / 8); e += FT_THREADS) {
+    const int nrow = e / (K1 / 8), kc = e % (K1 / 8);
+    *reinterpret_cast<uint4*>(sm + SM_W1 + blk_off(nrow, kc, H)) =
+        *reinterpret_cast<const uint4*>(packed + P_W1T + nrow * KP1 + 8 * kc);
+  }
+  for (int e = tid; e < H * (H / 8); e += FT_THREADS) {
+    const int nrow = e / (H / 8), kc = e % (H / 8);
+    *reinterpret_cast<uint4*>(sm + SM_W2 + blk_off(nrow, kc, H)) =
+        *reinterpret_cast<const uint4*>(packed + P_W2T + nrow * KP2 + 8 * kc);
+  }
+  for (int e = tid; e < N3P * (H / 8); e += FT_THREADS) {
+    const int nrow = e / (H / 8), kc = e % (H / 8);
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (nrow < N3) v = *reinterpret_cast<const uint4*>(packed + P_W3T + nrow * KP2 + 8 * kc);
+    *reinterpret_cast<uint4*>(sm + SM_W3 + blk_off(nrow, kc, N3P)) = v;
+  }
+  for (int e = tid; e < 2 * H + N3P; e += FT_THREADS)
+    bias[e] = e < H ? params[OFF_B1 + e] : (e < 2 * H ? params[OFF_B2 + e - H] : (e - 2 * H < N3 ? params[OFF_B3 + e - 2 * H] : 0.f));
+  if (tid == 0) {
+    mbar_init(&bar_x[0], 1);
+    mbar_init(&bar_x[1], 1);
+    mbar_init(bar_mma, 1);
+    mbar_init_fence();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, TMEM_COLS);
+    tmem_relinquish();
+  }
+  fence_proxy_async_smem();  // the weights are read by the tensor cores
+  tc_fence_before();
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned char* mine = smem_raw + SMEM_W + warp * SMEM_TILE_INFER;
-  bf16* X = reinterpret_cast<bf16*>(mine);
-  bf16* h1 = reinterpret_cast<bf16*>(mine + SMEM_X);
-  bf16* h2 = X;
+  tc_fence_after();
+  const unsigned tmem = *tmem_slot;
   const float os = params[OFF_OS];
-  const long long ntiles = (n + IROWS - 1) / IROWS;
-  for (long long tile = (long long)blockIdx.x * WARPS + warp; tile < ntiles; tile += (long long)gridDim.x * WARPS) {
-    // 32 rows x 26 chunks of 16 bytes, all in flight at once (cp.async); rows past n repeat row n-1
-    for (int e = lane; e < IROWS * (K1 / 8); e += 32) {
-      const int r = e / (K1 / 8), q = e - r * (K1 / 8);
-      long long i = tile * IROWS + r;
-      if (i >= n) i = n - 1;
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(X + r * XP + 8 * q);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(Xg + i * K1 + 8 * q) : "memory");
+  const long long ntiles = (n + TM - 1) / TM;
+  constexpr unsigned ID1 = umma_idesc_bf16(128, 128), ID3 = umma_idesc_bf16(128, N3P);
+  unsigned ph_mma = 0;
+  bool failed = false;
+  if (tid == 0 && (long long)blockIdx.x < ntiles) {
+    mbar_expect_tx(&bar_x[0], TILE_X_BYTES);
+    bulk_g2s(sm + SM_X0, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
+  }
+  int it = 0;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    const int b = it & 1;
+    unsigned char* Xs = sm + (b ? SM_X1 : SM_X0);
+    // prefetch the next tile into the other buffer (its last reader, layer 1 of the previous tile,
+    // has completed)
+    if (tid == 0 && tile + gridDim.x < ntiles) {
+      mbar_expect_tx(&bar_x[b ^ 1], TILE_X_BYTES);
+      bulk_g2s(sm + (b ? SM_X0 : SM_X1), Xg + (tile + gridDim.x) * (long long)TILE_X_BYTES, TILE_X_BYTES,
+               &bar_x[b ^ 1]);
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    __syncwarp();
-    {
-      float acc[2][16][4];
-      warp_gemm_rg<2, 16, K1>(acc, X, XP, s_w1t, KP1, lane);
-      act_store(acc, params + OFF_B1, h1, lane);
-      __syncwarp();
-      warp_gemm_rg<2, 16, H>(acc, h1, KP2, s_w2t, KP2, lane);
-      act_store(acc, params + OFF_B2, h2, lane);
-      __syncwarp();
+    failed = __syncthreads_or(!mbar_wait_bounded(&bar_x[b], (unsigned)(it >> 1) & 1u, kWaitLimitMlp)) != 0;
+    if (failed) break;  // block-uniform
+    // layer 1
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int k = 0; k < K1 / 16; ++k)
+        umma_bf16(tmem, umma_desc(Xs + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+                  umma_desc(sm + SM_W1 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
+      umma_commit(bar_mma);
     }
-    float a3[2][1][4];
-    warp_gemm_rg<2, 1, H>(a3, h2, KP2, s_w3t, KP2, lane);
-    const int g = lane >> 2, t = lane & 3;
+    for (int layer = 0; layer < 2; ++layer) {
+      failed = __syncthreads_or(!mbar_wait_bounded(bar_mma, ph_mma, kWaitLimitMlp)) != 0;
+      ph_mma ^= 1u;
+      if (failed) break;
+      tc_fence_after();
+      // epilogue: rows 32 (warp & 3) + lane, columns 64 (warp >> 2) .. + 63
+      {
+        const int sub = warp & 3, half = warp >> 2;
+        const int row = 32 * sub + lane;
+        const float* bl = bias + layer * H;
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
+        for (int cc = 0; cc < 4; ++cc) {
+          const int col0 = 64 * half + 16 * cc;
+          float v[16];
+          tmem_ld16(tmem + ((unsigned)(32 * sub) << 16) + (unsigned)col0, v);
+          unsigned w[8];
 #pragma unroll
-      for (int hh = 0; hh < 2; ++hh) {
-        const long long i = tile * IROWS + 16 * r + g + 8 * hh;
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int c = 2 * t + q;  // canonical component
-          if (i < n && c < D_OUT) {
-            const float* ax = auxg + i * 8;
-            const int code = __float_as_int(ax[4]);
-            const int cg = frame_perm(code, c);
-            const float y = a3[r][0][2 * hh + q] + params[OFF_B3 + c];
-            out[3 * i + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
-          }
+          for (int j = 0; j < 8; ++j)
+            w[j] = pack2(silu(v[2 * j] + bl[col0 + 2 * j]), silu(v[2 * j + 1] + bl[col0 + 2 * j + 1]));
+          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8, TM)) = make_uint4(w[0], w[1], w[2], w[3]);
+          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8 + 1, TM)) = make_uint4(w[4], w[5], w[6], w[7]);
         }
       }
-    __syncwarp();
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        if (layer == 0) {
+#pragma unroll 1
+          for (int k = 0; k < H / 16; ++k)
+            umma_bf16(tmem, umma_desc(sm + SM_H + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+                      umma_desc(sm + SM_W2 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
+        } else {
+#pragma unroll 1
+          for (int k = 0; k < H / 16; ++k)
+            umma_bf16(tmem + 128, umma_desc(sm + SM_H + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+                      umma_desc(sm + SM_W3 + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), ID3, k > 0);
+        }
+        umma_commit(bar_mma);
+      }
+    }
+    if (failed) break;
+    failed = __syncthreads_or(!mbar_wait_bounded(bar_mma, ph_mma, kWaitLimitMlp)) != 0;
+    ph_mma ^= 1u;
+    if (failed) break;
+    tc_fence_after();
+    if (warp < 4) {
+      const int row = 32 * warp + lane;
+      float v[16];
+      tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + 128u, v);
+      const long long i = tile * TM + row;
+      if (i < n) {
+        const float* ax = auxg + i * 8;
+        const int code = __float_as_int(ax[4]);
+#pragma unroll
+        for (int c = 0; c < D_OUT; ++c) {
+          const int cg = frame_perm(code, c);
+          const float y = v[c] + bias[2 * H + c];
+          out[3 * i + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
   }
+  if (failed && tid == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
 }
 
 // ---- training samples ------------------------------------------------------------------------------
@@ -944,49 +998,48 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
   if (n == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;
-  static_assert(SMEM_INFER <= 227 * 1024, "inference tile exceeds shared memory");
-  // feature rows and aux live in the plan's transform workspace (idle during droplet stages):
-  // droplets are taken in batches that fit it
+  static_assert(SMEM_FWD <= 227 * 1024, "tensor-core forward exceeds shared memory");
+  // feature tiles and aux live in the plan's transform workspace (idle during droplet stages):
+  // droplets are taken in batches of whole tiles that fit it
   const size_t per = sizeof(bf16) * K1 + sizeof(float) * 8;
   long long cap = (long long)(p->work_bytes / per);
-  cap -= cap % 32;
-  if (cap < 32) return ld_fail(LD_ERR_CAPACITY, "ld_mlp_infer: no workspace");
-  bf16* X = (bf16*)p->work;
+  cap -= cap % TM;
+  if (cap < TM) return ld_fail(LD_ERR_CAPACITY, "ld_mlp_infer: no workspace");
+  unsigned char* X = (unsigned char*)p->work;
   for (long long b0 = 0; b0 < n; b0 += cap) {
     const long long nb = n - b0 < cap ? n - b0 : cap;
-    float* aux = (float*)((char*)p->work + sizeof(bf16) * K1 * nb);
+    const long long tiles = (nb + TM - 1) / TM;
+    float* aux = (float*)(X + tiles * (long long)TILE_X_BYTES);
     const long long groups = (nb + FROWS - 1) / FROWS;
     long long gf = (groups + FWARPS - 1) / FWARPS;
-    if (gf > 148LL * 4 * 4) gf = 148LL * 4 * 4;
-    const long long tiles = (nb + IROWS - 1) / IROWS;
-    long long gm = (tiles + WARPS - 1) / WARPS;
-    if (gm > 148) gm = 148;  // one CTA per SM (shared memory), persistent warps
+    if (gf > 148LL * 2 * 4) gf = 148LL * 2 * 4;
+    const long long gm = tiles < 148 ? tiles : 148;  // one CTA per SM (shared memory, TMEM), persistent
     if (p->prec == LD_F32) {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM_FEAT));
-      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_INFER));
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_FWD));
       {
         ProfScope ps(p, KID_MLP_FEAT, s);
         k_mlp_features<float><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const float4*)u4, p->N, L,
-                                                                          pos + 3 * b0, nb, params, X, aux);
+                                                                          pos + 3 * b0, nb, params, (bf16*)X, aux);
       }
       ProfScope ps(p, KID_MLP_INFER, s);
-      k_mlp_forward<float><<<(unsigned)gm, WARPS * 32, SMEM_INFER, s>>>(X, aux, nb, (const bf16*)packed, params,
-                                                                        (float*)out + 3 * b0);
+      k_mlp_forward_tc<float><<<(unsigned)gm, FT_THREADS, SMEM_FWD, s>>>(X, aux, nb, (const bf16*)packed, params,
+                                                                        (float*)out + 3 * b0, p->status);
     } else {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM_FEAT));
-      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_INFER));
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward_tc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)SMEM_FWD));
       {
         ProfScope ps(p, KID_MLP_FEAT, s);
         k_mlp_features<double><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const double4*)u4, p->N, L,
-                                                                            pos + 3 * b0, nb, params, X, aux);
+                                                                            pos + 3 * b0, nb, params, (bf16*)X, aux);
       }
       ProfScope ps(p, KID_MLP_INFER, s);
-      k_mlp_forward<double><<<(unsigned)gm, WARPS * 32, SMEM_INFER, s>>>(X, aux, nb, (const bf16*)packed, params,
-                                                                         (double*)out + 3 * b0);
+      k_mlp_forward_tc<double><<<(unsigned)gm, FT_THREADS, SMEM_FWD, s>>>(X, aux, nb, (const bf16*)packed,
+                                                                         params, (double*)out + 3 * b0, p->status);
     }
     LD_LAUNCH_CHECK();
   }
