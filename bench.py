@@ -20,8 +20,11 @@ Learned interpolation protocol (--interp learned, the default):
   3. the judge at the end: exact spectral sum at a random 1% of the droplets, against the learned
      and the tricubic values.  Its device time is charged to the step time once per output
      interval (500 steps: the reference saves every 0.5 time units).
-The plain comparator (``plain_fp64``) runs the same seed and droplets in FP64 with tricubic
-interpolation for 500 steps, timed over its last ``steps`` steps, with its own error at the end.
+The plain comparators run the same seed and droplets in FP64 with tricubic interpolation for 500
+steps, timed over their last ``steps`` steps, with their own errors at the end: ``plain_fp64`` on
+the same grid, and ``plain_fp64_same_error`` on the first power-of-two grid on which plain
+tricubic meets the error tolerance (its error scales as dx^4), from the same physical initial
+field embedded in the finer grid.
 
 A "step" is one full time step (two flow stages, two droplet stages, epilogue, collisions).
 ``value`` is steps/s of the whole job (N replicas, one per GPU: the single-box step does not
@@ -63,7 +66,9 @@ def parse_args(argv=None):
     ap.add_argument("--judge-frac", type=float, default=0.01)
     ap.add_argument("--train-pairs", type=int, default=20_000_000)
     ap.add_argument("--train-epochs", type=int, default=16)
-    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 tricubic comparator")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 tricubic comparators")
+    ap.add_argument("--no-plain-fine", action="store_true", help="skip the plain FP64 run on the finer grid")
+    ap.add_argument("--tolerance", type=float, default=1e-4, help="droplet-velocity error tolerance")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--sort-every", type=int, default=20)
@@ -238,16 +243,41 @@ def flow_params_for(N):
     return (2.5e-3, 1e-3) if N == 256 else ((1e-3, 5e-4) if N == 512 else (0.01, 2e-3))
 
 
-def build_workload(a, seed, precision=None, interp=None, droplets=True):
-    """DNS (+ droplets at the interpolated fluid velocity, + collider) from seeded inputs."""
+def embed_spectrum(uk_full, N2):
+    """A reference-layout spectrum (3, N, N, N/2+1) of an N^3 field as the same physical field on an
+    N2^3 grid (N2 > N): the modes keep their wavenumbers, times (N2/N)^3 for the unnormalised
+    forward transform."""
+    import torch
+    N = uk_full.shape[1]
+    src = torch.as_tensor(uk_full).cuda()
+    out = torch.zeros((3, N2, N2, N2 // 2 + 1), dtype=torch.complex128, device="cuda")
+    h = N // 2
+    si = torch.cat([torch.arange(0, h), torch.arange(h + 1, N)]).cuda()          # Nyquist dropped
+    di = torch.cat([torch.arange(0, h), torch.arange(N2 - h + 1, N2)]).cuda()
+    blk = src[:, si][:, :, si][..., : h + 1].to(torch.complex128) * (N2 / N) ** 3
+    out[:, di[:, None], di[None, :], : h + 1] = blk
+    return out
+
+
+def build_workload(a, seed, precision=None, interp=None, droplets=True, N=None):
+    """DNS (+ droplets at the interpolated fluid velocity, + collider) from seeded inputs.  With N
+    larger than the configuration's grid, the configuration's initial field is embedded in the
+    finer grid (same physics, same field, finer resolution)."""
     import torch
     from lucky_droplets_b200.dns import ForcedDNS, Droplets
     from lucky_droplets_b200.init import init_flow, init_droplets
     precision = precision or a.precision
     interp = interp or a.interp
     nu, dt = flow_params_for(a.N)
-    dns = ForcedDNS.config(a.N, nu, dt, eps=0.1, kf=2, precision=precision)
-    init_flow(dns, seed)
+    Ng = N or a.N
+    dns = ForcedDNS.config(Ng, nu, dt, eps=0.1, kf=2, precision=precision)
+    if Ng == a.N:
+        init_flow(dns, seed)
+    else:
+        base = ForcedDNS.config(a.N, nu, dt, eps=0.1, kf=2, precision="f64")
+        init_flow(base, seed)
+        dns.set_uk_full(embed_spectrum(base.uk_full(), Ng))
+        del base
     d = None
     if droplets and a.nd > 0:
         from lucky_droplets_b200.collide import Collider
@@ -413,17 +443,18 @@ def cpu_baseline(dns, d, a):
                       f"scipy.fft workers={C._WORKERS}"}
 
 
-def run_plain(a, seed, world):
-    """The plain comparator: the same seed and droplets, FP64 fields and transforms, tricubic."""
+def run_plain(a, seed, world, N=None):
+    """The plain comparator: the same seed and droplets, FP64 fields and transforms, tricubic
+    (on the configuration's grid, or on a finer one N with the same initial field)."""
     import torch
-    dns, d = build_workload(a, seed, precision="f64", interp="tricubic")
+    dns, d = build_workload(a, seed, precision="f64", interp="tricubic", N=N)
     advance_to_window(dns, a)
     ms = time_steps(dns, a.steps, a.warmup, world)
     ms = allreduce_max(ms, world)
     dns.check()
     err = error_plain(dns, d, a.judge_frac, seed + 99) if d is not None else None
     out = {"value": world * a.steps / (ms / 1e3), "unit": "steps/s", "ms_per_step": ms / a.steps,
-           "precision": "f64", "interp": "tricubic", "droplet_velocity_rel_l2": err,
+           "N": dns.N, "precision": "f64", "interp": "tricubic", "droplet_velocity_rel_l2": err,
            "at_step": dns.nstep}
     del dns, d
     torch.cuda.empty_cache()
@@ -527,12 +558,22 @@ def run_ours(a):
         torch.cuda.empty_cache()
         plain = run_plain(a, seed, world)
         out["plain_fp64"] = plain
-        out["speedup_vs_plain_fp64"] = value / plain["value"]
+        out["speedup_vs_plain_fp64_same_grid"] = value / plain["value"]
         e_plain = plain["droplet_velocity_rel_l2"]
         out["error"] = {"learned_f32": judge["learned"], "tricubic_f32": judge["tricubic"],
-                        "plain_fp64_tricubic": e_plain, "tolerance": 1e-4,
-                        "learned_within_tolerance": judge["learned"] <= 1e-4,
+                        "plain_fp64_tricubic": e_plain, "tolerance": a.tolerance,
+                        "learned_within_tolerance": judge["learned"] <= a.tolerance,
                         "learned_over_plain": judge["learned"] / e_plain if e_plain else None}
+        # plain FP64 at equal error: its tricubic error scales as dx^4, so the first power-of-two
+        # grid on which it meets the tolerance; the same physical initial field and droplets
+        if e_plain is not None and e_plain > a.tolerance and not a.no_plain_fine:
+            N2 = a.N
+            while e_plain * (a.N / N2) ** 4 > a.tolerance:
+                N2 *= 2
+            fine = run_plain(a, seed, world, N=N2)
+            out["plain_fp64_same_error"] = fine
+            out["speedup_vs_plain_fp64_same_error"] = value / fine["value"]
+            out["error"]["plain_fp64_same_error_tricubic"] = fine["droplet_velocity_rel_l2"]
     if cpu_state is not None:
         out["cpu_baseline"] = cpu_baseline(*cpu_state, a)
     if rank == 0:

@@ -82,9 +82,21 @@ __device__ __forceinline__ void mma16816(float* d, const unsigned* a, const unsi
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// SiLU with the logistic function from the hardware tanh approximation, sigma(z) = (1 + tanh(z/2))/2
+// (relative error ~5e-4, below the BF16 rounding of the activations); training and inference use
+// the same function.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigm(float z) { return fmaf(0.5f, tanh_fast(0.5f * z), 0.5f); }
+__device__ __forceinline__ float silu(float z) {
+  const float h = 0.5f * z;
+  return fmaf(h, tanh_fast(h), h);
+}
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.f / (1.f + __expf(-z));
+  const float s = sigm(z);
   return s * (1.f + z * (1.f - s));
 }
 
@@ -174,30 +186,6 @@ __device__ __forceinline__ void point_frame(double px, double py, double pz, int
   f.code = make_frame(toff, f.tc);
 }
 
-// Tap `tap` (canonical j0*16 + j1*4 + j2, j in 0..3 <-> offsets -1..2) of the point's stencil (component
-// blocks CS floats apart) in
-// its canonical frame: along canonical axis k the taps run over grid axis p[k], reversed when that
-// axis is reflected; canonical component cc is grid component p[cc] with the reflection's sign.
-template <typename T, int CS>
-__device__ __forceinline__ void canon_tap(const vec4<T>* __restrict__ u4, int N, const int* ci, int code, int tap,
-                                          float* st) {
-  const int j[3] = {tap >> 4, (tap >> 2) & 3, tap & 3};
-  int g[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const int d = frame_perm(code, k);
-    const int o = (code >> (6 + d)) & 1 ? 3 - j[k] : j[k];
-    g[d] = (ci[d] - 1 + o + N) & (N - 1);
-  }
-  const vec4<T> v = u4[((long long)g[0] * N + g[1]) * N + g[2]];
-  const float comp[3] = {float(v.x), float(v.y), float(v.z)};
-#pragma unroll
-  for (int cc = 0; cc < 3; ++cc) {
-    const int d = frame_perm(code, cc);
-    st[cc * CS + tap] = frame_sign(code, d) * comp[d];
-  }
-}
-
 // Tricubic weights of the canonical offsets in the polynomial basis (per canonical axis): the
 // tricubic value is sum_i D_i wh0[i0] wh1[i1] wh2[i2] (P orthonormal: w.s = (P w).(P s)).
 __device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4]) {
@@ -265,6 +253,40 @@ __device__ __forceinline__ void tail_features(const float* tc, unsigned (&w)[8])
   for (int j = 2; j < 8; ++j) w[j] = 0u;
 }
 
+// Grid-memory offset (in vec4 elements) of canonical index j along canonical axis k of a point
+// (cell ci, frame code): along grid axis p[k], reversed when that axis is reflected.
+__device__ __forceinline__ long long canon_offset(const int* ci, int code, int N, int k, int j) {
+  const int d = frame_perm(code, k);
+  const int o = (code >> (6 + d)) & 1 ? 3 - j : j;
+  const int cid = d == 0 ? ci[0] : (d == 1 ? ci[1] : ci[2]);
+  const long long g = (cid - 1 + o + N) & (N - 1);
+  return d == 0 ? g * N * N : (d == 1 ? g * N : g);
+}
+
+// Canonical component c of the point's 64-tap stencil, straight from the interleaved field into
+// registers (canonical tap order j0*16 + j1*4 + j2).
+template <typename T>
+__device__ __forceinline__ void gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
+                                                 float (&v)[64]) {
+  long long o0[4], o1[4], o2[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    o0[j] = canon_offset(f.i, f.code, N, 0, j);
+    o1[j] = canon_offset(f.i, f.code, N, 1, j);
+    o2[j] = canon_offset(f.i, f.code, N, 2, j);
+  }
+  const int d = frame_perm(f.code, c);
+  const float sg = frame_sign(f.code, d);
+  const T* base = reinterpret_cast<const T*>(u4) + d;
+#pragma unroll
+  for (int j0 = 0; j0 < 4; ++j0)
+#pragma unroll
+    for (int j1 = 0; j1 < 4; ++j1)
+#pragma unroll
+      for (int j2 = 0; j2 < 4; ++j2)
+        v[16 * j0 + 4 * j1 + j2] = sg * float(__ldg(base + 4 * (o0[j0] + o1[j1] + o2[j2])));
+}
+
 // Thread-per-point features (training samples): st is a 192-float scratch.  Returns the scale;
 // tric (grid frame), the canonical tricubic value and the frame code come back through the
 // arguments.
@@ -274,14 +296,12 @@ __device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, 
                                                 float* tric_grid, int& code, float* tric_can) {
   PtFrame f;
   point_frame(px, py, pz, N, L, f);
-  for (int tap = 0; tap < 64; ++tap) canon_tap<T, 64>(u4, N, f.i, f.code, tap, st);
   float wh[3][4];
   tric_weights(f.tc, wh);
   CompSums cs[3];
   for (int c = 0; c < 3; ++c) {
     float v[64];
-#pragma unroll
-    for (int j = 0; j < 64; ++j) v[j] = st[64 * c + j];
+    gather_component<T>(u4, N, f, c, v);
     comp_transform(v);
     cs[c] = comp_sums(v, wh);
 #pragma unroll
@@ -406,94 +426,47 @@ __host__ __device__ constexpr int blk_off(int row, int kc, int rows) {
 constexpr int TM = 128;                             // droplets per tensor-core tile
 constexpr int TILE_X_BYTES = TM * K1 * 2;           // one tile of feature rows
 
-constexpr int FWARPS = 8;
-constexpr int FROWS = 8;              // droplets per warp group; lanes 3r + c (r < 8, c < 3) transform
-constexpr int SCS = 65;               // component stride of the staged taps (= 1 mod 32)
-constexpr int SRS = 3 * SCS;          // droplet stride (= 3 mod 32): the 24 lanes hit distinct banks
-constexpr size_t SMEM_FEAT = sizeof(float) * FWARPS * FROWS * SRS;
-
-// Grid-memory offset of canonical index j along canonical axis k of a point (cell ci, frame code).
-__device__ __forceinline__ long long canon_offset(const int* ci, int code, int N, int k, int j) {
-  const int d = frame_perm(code, k);
-  const int o = (code >> (6 + d)) & 1 ? 3 - j : j;
-  const int cid = d == 0 ? ci[0] : (d == 1 ? ci[1] : ci[2]);
-  const long long g = (cid - 1 + o + N) & (N - 1);
-  return d == 0 ? g * N * N : (d == 1 ? g * N : g);
-}
+// k_mlp_features: lane 3r + c of a warp takes canonical component c of droplet r (10 droplets
+// per warp; lanes 30, 31 shadow droplet 9): the component's stencil is gathered into registers,
+// transformed, reduced to its partial sums, and the three lanes of a droplet combine them by
+// shuffles; each lane writes its 64 features (128 contiguous bytes of the tile layout), lane 3r
+// also the offsets and the aux (tricubic xyz in the grid frame, scale, frame code).
+constexpr int FDROP = 10;
+constexpr int FTHREADS = 256;
 
 template <typename T>
-__global__ void __launch_bounds__(FWARPS * 32, 2)
+__global__ void __launch_bounds__(FTHREADS, 2)
 k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __restrict__ pos, long long n,
                const float* __restrict__ params, bf16* __restrict__ Xg, float* __restrict__ auxg) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* st = reinterpret_cast<float*>(smem_raw) + warp * FROWS * SRS;
+  const int lane = threadIdx.x & 31;
+  const long long wg = ((long long)blockIdx.x * FTHREADS + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * FTHREADS) >> 5;
+  const int r = lane < 3 * FDROP ? lane / 3 : FDROP - 1;
+  const int c = lane < 3 * FDROP ? lane - 3 * r : 0;
   const float* fs = params + OFF_FS;
   const float mode = params[OFF_OS + 1];
-  // this lane's taps: lane and lane + 32 (canonical j0 = lane>>4 and 2 + (lane>>4), shared j1, j2)
-  const int j0a = lane >> 4, j1 = (lane >> 2) & 3, j2 = lane & 3;
-  const long long ngroups = (n + FROWS - 1) / FROWS;
-  for (long long grp = (long long)blockIdx.x * FWARPS + warp; grp < ngroups; grp += (long long)gridDim.x * FWARPS) {
-    const long long i0 = grp * FROWS;
-    const int rows = (int)(n - i0 < FROWS ? n - i0 : FROWS);
-    // frame of droplet `lane` (lanes 0..7)
+  const long long ngroups = (n + FDROP - 1) / FDROP;
+  for (long long grp = wg; grp < ngroups; grp += nw) {
+    const long long i = grp * FDROP + r;
+    const long long ii = i < n ? i : n - 1;
     PtFrame f;
-    {
-      long long i = i0 + (lane & (FROWS - 1));
-      if (i >= n) i = n - 1;
-      point_frame(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], N, L, f);
-    }
-    // canonical taps of the 8 droplets into shared memory
-#pragma unroll 2
-    for (int r = 0; r < FROWS; ++r) {
-      int ci[3];
-      ci[0] = __shfl_sync(0xffffffffu, f.i[0], r);
-      ci[1] = __shfl_sync(0xffffffffu, f.i[1], r);
-      ci[2] = __shfl_sync(0xffffffffu, f.i[2], r);
-      const int code = __shfl_sync(0xffffffffu, f.code, r);
-      const long long o12 = canon_offset(ci, code, N, 1, j1) + canon_offset(ci, code, N, 2, j2);
-      const vec4<T> va = u4[canon_offset(ci, code, N, 0, j0a) + o12];
-      const vec4<T> vb = u4[canon_offset(ci, code, N, 0, j0a + 2) + o12];
-      float* sr = st + r * SRS;
-#pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const int d = frame_perm(code, cc);
-        const float sg = frame_sign(code, d);
-        const float xa = d == 0 ? float(va.x) : (d == 1 ? float(va.y) : float(va.z));
-        const float xb = d == 0 ? float(vb.x) : (d == 1 ? float(vb.y) : float(vb.z));
-        sr[cc * SCS + lane] = sg * xa;
-        sr[cc * SCS + lane + 32] = sg * xb;
-      }
-    }
-    __syncwarp();
-    // lane 3r + c: component c of droplet r
-    const int r = lane / 3, c = lane - 3 * (lane / 3);
-    const int rr = r < FROWS ? r : FROWS - 1;
-    float tc[3];
-    tc[0] = __shfl_sync(0xffffffffu, f.tc[0], rr);
-    tc[1] = __shfl_sync(0xffffffffu, f.tc[1], rr);
-    tc[2] = __shfl_sync(0xffffffffu, f.tc[2], rr);
-    const int code = __shfl_sync(0xffffffffu, f.code, rr);
+    point_frame(pos[3 * ii], pos[3 * ii + 1], pos[3 * ii + 2], N, L, f);
     float v[64];
-    const float* sv = st + rr * SRS + c * SCS;
-#pragma unroll
-    for (int j = 0; j < 64; ++j) v[j] = sv[j];
+    gather_component<T>(u4, N, f, c, v);
     comp_transform(v);
     float wh[3][4];
-    tric_weights(tc, wh);
+    tric_weights(f.tc, wh);
     const CompSums cs = comp_sums(v, wh);
-    // the droplet's three components: lanes 3r, 3r+1, 3r+2
-    const int b0 = 3 * rr;
+    const int b0 = 3 * r;
     const float ss0 = __shfl_sync(0xffffffffu, cs.ss, b0), ss1 = __shfl_sync(0xffffffffu, cs.ss, b0 + 1),
                 ss2 = __shfl_sync(0xffffffffu, cs.ss, b0 + 2);
     const float sh0 = __shfl_sync(0xffffffffu, cs.sh, b0), sh1 = __shfl_sync(0xffffffffu, cs.sh, b0 + 1),
                 sh2 = __shfl_sync(0xffffffffu, cs.sh, b0 + 2);
     const float tr1 = __shfl_sync(0xffffffffu, cs.tr, b0 + 1), tr2 = __shfl_sync(0xffffffffu, cs.tr, b0 + 2);
     const float scale = scale_of(ss0, ss1, ss2, sh0, sh1, sh2, mode);
-    if (r < rows) {
+    if (lane < 3 * FDROP && i < n) {
       unsigned w[32];
       comp_features(v, fs, 1.f / scale, w);
-      const long long i = i0 + r;
       unsigned char* tb = reinterpret_cast<unsigned char*>(Xg) + (i / TM) * TILE_X_BYTES;
       const int rr = (int)(i % TM);
 #pragma unroll
@@ -502,38 +475,38 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
             make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
       if (c == 0) {
         unsigned wt[8];
-        tail_features(tc, wt);
+        tail_features(f.tc, wt);
         *reinterpret_cast<uint4*>(tb + blk_off(rr, 24, TM)) = make_uint4(wt[0], wt[1], wt[2], wt[3]);
         *reinterpret_cast<uint4*>(tb + blk_off(rr, 25, TM)) = make_uint4(wt[4], wt[5], wt[6], wt[7]);
         const float trc[3] = {cs.tr, tr1, tr2};
-        float* ax = auxg + (i0 + r) * 8;
+        float* ax = auxg + i * 8;
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
-          const int d = frame_perm(code, cc);
-          const float val = frame_sign(code, d) * trc[cc];
+          const int d = frame_perm(f.code, cc);
+          const float val = frame_sign(f.code, d) * trc[cc];
           if (d == 0) ax[0] = val;
           else if (d == 1) ax[1] = val;
           else ax[2] = val;
         }
         ax[3] = scale;
-        ax[4] = __int_as_float(code);
+        ax[4] = __int_as_float(f.code);
       }
     }
-    __syncwarp();
   }
 }
 
 // ---- MLP forward on the 5th-generation tensor cores --------------------------------------------
-// Persistent CTA per SM, 8 warps.  Per tile of TM = 128 droplets:
+// Persistent CTA per SM, 16 warps.  Per tile of TM = 128 droplets:
 //   X tile (128 x 208 bf16, tile layout) arrives by one bulk asynchronous copy, double-buffered;
 //   layer 1: 13 tcgen05.mma (M 128, N 128, K 16) from X and W1 into TMEM columns 0..127;
-//   epilogue: 8 warps read the accumulators (tcgen05.ld), add b1, SiLU, bf16 -> H (tile layout);
+//   epilogue: 16 warps read the accumulators (tcgen05.ld; warp w: TMEM lanes 32 (w % 4), columns
+//   32 (w / 4)), add b1, SiLU, bf16 -> H (tile layout);
 //   layer 2: 8 MMAs from H and W2 into TMEM 0..127; epilogue as above -> H;
 //   layer 3: 8 MMAs (N 16: W3 padded) into TMEM 128..143; warps 0..3 write
 //   out = tricubic + scale * os * MLP back in the grid frame.
 // One thread issues the MMAs and commits them to an mbarrier that all threads wait on (bounded:
 // a wait that runs out raises LD_STATUS_WAIT_TIMEOUT and the CTA frees its TMEM and returns).
-constexpr int FT_THREADS = 256;
+constexpr int FT_THREADS = 512;
 constexpr int N3P = 16;                               // layer-3 N padded for M = 128
 constexpr int SM_W1 = 0;
 constexpr int SM_W2 = SM_W1 + H * K1 * 2;             // 53248
@@ -629,23 +602,25 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
       ph_mma ^= 1u;
       if (failed) break;
       tc_fence_after();
-      // epilogue: rows 32 (warp & 3) + lane, columns 64 (warp >> 2) .. + 63
+      // epilogue: rows 32 (warp & 3) + lane, columns 32 (warp >> 2) .. + 31
       {
-        const int sub = warp & 3, half = warp >> 2;
+        const int sub = warp & 3, quarter = warp >> 2;
         const int row = 32 * sub + lane;
-        const float* bl = bias + layer * H;
+        const int col0 = 32 * quarter;
+        const float4* bl = reinterpret_cast<const float4*>(bias + layer * H + col0);
+        float v[32];
+        tmem_ld32(tmem + ((unsigned)(32 * sub) << 16) + (unsigned)col0, v);
+        unsigned w[16];
 #pragma unroll
-        for (int cc = 0; cc < 4; ++cc) {
-          const int col0 = 64 * half + 16 * cc;
-          float v[16];
-          tmem_ld16(tmem + ((unsigned)(32 * sub) << 16) + (unsigned)col0, v);
-          unsigned w[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j)
-            w[j] = pack2(silu(v[2 * j] + bl[col0 + 2 * j]), silu(v[2 * j + 1] + bl[col0 + 2 * j + 1]));
-          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8, TM)) = make_uint4(w[0], w[1], w[2], w[3]);
-          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8 + 1, TM)) = make_uint4(w[4], w[5], w[6], w[7]);
+        for (int j = 0; j < 8; ++j) {
+          const float4 b4 = bl[j];
+          w[2 * j] = pack2(silu(v[4 * j] + b4.x), silu(v[4 * j + 1] + b4.y));
+          w[2 * j + 1] = pack2(silu(v[4 * j + 2] + b4.z), silu(v[4 * j + 3] + b4.w));
         }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8 + q, TM)) =
+              make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
       }
       fence_proxy_async_smem();
       tc_fence_before();
@@ -1010,31 +985,27 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
     const long long nb = n - b0 < cap ? n - b0 : cap;
     const long long tiles = (nb + TM - 1) / TM;
     float* aux = (float*)(X + tiles * (long long)TILE_X_BYTES);
-    const long long groups = (nb + FROWS - 1) / FROWS;
-    long long gf = (groups + FWARPS - 1) / FWARPS;
-    if (gf > 148LL * 2 * 4) gf = 148LL * 2 * 4;
+    const long long groups = (nb + FDROP - 1) / FDROP;
+    long long gf = (groups + FTHREADS / 32 - 1) / (FTHREADS / 32);
+    if (gf > 148LL * 2 * 8) gf = 148LL * 2 * 8;
     const long long gm = tiles < 148 ? tiles : 148;  // one CTA per SM (shared memory, TMEM), persistent
     if (p->prec == LD_F32) {
-      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_FEAT));
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward_tc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM_FWD));
       {
         ProfScope ps(p, KID_MLP_FEAT, s);
-        k_mlp_features<float><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const float4*)u4, p->N, L,
+        k_mlp_features<float><<<(unsigned)gf, FTHREADS, 0, s>>>((const float4*)u4, p->N, L,
                                                                           pos + 3 * b0, nb, params, (bf16*)X, aux);
       }
       ProfScope ps(p, KID_MLP_INFER, s);
       k_mlp_forward_tc<float><<<(unsigned)gm, FT_THREADS, SMEM_FWD, s>>>(X, aux, nb, (const bf16*)packed, params,
                                                                         (float*)out + 3 * b0, p->status);
     } else {
-      LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_features<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_FEAT));
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward_tc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM_FWD));
       {
         ProfScope ps(p, KID_MLP_FEAT, s);
-        k_mlp_features<double><<<(unsigned)gf, FWARPS * 32, SMEM_FEAT, s>>>((const double4*)u4, p->N, L,
+        k_mlp_features<double><<<(unsigned)gf, FTHREADS, 0, s>>>((const double4*)u4, p->N, L,
                                                                             pos + 3 * b0, nb, params, (bf16*)X, aux);
       }
       ProfScope ps(p, KID_MLP_INFER, s);
