@@ -6,8 +6,10 @@
 //   starts    cs[k] = first sorted index of cell k (k = 0..ncell; cs[ncell] = n)
 //   reorder   sorted copies of wrapped positions and radii (FP64, and an FP32 copy for the filter)
 //   count     per sorted droplet: partners among the cell itself and its 13 forward neighbours
+//             (the first KEEP of them recorded)
 //   scan      exclusive scan of the counts in sorted order -> offsets, total
-//   emit      pairs at offset + t in a fixed visiting order, then mapped to droplet ids (i < j)
+//   emit      pairs at offset + t in the fixed visiting order (copied from the record, or searched
+//             again for droplets with more partners), then mapped to droplet ids (i < j)
 // The FP64 arithmetic (wrap, cell index, minimum image, squared distance) is done with explicit
 // round-to-nearest operations and no fused multiply-add, in the same order as the CPU rule, so
 // the pair list is bit-exact given identical inputs.
@@ -273,16 +275,17 @@ __device__ __forceinline__ bool near_f(const float4 a, const float4 b, float L, 
 // cells z-1, z, z+1: the cell itself and its 13 forward neighbours, so every unordered pair is
 // tested exactly once.  The FP32 copies of the five columns are staged in shared memory (read
 // from global memory when they exceed cap_smem).  Each droplet visits its partners in a fixed
-// order; MODE 0 stores the count per sorted index, MODE 1 writes the pairs (sorted indices)
-// from off[i].
+// order, stores its partner count per sorted index and records its first KEEP partners (sorted
+// indices) in scr; k_emit_pairs then writes the pairs from the scanned counts, searching again
+// only for the rare droplets with more than KEEP partners.
 constexpr int COL_THREADS = 256;
+constexpr int KEEP = 4;
 constexpr int kColSmemRows = 12288;  // 192 KB of staged FP32 rows per block at most
 
-template <int MODE>
 __global__ void __launch_bounds__(COL_THREADS)
 k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
             const int* __restrict__ cs, int nc, int parts, double L, int cap_smem, unsigned* __restrict__ cnt,
-            const unsigned* __restrict__ off, int* __restrict__ pairs, long long cap) {
+            int* __restrict__ scr) {
   extern __shared__ float4 colbuf[];
   __shared__ int lo[5], len[5], so[6];
   const long long col = blockIdx.x / parts;
@@ -316,7 +319,6 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
     const float mar = margin + 1e-6f * mf.w;
     const int cz = (int)(skey[i] % (unsigned)nc);
     unsigned c = 0;
-    long long o = MODE == 1 ? (long long)off[i] : 0;
     double4 me;
     bool have_me = false;
     // target q, cell z: the sorted range [g0, g1)
@@ -341,15 +343,52 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
         if (!near_f(mf, b, Lf, hf, mar)) continue;
         if (!have_me) { me = sp[i]; have_me = true; }
         if (!overlap(me, sp[g], L)) continue;
-        if (MODE == 0) {
-          ++c;
-        } else {
-          if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
-          ++o;
-        }
+        if (c < KEEP) scr[(long long)KEEP * i + c] = g;
+        ++c;
       }
     }
-    if (MODE == 0) cnt[i] = c;
+    cnt[i] = c;
+  }
+}
+
+// Pairs of sorted droplet i at off[i]..: copied from scr when it has at most KEEP partners,
+// otherwise found again from global memory in the same visiting order.
+__global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf,
+                             const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc, double L,
+                             long long n, const unsigned* __restrict__ off, const int* __restrict__ scr,
+                             int* __restrict__ pairs, long long cap) {
+  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
+  for (long long ii = blockIdx.x * (long long)blockDim.x + threadIdx.x; ii < n; ii += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)ii;
+    const long long o0 = off[i];
+    const unsigned cnt = off[i + 1] - off[i];
+    if (cnt <= (unsigned)KEEP) {
+      for (unsigned k = 0; k < cnt; ++k)
+        if (o0 + k < cap) { pairs[2 * (o0 + k)] = i; pairs[2 * (o0 + k) + 1] = scr[(long long)KEEP * i + k]; }
+      continue;
+    }
+    const unsigned key = skey[i];
+    const int cz = (int)(key % (unsigned)nc), cy = (int)((key / nc) % nc), cx = (int)(key / ((unsigned)nc * nc));
+    const float4 mf = spf[i];
+    const float mar = margin + 1e-6f * mf.w;
+    const double4 me = sp[i];
+    long long o = o0;
+    for (int r = 0; r < 14; ++r) {
+      int q, dz;
+      if (r < 2) { q = 0; dz = r; }
+      else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
+      const int z = (cz + dz + nc) % nc;
+      const int ox = q < 2 ? 0 : 1;
+      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+      const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc + z;
+      const int g1 = cs[k + 1];
+      for (int g = r == 0 ? i + 1 : cs[k]; g < g1; ++g) {
+        if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
+        if (!overlap(me, sp[g], L)) continue;
+        if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
+        ++o;
+      }
+    }
   }
 }
 
@@ -397,6 +436,7 @@ struct ld_collider {
   int* start = nullptr;  // cell starts, ncell + 1 entries
   double4* sp = nullptr;
   float4* spf = nullptr;
+  int* scr = nullptr;  // first KEEP partners of each sorted droplet
   unsigned* status = nullptr;
   unsigned* sums = nullptr;  // scan tile totals
   int nblocks = 0;
@@ -442,6 +482,7 @@ int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
   A((void**)&c->start, 4 * (ncell + 1));
   A((void**)&c->sp, sizeof(double4) * nmax);
   A((void**)&c->spf, sizeof(float4) * nmax);
+  A((void**)&c->scr, sizeof(int) * KEEP * nmax);
   A((void**)&c->status, sizeof(unsigned));
   {
     long long m = (nmax + 1) > (long long)RADIX * c->nblocks ? (nmax + 1) : (long long)RADIX * c->nblocks;
@@ -461,7 +502,7 @@ int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
 int ld_collider_destroy(ld_collider* c) {
   if (!c) return LD_OK;
   cudaFree(c->key); cudaFree(c->val); cudaFree(c->key2); cudaFree(c->val2); cudaFree(c->hist);
-  cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->status);
+  cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->scr); cudaFree(c->status);
   cudaFree(c->sums);
   delete c;
   return LD_OK;
@@ -526,14 +567,13 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
     const int cap_smem = (int)want;
     const size_t smem = sizeof(float4) * (size_t)cap_smem;
     if (ncol * parts > 0x7fffffffLL) return ld_fail(LD_ERR_UNSUPPORTED, "ld_collide: too many cell columns");
-    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const unsigned gb = (unsigned)(ncol * parts);
-    k_col_pairs<0><<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem,
-                                                 c->cnt, nullptr, nullptr, 0);
+    k_col_pairs<<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem, c->cnt,
+                                              c->scr);
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
-    k_col_pairs<1><<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem,
-                                                 nullptr, c->cnt, pairs, cap);
+    k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, n, c->cnt, c->scr, pairs,
+                                               cap);
     k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + n, cap, c->val, pairs);
   } else {
     const int* end = c->start + 1;  // end of cell k = start of cell k + 1

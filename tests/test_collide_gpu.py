@@ -165,3 +165,15 @@ def test_contact_distance_boundary(torch, rel_gap):
     ref = K.collide(pos, rad, cell)
     assert len(ref) >= 5000  # the inside half, mostly
     assert got.shape == ref.shape and np.array_equal(got, ref)
+
+
+def test_dense_cluster_many_partners(torch):
+    """About 7 partners per droplet (most beyond the recorded first four, nc >= 3): the emitted
+    list still equals the FP64 rule's."""
+    rng = np.random.default_rng(21)
+    pos = rng.uniform(0.0, 1.0, (8000, 3))
+    rad = np.full(8000, 0.03)
+    got, _ = gpu_pairs(torch, pos, rad, 0.06, cap=400000)
+    ref = K.collide(pos, rad, 0.06)
+    assert len(ref) > 20000
+    assert got.shape == ref.shape and np.array_equal(got, ref)
