@@ -237,6 +237,9 @@ LD_API int ld_cell_order(ld_collider* collider, const double* pos, int64_t n, do
 /* dst row i = src row order[i] for n rows of row_bytes bytes (a multiple of 4); src != dst.  Applies
  * a droplet permutation to every per-droplet array (the reference's send(), P:233-275, reorders the
  * droplets the same way and tracks them by prtclid). */
+/* Device-to-device copy of `bytes` on the stream (the in-place re-sort copies the permuted rows
+ * back, so that the droplet arrays keep their addresses across CUDA-graph replays). */
+LD_API int ld_copy_async(void* dst, const void* src, int64_t bytes, void* stream);
 LD_API int ld_permute_rows(const void* src, void* dst, const uint32_t* order, int64_t n, int32_t row_bytes,
                            void* stream);
 /* Stable LSD radix sort of n (key, value) pairs on the low `bits` bits of the keys, in place,

@@ -66,6 +66,7 @@ SIGNATURES = {
     "ld_interleave3": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_gather4": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
     "ld_mlp_partial_floats": (_c_i64, [_c_i64]),
+    "ld_copy_async": (_c_i, [_c_p, _c_p, _c_i64, _c_p]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),
     "ld_droplet_update": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_p]),
     "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),

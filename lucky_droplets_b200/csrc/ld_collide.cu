@@ -616,6 +616,13 @@ int ld_permute_rows(const void* src, void* dst, const uint32_t* order, int64_t n
   return LD_OK;
 }
 
+int ld_copy_async(void* dst, const void* src, int64_t bytes, void* stream) {
+  if (bytes < 0 || (bytes > 0 && (!dst || !src))) return ld_fail(LD_ERR_ARG, "ld_copy_async: bad arguments");
+  if (bytes == 0) return LD_OK;
+  LD_CUDA_CHECK(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return LD_OK;
+}
+
 int ld_collider_trace(ld_collider* c, ld_plan* plan) {
   if (!c) return ld_fail(LD_ERR_ARG, "ld_collider_trace: null collider");
   c->trace = plan;

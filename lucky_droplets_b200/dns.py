@@ -229,15 +229,23 @@ class Droplets:
         return out
 
     def sort(self, collider, stream=None):
-        """Re-order every per-droplet array into the collider's cell order."""
+        """Re-order every per-droplet array into the collider's cell order, in place: each array
+        is permuted into a persistent scratch buffer and copied back, so the arrays keep their
+        device addresses (a captured CUDA graph replays against the same buffers)."""
+        torch = _torch()
         L = _lib.lib()
         st = stream_ptr(stream)
         check(L.ld_cell_order(collider._h, ptr(self.pos), self.n, collider.L, ptr(self._order), st))
+        if not hasattr(self, "_scratch"):
+            self._scratch = {}
         for name, t in self.arrays():
-            tmp = _torch().empty_like(t)
             row = t.element_size() * (t.shape[1] if t.dim() > 1 else 1)
+            tmp = self._scratch.get(name)
+            if tmp is None or tmp.dtype != t.dtype or tmp.shape != t.shape:
+                tmp = torch.empty_like(t)
+                self._scratch[name] = tmp
             check(L.ld_permute_rows(ptr(t), ptr(tmp), ptr(self._order), self.n, row, st))
-            setattr(self, name, tmp)
+            check(L.ld_copy_async(ptr(t), ptr(tmp), t.numel() * t.element_size(), st))
 
     def collide(self, collider, pairs, stream=None):
         """Colliding pairs (array indices, i < j) into ``pairs``; the count stays on the device."""
