@@ -114,6 +114,13 @@ LD_API int ld_spec_from_cube(ld_plan* plan, const void* cube, void* full, int nc
  * 3-vector, FP64, ek[0..N/2] (modes with |k| > N/2 + 1/2 are not counted, as np.histogram drops
  * them).  Deterministic: fixed-order FP64 reduction. */
 LD_API int ld_shell_spectrum(ld_plan* plan, const void* uk, double* ek, void* stream);
+/* Shell sums (Nf doubles) of Re(conj(a) . b) * normalize over the cube-layout 3-vectors a, b: with
+ * b the inviscid, unforced RHS of a this is the transfer behind Pik of save() (F:425-428); the
+ * flux spectrum is its reversed cumulative sum (F:428). */
+LD_API int ld_shell_cross(ld_plan* plan, const void* a, const void* b, double* out, void* stream);
+/* Spectral divergence i k . uk of a cube-layout 3-vector into one cube component (F:216-230; the
+ * physical divergence whose maximum save() prints at F:472 is its inverse transform). */
+LD_API int ld_divergence_spec(ld_plan* plan, const void* uk, void* divk, void* stream);
 
 /* ---- flow right-hand side, F:287-316 -------------------------------------------------- */
 /* ku = P[(u x omega)^ + f] * dealias - visc * nu k^2 uk for a cube-layout 3-vector uk, with

@@ -67,6 +67,8 @@ SIGNATURES = {
     "ld_gather4": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
     "ld_mlp_partial_floats": (_c_i64, [_c_i64]),
     "ld_copy_async": (_c_i, [_c_p, _c_p, _c_i64, _c_p]),
+    "ld_shell_cross": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
+    "ld_divergence_spec": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),
     "ld_droplet_update": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_p]),
     "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),

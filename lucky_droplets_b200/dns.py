@@ -99,6 +99,53 @@ class ForcedDNS:
         """Shell spectrum ek_arr of F:423, F:431 (FP64 numpy)."""
         return self.plan.e3d_to_e1d(self.uk).cpu().numpy()
 
+    def flux_spectrum(self):
+        """Pik_arr of save() (F:424-428): shell sums of Re(conj(uk) . N(uk)) with N the inviscid,
+        unforced RHS, then the reversed cumulative sum (FP64 numpy)."""
+        from .outputs import flux_from_transfer
+        p = self.plan
+        ku = p.velocity_rhs(self.uk, self.nu, 0.0, self.shell_no, visc=0.0)
+        return flux_from_transfer(p.shell_cross(self.uk, ku).cpu().numpy())
+
+    def diagnostics(self):
+        """What save() prints (F:464-484): energy from the physical field and from the shell
+        spectrum, and the maximum divergence."""
+        torch = _torch()
+        p = self.plan
+        u = self.velocity()
+        dx = TWO_PI / self.N
+        eng1 = float(0.5 * (u.double() ** 2).sum() * dx ** 3)
+        eng2 = float(self.energy_spectrum().sum())
+        divmax = float(p.divergence(self.uk).abs().max())
+        del u
+        return {"t": self.t, "energy": eng1, "energy_spectral": eng2, "divergence_max": divmax}
+
+    def save(self, dirpath, droplets=None, state_dir=None):
+        """Write the reference's output files (Fields_k_0, Energy_spectrum, Flux_spectrum and, with
+        droplets, state_0 with pos, vel, prtclid and the fluid velocity at the droplets, umat) into
+        dirpath; returns (paths, diagnostics)."""
+        from .outputs import write_outputs
+        state = None
+        d = droplets if droplets is not None else self.droplets
+        if d is not None:
+            u = self.velocity()
+            umat = d.gather(u).double()
+            order = _torch().argsort(d.ids)
+            state = {"pos": d.pos[order].cpu().numpy(), "vel": d.vel[order].double().cpu().numpy(),
+                     "prtclid": d.ids[order].cpu().numpy(), "umat": umat[order].cpu().numpy()}
+            if getattr(d, "mass", None) is not None:
+                state["mass"] = d.mass[order].double().cpu().numpy()
+            if state_dir is not None:
+                state["dir"] = state_dir
+            del u
+        paths = write_outputs(dirpath, self.uk_full(), self.energy_spectrum(), self.flux_spectrum(), state=state)
+        return paths, self.diagnostics()
+
+    def load(self, dirpath):
+        """Restart from Fields_k_0.npz (the spectral velocity in the reference's layout)."""
+        from .outputs import read_fields
+        return self.set_uk_full(read_fields(dirpath))
+
     def attach(self, droplets, collider=None, sort_every=0, pair_capacity=None):
         """Advance ``droplets`` with the flow.
 

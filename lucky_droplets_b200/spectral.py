@@ -154,6 +154,22 @@ class Plan:
         check(_lib.lib().ld_shell_spectrum(self._h, ptr(uk), ptr(out), stream_ptr(stream)))
         return out
 
+    def shell_cross(self, a, b, out=None, stream=None):
+        """Shell sums of Re(conj(a) . b) * normalize (FP64, length N/2+1) of cube-layout 3-vectors."""
+        self._chk(a, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        self._chk(b, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        if out is None:
+            out = _torch().zeros(self.Nf, dtype=_torch().float64, device=self.device)
+        check(_lib.lib().ld_shell_cross(self._h, ptr(a), ptr(b), ptr(out), stream_ptr(stream)))
+        return out
+
+    def divergence(self, uk, stream=None):
+        """Physical divergence (N, N, N) of a cube-layout 3-vector (spectral derivatives)."""
+        self._chk(uk, self.cdtype, (3, self.Mx, self.My, self.Mzp))
+        dk = self.empty_cube(1)
+        check(_lib.lib().ld_divergence_spec(self._h, ptr(uk), ptr(dk), stream_ptr(stream)))
+        return self.irfft_cube(dk, stream=stream)[0]
+
     def velocity_rhs(self, uk, nu, f0=0.0, shell_no=(1,), visc=1.0, ku=None, u_out=None, stream=None):
         """ku = P[(u x w)^ + f] dealias - visc nu k^2 uk  (full_RHS velocity part, F:287-316)."""
         self._chk(uk, self.cdtype, (3, self.Mx, self.My, self.Mzp))
