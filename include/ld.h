@@ -148,6 +148,11 @@ LD_API int ld_rk4_stage(ld_plan* plan, int stage, void* uk, void* y, void* acc, 
 /* End of a time step, F:596-620: the irfft->rfft "reality" round trip (which symmetrises the
  * kz = 0 plane: uk(k) <- (uk(k) + conj uk(-k)) / 2), the div-free projection, and the blow-up
  * and NaN test, which raises LD_STATUS_BLOWUP / LD_STATUS_NONFINITE in the status word. */
+/* While vk is set (a cube-layout 3-vector), every RHS evaluation of the plan (ld_velocity_rhs,
+ * ld_rk4_stage, ld_rk2if_stage) also writes the spectrum of the small-droplet (slow-manifold)
+ * velocity of its stage input, v = u - tps Du/Dt - tps g z with Du/Dt = -grad p + nu lap u
+ * (F:319-321); vk = NULL switches it off. */
+LD_API int ld_slow_manifold(ld_plan* plan, void* vk, double tps, double g);
 LD_API int ld_step_epilogue(ld_plan* plan, void* uk, void* stream);
 
 /* ---- droplets, P:52-111, P:435-511, P:817-837 ----------------------------------------- */
@@ -216,6 +221,38 @@ LD_API int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on the FP32 parameters, then re-packs the BF16 copy. */
 LD_API int ld_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t step, float lr, void* packed,
                        void* stream);
+
+/* ---- the reference's droplet physics (F:278-362, P:514-577, P:817-837), FP64 ---------------- */
+/* clip_zero of F:278-285 on x (m doubles): out = max(x, 0) * mean(x) / mean(max(x, 0)); with
+ * clip_src x itself is clipped too (the reference clips its argument in place).  Deterministic
+ * sums; work holds ld_ref_workspace_doubles() doubles. */
+LD_API int64_t ld_ref_workspace_doubles(void);
+LD_API int ld_clip_zero(double* x, double* out, int64_t m, int clip_src, double* work, void* stream);
+/* RK4 bookkeeping of the physical n field and the droplet coordinates (F:341-360):
+ * y += a x ; z = x + a y. */
+LD_API int ld_axpy(double* y, double a, const double* x, int64_t m, void* stream);
+LD_API int ld_waxpy(double* z, const double* x, double a, const double* y, int64_t m, void* stream);
+/* n-field RHS pieces (F:325-330): nv = n v (planar 3 x N^3), and on the cube
+ * knk = -i k . nvk - fck (the spectra of n v and of the deposited sink fc). */
+LD_API int ld_n_products(ld_plan* plan, const double* n, const double* v, double* nv, void* stream);
+LD_API int ld_n_combine(ld_plan* plan, const void* nvk, const void* fck, void* knk, void* stream);
+/* pRHS of P:817-837 for coord (n, 7) = (x, v, m) with the cosine-interpolated fluid velocity iu,
+ * slow-manifold velocity iv (n, 3) and number density ic (n): kp (n, 7) = (v, (u - v)/(St tau_eta)
+ * - g z, mdot), mdot (n) = growthfactor (1 + sqrt(st_s/St))^2 n |v - v_slow|, St = (m/factor)^(2/3). */
+LD_API int ld_prhs_ref(const double* coord, const double* iu, const double* iv, const double* ic, int64_t n,
+                       double factor, double growthfactor, double st_s, double tau_eta, double g, double* kp,
+                       double* mdot, void* stream);
+/* Positions (n, 3) of the droplet coordinates (n, 7). */
+LD_API int ld_extract_pos(const double* coord, int64_t n, double* pos, void* stream);
+/* Deposition of mdot with the cosine kernel (exterp_cosine_scalar, P:514-577), deterministic:
+ * ld_cell_weights gives each droplet its grid cell (key, with val = index) and its 12 weights;
+ * after a stable sort of (key, val) (ld_radix_sort_u32) and ld_cell_starts (N^3 + 1 starts),
+ * ld_deposit_pull sums, per grid cell, mdot wx wy wz / dx^3 in the reference's order. */
+LD_API int ld_cell_weights(const double* coord, int64_t n, int N, double L, uint32_t* key, uint32_t* val, double* w,
+                           void* stream);
+LD_API int ld_cell_starts(const uint32_t* skey, int64_t n, int64_t ncell, int32_t* cs, void* stream);
+LD_API int ld_deposit_pull(const uint32_t* sval, const int32_t* cs, const double* w, const double* mdot, int N,
+                           double L, double* fc, void* stream);
 
 /* ---- collisions (no counterpart in the reference: droplets there never collide) ----------- */
 /* A collider owns the workspace of the cell-list search for up to nmax droplets on an

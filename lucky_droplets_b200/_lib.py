@@ -67,6 +67,18 @@ SIGNATURES = {
     "ld_gather4": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
     "ld_mlp_partial_floats": (_c_i64, [_c_i64]),
     "ld_copy_async": (_c_i, [_c_p, _c_p, _c_i64, _c_p]),
+    "ld_ref_workspace_doubles": (_c_i64, []),
+    "ld_clip_zero": (_c_i, [_c_p, _c_p, _c_i64, _c_i, _c_p, _c_p]),
+    "ld_axpy": (_c_i, [_c_p, _c_d, _c_p, _c_i64, _c_p]),
+    "ld_waxpy": (_c_i, [_c_p, _c_p, _c_d, _c_p, _c_i64, _c_p]),
+    "ld_n_products": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
+    "ld_n_combine": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
+    "ld_prhs_ref": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_d, _c_d, _c_d, _c_p, _c_p, _c_p]),
+    "ld_extract_pos": (_c_i, [_c_p, _c_i64, _c_p, _c_p]),
+    "ld_cell_weights": (_c_i, [_c_p, _c_i64, _c_i, _c_d, _c_p, _c_p, _c_p, _c_p]),
+    "ld_cell_starts": (_c_i, [_c_p, _c_i64, _c_i64, _c_p, _c_p]),
+    "ld_deposit_pull": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i, _c_d, _c_p, _c_p]),
+    "ld_slow_manifold": (_c_i, [_c_p, _c_p, _c_d, _c_d]),
     "ld_shell_cross": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_divergence_spec": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),

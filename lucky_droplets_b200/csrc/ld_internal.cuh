@@ -55,6 +55,8 @@ struct ld_plan {
   size_t work_bytes = 0;
   void* W1 = nullptr;  // 6 * N * My * Mzp complex
   void* W2 = nullptr;  // 6 * N * N * Mzp complex
+  void* sm_vk = nullptr;          // slow-manifold velocity output of every RHS (none when null)
+  double sm_tps = 0.0, sm_g = 0.0;
   bool prof = false;              // record per-launch events
   std::vector<ProfRec> recs;      // recorded launches
   std::vector<cudaEvent_t> pool;  // reusable events

@@ -186,6 +186,10 @@ template <typename T> struct UpdArgs {
   T h, nu, visc;
   int kc, My, Mzp;
   unsigned* status;
+  // optional slow-manifold velocity of the stage input y (F:319-321):
+  // vk = y + tps (k (k . rhs) / k^2 + visc nu k^2 y), minus vg = tps g N^3 on the mean of w
+  cplx<T>* vk;
+  T tps, vg;
 };
 
 template <typename T, int N, int MODE>
@@ -227,6 +231,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
 #pragma unroll
     for (int cc = 0; cc < 3; ++cc) y[cc] = A.s1[cc * A.cs + idx];
     cplx<T> rhs[3];
+    cplx<T> kd = czero<cplx<T>>();  // (k . rhs) / k^2 before the projection
     if (keep) {
       // forcing on shells kf_lo..kf_hi: factor[kint] * y  (F:253-264)
       T fac = T(0);
@@ -239,7 +244,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
       for (int cc = 0; cc < 3; ++cc) rhs[cc] = cadd(res[cc][m], cscale(y[cc], fac));
       if (k2 > 0) {  // pressure projection, invlap = -1/k^2 (F:309-316)
         const T inv = T(1) / T(k2);
-        cplx<T> kd = cadd(cadd(cscale(rhs[0], kx), cscale(rhs[1], ky)), cscale(rhs[2], kz));
+        kd = cadd(cadd(cscale(rhs[0], kx), cscale(rhs[1], ky)), cscale(rhs[2], kz));
         kd = cscale(kd, inv);
         rhs[0] = csub(rhs[0], cscale(kd, kx));
         rhs[1] = csub(rhs[1], cscale(kd, ky));
@@ -248,6 +253,18 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     } else {
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) rhs[cc] = czero<cplx<T>>();
+    }
+    if (A.vk) {
+      // -i k pk = -k (k . rhs) / k^2 and -nu k^2 y: the reference's Du/Dt of the slow manifold
+      const T lvs = A.visc * A.nu * T(k2);
+      const T kk[3] = {kx, ky, kz};
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        cplx<T> v = czero<cplx<T>>();
+        if (keep) v = cadd(y[cc], cscale(cadd(cscale(kd, kk[cc]), cscale(y[cc], lvs)), A.tps));
+        if (cc == 2 && k2 == 0) v.x -= A.vg;
+        A.vk[cc * A.cs + idx] = v;
+      }
     }
     const T h = A.h;
     if (MODE == UPD_RHS) {

@@ -246,6 +246,7 @@ template <typename T, int N> struct Ops {
     A.ifac = (const T*)p->ifac;
     A.h = T(prm->dt); A.nu = T(prm->nu); A.visc = T(visc);
     A.kc = kc; A.My = My; A.Mzp = Mzp; A.status = p->status;
+    A.vk = (C*)p->sm_vk; A.tps = T(p->sm_tps); A.vg = T(p->sm_tps * p->sm_g * (double)N * N * N);
     ProfScope ps(p, KID_XFWD_UPD, s);
     auto k = k_xfwd_update<T, N, MODE>;
     if (int rc = set_smem(k, COL_SMEM)) return rc;

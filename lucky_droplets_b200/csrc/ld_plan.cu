@@ -255,6 +255,14 @@ int ld_rk4_stage(ld_plan* p, int stage, void* uk, void* y, void* acc, void* u_ou
   return table_of(p)->rhs(p, ld::UPD_RK4_1 + stage - 1, uk, in, acc, y, u_out, prm, 1.0, S(stream));
 }
 
+int ld_slow_manifold(ld_plan* p, void* vk, double tps, double g) {
+  if (int rc = check_plan(p)) return rc;
+  p->sm_vk = vk;
+  p->sm_tps = tps;
+  p->sm_g = g;
+  return LD_OK;
+}
+
 int ld_step_epilogue(ld_plan* p, void* uk, void* stream) {
   if (int rc = check_plan(p)) return rc;
   if (!uk) return ld_fail(LD_ERR_ARG, "ld_step_epilogue: bad arguments");
