@@ -159,6 +159,72 @@ k_colfft(Ld ld, St st, int ncols, int nf, const cplx<T>* __restrict__ tw) {
   }
 }
 
+// Pipelined column pass over plain strided rows: a CTA loops over items (column block, field,
+// outer index), items of neighbouring CTAs adjacent in memory.  While an item is transformed, the
+// rows of the CTA's next item stream into the other shared buffer with 16-byte cp.async copies;
+// the buffer an item was staged in serves as its FFT exchange buffer once its values sit in
+// registers.  Rows the loader's row map drops (r < 0) and columns past ncols are not copied.
+template <typename T, int N, bool INV, class St>
+__global__ void __launch_bounds__(Cfg<N>::COL_THREADS, 3)
+k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>* __restrict__ tw) {
+  constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
+  constexpr int CPR = TB * (int)sizeof(cplx<T>) / 16;  // 16-byte chunks of a full row segment
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf0 = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* buf1 = buf0 + N * TB;
+  const int c = threadIdx.x % TB, j = threadIdx.x / TB;
+  const int ncb = (ncols + TB - 1) / TB;
+  const long long nitems = (long long)ncb * nf * nouter;
+  auto prefetch = [&](long long it, cplx<T>* dst) {
+    const int cb = (int)(it % ncb);
+    const long long rest = it / ncb;
+    const int f = (int)(rest % nf), o = (int)(rest / nf);
+    const int col0 = cb * TB;
+    const int w = ncols - col0 < TB ? ncols - col0 : TB;
+    const int cpr = w * (int)sizeof(cplx<T>) / 16;
+    for (int q = threadIdx.x; q < N * CPR; q += blockDim.x) {
+      const int n = q / CPR, k = q - n * CPR;
+      if (k >= cpr) continue;
+      const int r = in.kc < 0 ? n : crow(n, N, in.kc);
+      if (r < 0) continue;
+      const char* src = reinterpret_cast<const char*>(in.p + in.at(f, o, r, col0)) + 16 * k;
+      const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst + n * TB) + 16 * k);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  long long it = blockIdx.x;
+  if (it < nitems) prefetch(it, buf0);
+  int b = 0;
+  for (; it < nitems; it += gridDim.x) {
+    cplx<T>* cur = b ? buf1 : buf0;
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
+    const int cb = (int)(it % ncb);
+    const long long rest = it / ncb;
+    const int f = (int)(rest % nf), o = (int)(rest / nf);
+    const int col = cb * TB + c;
+    const bool ok = col < ncols;
+    cplx<T> a[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int n = j + NT * m;
+      const int r = in.kc < 0 ? n : crow(n, N, in.kc);
+      a[m] = (ok && r >= 0) ? cscale(cur[n * TB + c], in.scale) : czero<cplx<T>>();
+    }
+    __syncthreads();  // every value is in registers: cur becomes the exchange buffer
+    if (it + gridDim.x < nitems) prefetch(it + gridDim.x, b ? buf0 : buf1);
+    fft_run<T, N, E, INV, false>(a, cur + c, TB, j, tw, SyncBlock());
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) st(f, o, j + NT * m, col, a[m]);
+    }
+    __syncthreads();
+    b ^= 1;
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // ------------------------------------------------------------------------------------------
 // k-space update epilogue of the forward x pass (F:304-316 + the time integrators)
 // ------------------------------------------------------------------------------------------

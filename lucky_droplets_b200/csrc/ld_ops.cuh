@@ -48,6 +48,33 @@ template <typename T, int N> struct Ops {
     return LD_OK;
   }
 
+  // Column pass over plain strided rows: the pipelined kernel where two staging buffers fit.
+  static constexpr bool PIPE = 2 * COL_SMEM <= 72 * 1024;
+  template <bool INV, class St>
+  static int colpass_rows(ld_plan* p, int kid, RowsIO<T> in, St st, int ncols, int nf, int nouter, const C* tw,
+                          cudaStream_t s) {
+    if constexpr (!PIPE) {
+      return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
+    } else {
+      ProfScope ps(p, kid, s);
+      auto k = k_colfft_pipe<T, N, INV, St>;
+      if (int rc = set_smem(k, 2 * COL_SMEM)) return rc;
+      static int occ = 0;
+      if (occ == 0) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, Cfg<N>::COL_THREADS, 2 * COL_SMEM);
+        if (e != cudaSuccess || occ < 1) occ = 1;
+      }
+      int dev = 0, sms = 148;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      const long long items = cdiv(ncols, TB) * (long long)nf * nouter;
+      const long long grid = items < (long long)sms * occ ? items : (long long)sms * occ;
+      k<<<(unsigned)grid, Cfg<N>::COL_THREADS, 2 * COL_SMEM, s>>>(in, st, ncols, nf, nouter, tw);
+      LD_LAUNCH_CHECK();
+      return LD_OK;
+    }
+  }
+
   static RowsIO<T> io(const void* p, long long fs, long long os, int rs, int kc, T scale = T(1)) {
     RowsIO<T> r;
     r.p = (C*)p; r.fs = fs; r.os = os; r.rs = rs; r.kc = kc; r.scale = scale;
@@ -219,7 +246,7 @@ template <typename T, int N> struct Ops {
     // inverse y pass
     auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
     auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
-    if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, 6, N, tw, s)) return rc;
+    if (int rc = colpass_rows<true>(p, KID_YINV, yin, StRows<T, N>{yout}, Mzp, 6, N, tw, s)) return rc;
     // fused z pass: u, w -> u x w  (W2 -> W1 as (3, N*N, Mzp))
     {
       ProfScope ps(p, KID_ZCROSS, s);
@@ -237,7 +264,7 @@ template <typename T, int N> struct Ops {
     // forward y pass (W1 -> W2 as (3, N, My, Mzp))
     auto fyin = io(W1, w2s, (long long)N * Mzp, Mzp, -1);
     auto fyout = io(W2, w1s, (long long)My * Mzp, Mzp, kc);
-    if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{fyin}, StRows<T, N>{fyout}, Mzp, 3, N, tw, s)) return rc;
+    if (int rc = colpass_rows<false>(p, KID_YFWD, fyin, StRows<T, N>{fyout}, Mzp, 3, N, tw, s)) return rc;
     // forward x pass + k-space update
     UpdArgs<T> A;
     A.nl = W2; A.nls = w1s;
