@@ -7,11 +7,13 @@
 //
 // Features of a point with stencil values s (192 = 3 components x 64 taps, tap order
 // c*64 + a*16 + b*4 + q for offsets a, b, q in -1..2 along x, y, z) and cell offsets t (3):
-//   D_c      = (P x P x P) s_c    per component: the orthonormal discrete polynomial basis of
-//              orders 0..3 on 4 points along each axis (FP32)
+//   D_c      = (P x P x P) s_c    per component: the discrete polynomial basis of orders 0..3
+//              on 4 points along each axis, rows (1,1,1,1), (-3,-1,1,3), (1,-1,-1,1), (-1,3,-3,1)
+//              (orthogonal; their norms are absorbed by the feature scales) (FP32)
 //   scale    = RMS of all 192 coefficients (scale mode 0), or of the 162 coefficients of total
 //              order >= 3 (mode 1: tracks the small-scale content the correction depends on,
-//              so the normalised targets drift less while a flow develops), + 1e-30
+//              so the normalised targets drift less while a flow develops), + 1e-30, both in
+//              the basis above
 //   x[0:192] = D / scale * fs,  x[192:195] = t - 0.5,  x[195:208] = 0     (canonical frame)
 //   u(point) = tricubic(s, t) + scale * os * MLP(x)                     (back in the grid frame)
 // Canonical frame: the exact correction is equivariant under the 48 reflections and axis
@@ -130,14 +132,15 @@ __device__ __forceinline__ void warp_gemm(float (*acc)[4], const bf16* A, int ld
 // warp-cooperative inference kernel; every element goes through the same arithmetic in both,
 // so training and inference features agree bit for bit.
 
-// Orthonormal discrete polynomial basis on 4 points (orders 0..3), in place.
+// Discrete polynomial basis on 4 points (orders 0..3, rows (1,1,1,1), (-3,-1,1,3), (1,-1,-1,1),
+// (-1,3,-3,1): orthogonal, not normalised; the feature scales absorb the norms), in place.
 __device__ __forceinline__ void poly4(float* v, int stride) {
   const float s0 = v[0], s1 = v[stride], s2 = v[2 * stride], s3 = v[3 * stride];
-  const float r20 = 0.22360679774997896f;  // 1/sqrt(20)
-  v[0] = 0.5f * ((s0 + s1) + (s2 + s3));
-  v[stride] = r20 * ((3.f * (s3 - s0)) + (s2 - s1));
-  v[2 * stride] = 0.5f * ((s0 - s1) - (s2 - s3));
-  v[3 * stride] = r20 * ((s3 - s0) + 3.f * (s1 - s2));
+  const float a = s0 + s3, b = s1 + s2, c = s3 - s0, d = s2 - s1;
+  v[0] = a + b;
+  v[stride] = fmaf(3.f, c, d);
+  v[2 * stride] = a - b;
+  v[3 * stride] = fmaf(-3.f, d, c);
 }
 
 // Frame code: bits 0-5 hold p[0..2] (canonical axis k <- grid axis p[k], 2 bits each), bits 6-8
@@ -186,8 +189,9 @@ __device__ __forceinline__ void point_frame(double px, double py, double pz, int
   f.code = make_frame(toff, f.tc);
 }
 
-// Tricubic weights of the canonical offsets in the polynomial basis (per canonical axis): the
-// tricubic value is sum_i D_i wh0[i0] wh1[i1] wh2[i2] (P orthonormal: w.s = (P w).(P s)).
+// Tricubic weights of the canonical offsets in the polynomial basis (per canonical axis): with
+// U the basis above (row norms^2 4, 20, 4, 20), w.s = sum_i (U w)_i (U s)_i / |U_i|^2, so the
+// tricubic value is sum_i D_i wh0[i0] wh1[i1] wh2[i2] with wh = (U w) / |U|^2.
 __device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4]) {
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
@@ -197,6 +201,10 @@ __device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4])
     wh[k][2] = -(t + 1.f) * t * (t - 2.f) / 2.f;
     wh[k][3] = (t + 1.f) * t * (t - 1.f) / 6.f;
     poly4(wh[k], 1);
+    wh[k][0] *= 0.25f;
+    wh[k][1] *= 0.05f;
+    wh[k][2] *= 0.25f;
+    wh[k][3] *= 0.05f;
   }
 }
 
@@ -223,11 +231,21 @@ __device__ __forceinline__ CompSums comp_sums(const float (&v)[64], const float 
   CompSums p{0.f, 0.f, 0.f};
 #pragma unroll
   for (int j = 0; j < 64; ++j) {
-    const float v2 = v[j] * v[j];
-    p.ss += v2;
-    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh += v2;
-    p.tr += ((wh[0][j >> 4] * wh[1][(j >> 2) & 3]) * wh[2][j & 3]) * v[j];
+    p.ss = fmaf(v[j], v[j], p.ss);
+    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh = fmaf(v[j], v[j], p.sh);
   }
+  // tricubic value by separable contraction: z, then y, then x
+  float t1[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q)
+    t1[q] = fmaf(wh[2][3], v[4 * q + 3], fmaf(wh[2][2], v[4 * q + 2], fmaf(wh[2][1], v[4 * q + 1], wh[2][0] * v[4 * q])));
+  float tr = 0.f;
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const float t2 = fmaf(wh[1][3], t1[4 * a + 3], fmaf(wh[1][2], t1[4 * a + 2], fmaf(wh[1][1], t1[4 * a + 1], wh[1][0] * t1[4 * a])));
+    tr = fmaf(wh[0][a], t2, tr);
+  }
+  p.tr = tr;
   return p;
 }
 
@@ -496,30 +514,53 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
 }
 
 // ---- MLP forward on the 5th-generation tensor cores --------------------------------------------
-// Persistent CTA per SM, 16 warps.  Per tile of TM = 128 droplets:
-//   X tile (128 x 208 bf16, tile layout) arrives by one bulk asynchronous copy, double-buffered;
-//   layer 1: 13 tcgen05.mma (M 128, N 128, K 16) from X and W1 into TMEM columns 0..127;
-//   epilogue: 16 warps read the accumulators (tcgen05.ld; warp w: TMEM lanes 32 (w % 4), columns
-//   32 (w / 4)), add b1, SiLU, bf16 -> H (tile layout);
-//   layer 2: 8 MMAs from H and W2 into TMEM 0..127; epilogue as above -> H;
-//   layer 3: 8 MMAs (N 16: W3 padded) into TMEM 128..143; warps 0..3 write
-//   out = tricubic + scale * os * MLP back in the grid frame.
-// One thread issues the MMAs and commits them to an mbarrier that all threads wait on (bounded:
-// a wait that runs out raises LD_STATUS_WAIT_TIMEOUT and the CTA frees its TMEM and returns).
+// Persistent CTA per SM, 16 warps in two groups of 8.  The CTA's tiles (TM = 128 droplets each)
+// alternate between the groups, so that one group's epilogues overlap the other group's MMAs.
+// Per tile:
+//   X tile (128 x 208 bf16, tile layout) arrives by one bulk asynchronous copy into the single X
+//   buffer; the group whose layer 1 has just consumed X issues the copy of the CTA's next tile;
+//   layer 1: 13 tcgen05.mma (M 128, N 128, K 16) from X and W1 into the group's TMEM columns;
+//   epilogue: the group's 8 warps read the accumulators (tcgen05.ld; warp w: TMEM lanes
+//   32 (w % 4), columns 64 ((w / 4) % 2)), add b1, SiLU, bf16 -> the group's H (tile layout);
+//   layer 2: 8 MMAs from H and W2; epilogue as above -> H;
+//   layer 3: 8 MMAs (N 16: W3 padded); 4 warps write out = tricubic + scale * os * MLP in the grid
+//   frame.
+// The group's leader issues its MMAs and commits them to the group's mbarrier; group barriers are
+// named barriers.  Every wait is bounded: a wait that runs out raises LD_STATUS_WAIT_TIMEOUT and
+// the group stops; the CTA frees its tensor memory.
 constexpr int FT_THREADS = 512;
+constexpr int FT_GROUP = 256;                         // threads of a group
 constexpr int N3P = 16;                               // layer-3 N padded for M = 128
 constexpr int SM_W1 = 0;
 constexpr int SM_W2 = SM_W1 + H * K1 * 2;             // 53248
 constexpr int SM_W3 = SM_W2 + H * H * 2;              // + 32768
-constexpr int SM_X0 = SM_W3 + N3P * H * 2;            // + 4096
-constexpr int SM_X1 = SM_X0 + TILE_X_BYTES;
-constexpr int SM_H = SM_X1 + TILE_X_BYTES;
-constexpr int SM_BIAS = SM_H + TM * H * 2;            // b1[128], b2[128], b3[16]
-constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma
-constexpr int SM_TMEM = SM_BAR + 3 * 8;
+constexpr int SM_X = SM_W3 + N3P * H * 2;             // + 4096
+constexpr int SM_H0 = SM_X + TILE_X_BYTES;
+constexpr int SM_H1 = SM_H0 + TM * H * 2;
+constexpr int SM_BIAS = SM_H1 + TM * H * 2;           // b1[128], b2[128], b3[16]
+constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma[2]
+constexpr int SM_TMEM = SM_BAR + 4 * 8;
 constexpr size_t SMEM_FWD = SM_TMEM + 16;
-constexpr unsigned TMEM_COLS = 256;
+constexpr unsigned TMEM_COLS = 512;                   // group g: columns 256 g .. 256 g + 143
 constexpr unsigned kWaitLimitMlp = 1u << 24;
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(FT_GROUP) : "memory");
+}
+
+// group barrier that returns the OR of v over the group's threads (group-uniform decisions)
+__device__ __forceinline__ bool group_or(int g, bool v) {
+  unsigned r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, %2, %3, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((unsigned)v), "r"(1 + g), "r"(FT_GROUP)
+      : "memory");
+  return r != 0;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(FT_THREADS, 1)
@@ -528,7 +569,11 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
                  unsigned* __restrict__ status) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int g = warp >> 3, gw = warp & 7;             // group, warp within the group
+  const bool leader = (tid & (FT_GROUP - 1)) == 0;
   float* bias = reinterpret_cast<float*>(sm + SM_BIAS);
+  // copy i of the X buffer completes on bar_x[i % 2]: group g waits only on bar_x[g], so every
+  // barrier's k-th wait has parity k % 2 (a fresh barrier counts parity 1 as complete)
   uint64_t* bar_x = reinterpret_cast<uint64_t*>(sm + SM_BAR);
   uint64_t* bar_mma = bar_x + 2;
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + SM_TMEM);
@@ -554,7 +599,8 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   if (tid == 0) {
     mbar_init(&bar_x[0], 1);
     mbar_init(&bar_x[1], 1);
-    mbar_init(bar_mma, 1);
+    mbar_init(&bar_mma[0], 1);
+    mbar_init(&bar_mma[1], 1);
     mbar_init_fence();
   }
   if (warp == 0) {
@@ -565,112 +611,108 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const unsigned tmem = *tmem_slot;
+  const unsigned tmem = *tmem_slot + 256u * (unsigned)g;
+  unsigned char* Hs = sm + (g ? SM_H1 : SM_H0);
   const float os = params[OFF_OS];
   const long long ntiles = (n + TM - 1) / TM;
+  const long long mine = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // CTA's tiles
   constexpr unsigned ID1 = umma_idesc_bf16(128, 128), ID3 = umma_idesc_bf16(128, N3P);
-  unsigned ph_mma = 0;
-  bool failed = false;
-  if (tid == 0 && (long long)blockIdx.x < ntiles) {
+  if (tid == 0 && mine > 0) {
     mbar_expect_tx(&bar_x[0], TILE_X_BYTES);
-    bulk_g2s(sm + SM_X0, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
+    bulk_g2s(sm + SM_X, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
   }
-  int it = 0;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-    const int b = it & 1;
-    unsigned char* Xs = sm + (b ? SM_X1 : SM_X0);
-    // prefetch the next tile into the other buffer (its last reader, layer 1 of the previous tile,
-    // has completed)
-    if (tid == 0 && tile + gridDim.x < ntiles) {
-      mbar_expect_tx(&bar_x[b ^ 1], TILE_X_BYTES);
-      bulk_g2s(sm + (b ? SM_X0 : SM_X1), Xg + (tile + gridDim.x) * (long long)TILE_X_BYTES, TILE_X_BYTES,
-               &bar_x[b ^ 1]);
-    }
-    failed = __syncthreads_or(!mbar_wait_bounded(&bar_x[b], (unsigned)(it >> 1) & 1u, kWaitLimitMlp)) != 0;
-    if (failed) break;  // block-uniform
-    // layer 1
-    if (tid == 0) {
+  unsigned ph = 0;
+  bool failed = false;
+  for (long long i = g; i < mine && !failed; i += 2) {
+    const long long tile = blockIdx.x + i * (long long)gridDim.x;
+    // X of this tile (the i-th copy into the X buffer, on bar_x[g], the group's (i/2)-th wait);
+    // failures are made group-uniform
+    failed = group_or(g, !mbar_wait_bounded(&bar_x[g], (unsigned)((i >> 1) & 1), kWaitLimitMlp));
+    if (failed) break;
+    if (leader) {
       tc_fence_after();
 #pragma unroll 1
       for (int k = 0; k < K1 / 16; ++k)
-        umma_bf16(tmem, umma_desc(Xs + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+        umma_bf16(tmem, umma_desc(sm + SM_X + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
                   umma_desc(sm + SM_W1 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
-      umma_commit(bar_mma);
+      umma_commit(&bar_mma[g]);
     }
-    for (int layer = 0; layer < 2; ++layer) {
-      failed = __syncthreads_or(!mbar_wait_bounded(bar_mma, ph_mma, kWaitLimitMlp)) != 0;
-      ph_mma ^= 1u;
-      if (failed) break;
+    for (int layer = 0; layer < 3; ++layer) {
+      failed = group_or(g, !mbar_wait_bounded(&bar_mma[g], ph, kWaitLimitMlp));
+      ph ^= 1u;
       tc_fence_after();
-      // epilogue: rows 32 (warp & 3) + lane, columns 32 (warp >> 2) .. + 31
-      {
-        const int sub = warp & 3, quarter = warp >> 2;
+      if (layer == 0 && leader && !failed && i + 1 < mine) {
+        // layer 1 has consumed X: bring in the CTA's next tile (the other group's, on its barrier)
+        mbar_expect_tx(&bar_x[g ^ 1], TILE_X_BYTES);
+        bulk_g2s(sm + SM_X, Xg + (tile + gridDim.x) * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[g ^ 1]);
+      }
+      if (failed) break;
+      if (layer < 2) {
+        // epilogue: rows 32 (gw % 4) + lane, columns 64 (gw / 4) .. + 63
+        const int sub = gw & 3, half = gw >> 2;
         const int row = 32 * sub + lane;
-        const int col0 = 32 * quarter;
-        const float4* bl = reinterpret_cast<const float4*>(bias + layer * H + col0);
-        float v[32];
-        tmem_ld32(tmem + ((unsigned)(32 * sub) << 16) + (unsigned)col0, v);
-        unsigned w[16];
+        const float* bl = bias + layer * H;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const float4 b4 = bl[j];
-          w[2 * j] = pack2(silu(v[4 * j] + b4.x), silu(v[4 * j + 1] + b4.y));
-          w[2 * j + 1] = pack2(silu(v[4 * j + 2] + b4.z), silu(v[4 * j + 3] + b4.w));
+        for (int cc = 0; cc < 2; ++cc) {
+          const int col0 = 64 * half + 32 * cc;
+          float v[32];
+          tmem_ld32(tmem + ((unsigned)(32 * sub) << 16) + (unsigned)col0, v);
+          const float4* b4p = reinterpret_cast<const float4*>(bl + col0);
+          unsigned w[16];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float4 b4 = b4p[j];
+            w[2 * j] = pack2(silu(v[4 * j] + b4.x), silu(v[4 * j + 1] + b4.y));
+            w[2 * j + 1] = pack2(silu(v[4 * j + 2] + b4.z), silu(v[4 * j + 3] + b4.w));
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(Hs + blk_off(row, col0 / 8 + q, TM)) =
+                make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
         }
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-          *reinterpret_cast<uint4*>(sm + SM_H + blk_off(row, col0 / 8 + q, TM)) =
-              make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
-      }
-      fence_proxy_async_smem();
-      tc_fence_before();
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        if (layer == 0) {
+        fence_proxy_async_smem();
+        tc_fence_before();
+        group_sync(g);
+        if (leader) {
+          tc_fence_after();
+          if (layer == 0) {
 #pragma unroll 1
-          for (int k = 0; k < H / 16; ++k)
-            umma_bf16(tmem, umma_desc(sm + SM_H + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
-                      umma_desc(sm + SM_W2 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
-        } else {
+            for (int k = 0; k < H / 16; ++k)
+              umma_bf16(tmem, umma_desc(Hs + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+                        umma_desc(sm + SM_W2 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
+          } else {
 #pragma unroll 1
-          for (int k = 0; k < H / 16; ++k)
-            umma_bf16(tmem + 128, umma_desc(sm + SM_H + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
-                      umma_desc(sm + SM_W3 + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), ID3, k > 0);
+            for (int k = 0; k < H / 16; ++k)
+              umma_bf16(tmem + 128, umma_desc(Hs + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
+                        umma_desc(sm + SM_W3 + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), ID3, k > 0);
+          }
+          umma_commit(&bar_mma[g]);
         }
-        umma_commit(bar_mma);
-      }
-    }
-    if (failed) break;
-    failed = __syncthreads_or(!mbar_wait_bounded(bar_mma, ph_mma, kWaitLimitMlp)) != 0;
-    ph_mma ^= 1u;
-    if (failed) break;
-    tc_fence_after();
-    if (warp < 4) {
-      const int row = 32 * warp + lane;
-      float v[16];
-      tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + 128u, v);
-      const long long i = tile * TM + row;
-      if (i < n) {
-        const float* ax = auxg + i * 8;
-        const int code = __float_as_int(ax[4]);
+      } else if (gw < 4) {
+        const int row = 32 * gw + lane;
+        float v[16];
+        tmem_ld16(tmem + ((unsigned)(32 * gw) << 16) + 128u, v);
+        const long long ii = tile * TM + row;
+        if (ii < n) {
+          const float* ax = auxg + ii * 8;
+          const int code = __float_as_int(ax[4]);
 #pragma unroll
-        for (int c = 0; c < D_OUT; ++c) {
-          const int cg = frame_perm(code, c);
-          const float y = v[c] + bias[2 * H + c];
-          out[3 * i + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
+          for (int c = 0; c < D_OUT; ++c) {
+            const int cg = frame_perm(code, c);
+            const float y = v[c] + bias[2 * H + c];
+            out[3 * ii + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
+          }
         }
       }
     }
     tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
+    group_sync(g);  // the group's TMEM and H are free for its next tile
   }
-  if (failed && tid == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
+  if (failed && (tid & (FT_GROUP - 1)) == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
+  if (warp == 0) tmem_dealloc(*tmem_slot, TMEM_COLS);
 }
 
 // ---- training samples ------------------------------------------------------------------------------

@@ -3,8 +3,8 @@
 TEST INFRASTRUCTURE ONLY.
 
 Network: 195 inputs (the 4x4x4 stencil of (u, v, w) in tap order (c, a, b, q) -> c*64 + a*16 + b*4
-+ q, transformed per component into the orthonormal discrete polynomial basis of orders 0..3 along
-each axis, divided by the stencil RMS and multiplied by fixed per-coefficient scales; then the
++ q, transformed per component into the (orthogonal, unnormalised) discrete polynomial basis of
+orders 0..3 along each axis, divided by the stencil RMS and multiplied by fixed per-coefficient scales; then the
 three fractional cell offsets minus 1/2) -> 128 SiLU -> 128 SiLU -> 3, times a fixed output
 scale.  The GPU kernels feed
 BF16 operands to the tensor cores with FP32 accumulation; this oracle rounds the same operands to
@@ -26,9 +26,8 @@ def bf16(x):
     return out
 
 
-# orthonormal discrete polynomials on 4 points, orders 0..3 (rows)
+# discrete polynomials on 4 points, orders 0..3 (rows; orthogonal, not normalised)
 P4 = np.array([[1, 1, 1, 1], [-3, -1, 1, 3], [1, -1, -1, 1], [-1, 3, -3, 1]], np.float64)
-P4 /= np.linalg.norm(P4, axis=1)[:, None]
 
 
 def frames(t):
@@ -70,7 +69,7 @@ _ORDER = (np.arange(64) >> 4) + ((np.arange(64) >> 2) & 3) + (np.arange(64) & 3)
 def features(st, t, fs, scale_mode=1):
     """Network inputs (n, 195) from stencils st (n, 192), offsets t (n, 3) and feature scales fs
     (64): returns (X rounded to BF16, scale, perm, refl).  scale: RMS of all coefficients (mode 0)
-    or of those of total order >= 3 (mode 1)."""
+    or of those of total order >= 3 (mode 1), in the polynomial basis."""
     n = st.shape[0]
     v = st.reshape(n, 3, 4, 4, 4)
     d = np.einsum("ia,jb,kq,ncabq->ncijk", P4, P4, P4, v, optimize=True)
@@ -78,7 +77,7 @@ def features(st, t, fs, scale_mode=1):
     if scale_mode:
         scale = np.sqrt((d64[:, :, _ORDER >= 3] ** 2).sum(axis=(1, 2)) / 162.0) + 1e-30
     else:
-        scale = np.sqrt((st ** 2).mean(axis=1)) + 1e-30
+        scale = np.sqrt((d64 ** 2).sum(axis=(1, 2)) / 192.0) + 1e-30
     perm, refl, tc = frames(t)
     out = np.empty((n, 3, 4, 4, 4))
     # reflection of grid axis g multiplies order-j coefficients along g by (-1)^j

