@@ -148,6 +148,13 @@ LD_API int ld_rk4_stage(ld_plan* plan, int stage, void* uk, void* y, void* acc, 
 /* End of a time step, F:596-620: the irfft->rfft "reality" round trip (which symmetrises the
  * kz = 0 plane: uk(k) <- (uk(k) + conj uk(-k)) / 2), the div-free projection, and the blow-up
  * and NaN test, which raises LD_STATUS_BLOWUP / LD_STATUS_NONFINITE in the status word. */
+/* Autotuner of the plan's strided-row (y) transform passes (no counterpart in the reference):
+ * times each launch variant on the plan's workspace - ms[8] = [inverse, forward] x [one-shot
+ * tiles, pipelined with 1, 2, 3 CTAs per SM] (-1: not available) - and keeps the fastest;
+ * choice[2] receives it (0 one-shot, k pipelined with k CTAs per SM).  Synchronises the stream.
+ * ld_plan_set_tuning applies a choice found on another plan of the same N and precision. */
+LD_API int ld_plan_autotune(ld_plan* plan, double* ms, int32_t* choice, void* stream);
+LD_API int ld_plan_set_tuning(ld_plan* plan, const int32_t* choice);
 /* While vk is set (a cube-layout 3-vector), every RHS evaluation of the plan (ld_velocity_rhs,
  * ld_rk4_stage, ld_rk2if_stage) also writes the spectrum of the small-droplet (slow-manifold)
  * velocity of its stage input, v = u - tps Du/Dt - tps g z with Du/Dt = -grad p + nu lap u

@@ -79,6 +79,8 @@ SIGNATURES = {
     "ld_cell_starts": (_c_i, [_c_p, _c_i64, _c_i64, _c_p, _c_p]),
     "ld_deposit_pull": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i, _c_d, _c_p, _c_p]),
     "ld_slow_manifold": (_c_i, [_c_p, _c_p, _c_d, _c_d]),
+    "ld_plan_autotune": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
+    "ld_plan_set_tuning": (_c_i, [_c_p, _c_p]),
     "ld_shell_cross": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_divergence_spec": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),

@@ -55,6 +55,9 @@ struct ld_plan {
   size_t work_bytes = 0;
   void* W1 = nullptr;  // 6 * N * My * Mzp complex
   void* W2 = nullptr;  // 6 * N * N * Mzp complex
+  // launch choices of the strided-row (y) passes of the RHS, set by ld_plan_autotune:
+  // -1 pipelined with the occupancy-limited grid, 0 one-shot tiles, k > 0 pipelined, k CTAs/SM
+  int tune_y[2] = {-1, -1};  // [inverse, forward]
   void* sm_vk = nullptr;          // slow-manifold velocity output of every RHS (none when null)
   double sm_tps = 0.0, sm_g = 0.0;
   bool prof = false;              // record per-launch events
@@ -91,6 +94,9 @@ struct OpsTable {
                 cudaStream_t);
   int (*dstage)(ld_plan*, int stage, int method, const void* u, double* pos, void* vel, const void* tau,
                 void* a1, long long n, double h, double g, cudaStream_t);
+  // times every launch variant of the y passes (ms[2][4]: one-shot, pipelined with 1..3 CTAs/SM)
+  // and keeps the fastest in the plan
+  int (*autotune)(ld_plan*, cudaStream_t, double* ms);
 };
 
 #define LD_FOR_EACH_INSTANCE(X) \

@@ -52,10 +52,12 @@ template <typename T, int N> struct Ops {
   static constexpr bool PIPE = 2 * COL_SMEM <= 72 * 1024;
   template <bool INV, class St>
   static int colpass_rows(ld_plan* p, int kid, RowsIO<T> in, St st, int ncols, int nf, int nouter, const C* tw,
-                          cudaStream_t s) {
+                          cudaStream_t s, int variant = -2) {
+    const int choice = variant != -2 ? variant : p->tune_y[INV ? 0 : 1];
     if constexpr (!PIPE) {
       return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
     } else {
+      if (choice == 0) return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
       ProfScope ps(p, kid, s);
       auto k = k_colfft_pipe<T, N, INV, St>;
       if (int rc = set_smem(k, 2 * COL_SMEM)) return rc;
@@ -68,7 +70,8 @@ template <typename T, int N> struct Ops {
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       const long long items = cdiv(ncols, TB) * (long long)nf * nouter;
-      const long long grid = items < (long long)sms * occ ? items : (long long)sms * occ;
+      const int per_sm = choice > 0 && choice < occ ? choice : occ;
+      const long long grid = items < (long long)sms * per_sm ? items : (long long)sms * per_sm;
       k<<<(unsigned)grid, Cfg<N>::COL_THREADS, 2 * COL_SMEM, s>>>(in, st, ncols, nf, nouter, tw);
       LD_LAUNCH_CHECK();
       return LD_OK;
@@ -226,6 +229,48 @@ template <typename T, int N> struct Ops {
     return LD_OK;
   }
 
+  // ---- autotuner of the y passes: every launch variant timed on the plan's workspace ------------
+  static int autotune(ld_plan* p, cudaStream_t s, double* ms) {
+    const int My = p->My, Mzp = p->Mzp, kc = p->kc;
+    const C* tw = (const C*)p->tw;
+    C* W1 = (C*)p->W1;
+    C* W2 = (C*)p->W2;
+    const long long NN = (long long)N * N, w1s = (long long)N * My * Mzp, w2s = NN * Mzp;
+    cudaEvent_t a, b;
+    LD_CUDA_CHECK(cudaEventCreate(&a));
+    LD_CUDA_CHECK(cudaEventCreate(&b));
+    const int nv = PIPE ? 4 : 1;
+    for (int pass = 0; pass < 2; ++pass) {
+      double best = 1e30;
+      int pick = -1;
+      for (int v = 0; v < 4; ++v) {
+        ms[4 * pass + v] = -1.0;
+        if (v >= nv) continue;
+        auto run = [&]() -> int {
+          if (pass == 0)
+            return colpass_rows<true>(p, KID_YINV, io(W1, w1s, (long long)My * Mzp, Mzp, kc),
+                                      StRows<T, N>{io(W2, w2s, (long long)N * Mzp, Mzp, -1)}, Mzp, 6, N, tw, s, v);
+          return colpass_rows<false>(p, KID_YFWD, io(W1, w2s, (long long)N * Mzp, Mzp, -1),
+                                     StRows<T, N>{io(W2, w1s, (long long)My * Mzp, Mzp, kc)}, Mzp, 3, N, tw, s, v);
+        };
+        if (int rc = run()) return rc;  // warm-up
+        LD_CUDA_CHECK(cudaEventRecord(a, s));
+        for (int r = 0; r < 5; ++r)
+          if (int rc = run()) return rc;
+        LD_CUDA_CHECK(cudaEventRecord(b, s));
+        LD_CUDA_CHECK(cudaEventSynchronize(b));
+        float t = 0.f;
+        LD_CUDA_CHECK(cudaEventElapsedTime(&t, a, b));
+        ms[4 * pass + v] = t / 5.0;
+        if (t / 5.0 < best) { best = t / 5.0; pick = v; }
+      }
+      p->tune_y[pass] = PIPE ? pick : 0;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return LD_OK;
+  }
+
   // ---- RHS pipeline: y (stage input) -> update epilogue ------------------------------------------
   template <int MODE>
   static int rhs(ld_plan* p, C* s0, C* s1, C* s2, T* uout, const ld_flow_params* prm, double visc,
@@ -356,6 +401,7 @@ template <typename T, int N> struct Table {
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
+  static int autotune(ld_plan* p, cudaStream_t s, double* ms) { return O::autotune(p, s, ms); }
   static int rhs(ld_plan* p, int mode, void* s0, void* s1, void* s2, void* s3, void* uout,
                  const ld_flow_params* prm, double visc, cudaStream_t s) {
     C *a = (C*)s0, *b = (C*)s1, *c = (C*)s2, *d = (C*)s3;
@@ -390,7 +436,7 @@ template <typename T, int N> struct Table {
   }
   static const OpsTable* get() {
     static const OpsTable t = {rfft_full, irfft_full, irfft_cube, rfft_cube, to_cube, from_cube,
-                               shell_spectrum, rhs, epilogue, gather, dstage};
+                               shell_spectrum, rhs, epilogue, gather, dstage, autotune};
     return &t;
   }
 };

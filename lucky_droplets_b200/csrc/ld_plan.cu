@@ -255,6 +255,25 @@ int ld_rk4_stage(ld_plan* p, int stage, void* uk, void* y, void* acc, void* u_ou
   return table_of(p)->rhs(p, ld::UPD_RK4_1 + stage - 1, uk, in, acc, y, u_out, prm, 1.0, S(stream));
 }
 
+int ld_plan_autotune(ld_plan* p, double* ms, int32_t* choice, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  double t[8];
+  if (int rc = table_of(p)->autotune(p, S(stream), t)) return rc;
+  if (ms)
+    for (int i = 0; i < 8; ++i) ms[i] = t[i];
+  if (choice) { choice[0] = p->tune_y[0]; choice[1] = p->tune_y[1]; }
+  return LD_OK;
+}
+
+int ld_plan_set_tuning(ld_plan* p, const int32_t* choice) {
+  if (int rc = check_plan(p)) return rc;
+  if (!choice || choice[0] < -1 || choice[0] > 3 || choice[1] < -1 || choice[1] > 3)
+    return ld_fail(LD_ERR_ARG, "ld_plan_set_tuning: bad arguments");
+  p->tune_y[0] = choice[0];
+  p->tune_y[1] = choice[1];
+  return LD_OK;
+}
+
 int ld_slow_manifold(ld_plan* p, void* vk, double tps, double g) {
   if (int rc = check_plan(p)) return rc;
   p->sm_vk = vk;

@@ -85,6 +85,10 @@ class Ensemble:
             col = Collider(d.n, cell, device=dns.plan.device) if collide else None
             dns.attach(d, collider=col, sort_every=sort_every)
             self.boxes.append(dns)
+        # FFT launch variants: timed on the first box, applied to all (same N and precision)
+        self.fft_tuning = self.boxes[0].plan.autotune() if self.boxes else None
+        for b in self.boxes[1:]:
+            b.plan.set_tuning(self.fft_tuning["choice"])
         self.graph = None
         self.streams = []
         self.steps_per_graph = 0
@@ -246,7 +250,7 @@ def main(argv=None):
            "box_steps_per_s": a.boxes * a.steps / (ms / 1e3),
            "droplet_steps_per_s": sum(nd) * a.steps / (ms / 1e3),
            "graph": {"streams": ens.n_graph_streams, "steps_per_graph": ens.steps_per_graph},
-           "autotune": tuning, "setup_s": setup_s, "status_flags_max": max(flags) if flags else 0,
+           "autotune": tuning, "fft_autotune": ens.fft_tuning, "setup_s": setup_s, "status_flags_max": max(flags) if flags else 0,
            "droplets_per_box": nd, "collision_pairs_last_step_per_box": coll}
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -154,6 +154,19 @@ class Plan:
         check(_lib.lib().ld_shell_spectrum(self._h, ptr(uk), ptr(out), stream_ptr(stream)))
         return out
 
+    def autotune(self, stream=None):
+        """Time every launch variant of the y passes on this plan and keep the fastest; returns
+        {"ms": {pass: [one-shot, pipelined 1..3 CTAs/SM]}, "choice": [inverse, forward]}."""
+        ms = (ctypes.c_double * 8)()
+        ch = (ctypes.c_int32 * 2)()
+        check(_lib.lib().ld_plan_autotune(self._h, ms, ch, stream_ptr(stream)))
+        return {"ms": {"inverse_y": [round(x, 5) for x in ms[:4]], "forward_y": [round(x, 5) for x in ms[4:]]},
+                "choice": [int(ch[0]), int(ch[1])]}
+
+    def set_tuning(self, choice):
+        ch = (ctypes.c_int32 * 2)(*[int(c) for c in choice])
+        check(_lib.lib().ld_plan_set_tuning(self._h, ch))
+
     def shell_cross(self, a, b, out=None, stream=None):
         """Shell sums of Re(conj(a) . b) * normalize (FP64, length N/2+1) of cube-layout 3-vectors."""
         self._chk(a, self.cdtype, (3, self.Mx, self.My, self.Mzp))

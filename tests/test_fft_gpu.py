@@ -73,3 +73,24 @@ def test_cube_transforms(torch, N, prec):
     # inverse of the dealiased spectrum
     back = p.irfft_cube(cube).cpu().numpy()
     assert rel(back, sfft.irfftn(ref, s=(N, N, N), axes=(1, 2, 3))) < TOL[prec] * 2
+
+
+@pytest.mark.parametrize("N", [64, 256])
+def test_autotuned_variants_give_identical_rhs(N):
+    """Every launch variant of the y passes computes the same RHS bit for bit; the autotuner
+    reports a time for each available variant and keeps one of them."""
+    import torch
+    from lucky_droplets_b200.spectral import Plan
+    from oracle import config_np as C
+    prm = C.ConfigParams(N=N, nu=2.5e-3, dt=1e-3)
+    uk0, _ = C.init_flow(C.ConfigGrid(N), prm, seed=1)
+    p = Plan(N, "f32")
+    uk = p.to_cube(torch.as_tensor(uk0).to("cuda", p.cdtype).contiguous())
+    res = p.autotune()
+    assert all(c in (0, 1, 2, 3) for c in res["choice"])
+    outs = []
+    for choice in ([0, 0], [1, 1], [3, 3], res["choice"]):
+        p.set_tuning(choice)
+        outs.append(p.velocity_rhs(uk, prm.nu, prm.f0, prm.shell_no).clone())
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
