@@ -404,6 +404,34 @@ def time_e2e(dns, d, K, W, world):
     return e0.elapsed_time(e1), nbytes
 
 
+def count_launches(dns, steps=20):
+    """Kernels (and memset/memcpy operations) the step launches, counted from a CUDA-graph
+    capture of `steps` steps (capture runs nothing; the step counters are restored): per step."""
+    import torch
+    from cuda.bindings import runtime as rt
+    saved = (dns.t, dns.nstep)
+    try:
+        g = torch.cuda.CUDAGraph(keep_graph=True)
+        cap = torch.cuda.Stream()
+        cap.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.graph(g, stream=cap, capture_error_mode="thread_local"):
+            dns.step(steps, stream=cap)
+        graph = rt.cudaGraph_t(init_value=g.raw_cuda_graph())
+        err, _, n = rt.cudaGraphGetNodes(graph, 0)
+        err, nodes, n = rt.cudaGraphGetNodes(graph, n)
+        kinds = {}
+        for nd in nodes:
+            e, t = rt.cudaGraphNodeGetType(nd)
+            kinds[t] = kinds.get(t, 0) + 1
+        k = kinds.get(rt.cudaGraphNodeType.cudaGraphNodeTypeKernel, 0)
+        other = sum(v for t, v in kinds.items() if t != rt.cudaGraphNodeType.cudaGraphNodeTypeKernel)
+        del g
+        return {"kernels_per_step": k / steps, "memset_memcpy_per_step": other / steps,
+                "method": f"CUDA-graph capture of {steps} steps"}
+    finally:
+        dns.t, dns.nstep = saved
+
+
 def profile_kernels(dns, d, P):
     """Per-kernel device time over P steps with launch-bracketing events on the launch stream."""
     import torch
@@ -536,10 +564,17 @@ def run_ours(a):
            "roofline": roof,
            "kernels": kernels,
            "gpu_launches": int(round(launches_per_step * a.steps)),
+           "gpu_launches_detail": {"method": "profile scopes", "scopes_per_step": launches_per_step},
            "status_flags": flags,
            "collision_pairs_last_step": pairs,
            "fft_autotune": getattr(dns, "tuning", None),
            "clocks": clk}
+    try:
+        lc = count_launches(dns)
+        out["gpu_launches"] = int(round(lc["kernels_per_step"] * a.steps))
+        out["gpu_launches_detail"] = dict(lc, scopes_per_step=launches_per_step)
+    except Exception as e:  # keep the scope count, say why
+        out["gpu_launches_detail"]["capture_error"] = str(e)[:200]
     if judge is not None:
         out["judge"] = judge
         out["judge_ms_per_step_amortised"] = judge_ms_per_step
