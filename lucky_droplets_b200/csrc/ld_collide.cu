@@ -321,18 +321,26 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
     unsigned c = 0;
     double4 me;
     bool have_me = false;
-    // target q, cell z: the sorted range [g0, g1)
+    // target q, cell z: the sorted range [g0, g1).  The periodic image of a neighbour cell is
+    // fixed (nc >= 3: a colliding pair is closer than one cell, so its minimum image is the
+    // adjacent-cell image): the home droplet is shifted once per target cell instead of folding
+    // every candidate difference; a wrong image only lengthens the distance (the FP64 rule decides).
+    const float Lfs = Lf;
     for (int r = 0; r < 14; ++r) {
       int q, dz;
       if (r < 2) { q = 0; dz = r; }
       else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
-      const int z = (cz + dz + nc) % nc;
+      const int ox = q < 2 ? 0 : 1;
+      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+      const int zr = cz + dz;
+      const int z = (zr + nc) % nc;
+      const float sx = (cx + ox >= nc) ? -Lfs : 0.f;
+      const float sy = (cy + oy >= nc) ? -Lfs : ((cy + oy < 0) ? Lfs : 0.f);
+      const float sz = (zr >= nc) ? -Lfs : ((zr < 0) ? Lfs : 0.f);
+      const float ax = mf.x + sx, ay = mf.y + sy, az = mf.z + sz;
       const int base_cell = lo[q];
-      // cell start within column q: cs of the cell (column q, z)
       int g0, g1;
       {
-        const int ox = q < 2 ? 0 : 1;
-        const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
         const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * ncol_cells + z;
         g0 = cs[k];
         g1 = cs[k + 1];
@@ -340,7 +348,9 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
       if (r == 0) g0 = i + 1;
       for (int g = g0; g < g1; ++g) {
         const float4 b = staged ? colbuf[so[q] + (g - base_cell)] : spf[g];
-        if (!near_f(mf, b, Lf, hf, mar)) continue;
+        const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
+        const float rr = mf.w + b.w + mar;
+        if (dxf * dxf + dyf * dyf + dzf * dzf >= rr * rr) continue;
         if (!have_me) { me = sp[i]; have_me = true; }
         if (!overlap(me, sp[g], L)) continue;
         if (c < KEEP) scr[(long long)KEEP * i + c] = g;
