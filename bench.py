@@ -105,11 +105,13 @@ def barrier(world):
 
 
 def allreduce_max(x, world):
+    """The maximum of x over the ranks (device tensors under NCCL, host tensors under gloo)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
