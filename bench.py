@@ -435,13 +435,18 @@ def count_launches(dns, steps=20):
 
 
 def profile_kernels(dns, d, P):
-    """Per-kernel device time over P steps with launch-bracketing events on the launch stream."""
+    """Per-kernel device time over P steps with launch-bracketing events on the launch stream.
+    The steps run inside the NVTX range "profile_steps", so that an ncu capture can be limited to
+    production launches (`--nvtx --nvtx-include "profile_steps/"`)."""
     import torch
     p = dns.plan
     p.profile_read(reset=True)
     p.profile(True)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("profile_steps")
     dns.step(P)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     prof = p.profile_read(reset=True)
     p.profile(False)
     return prof

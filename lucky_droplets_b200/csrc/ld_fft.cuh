@@ -129,10 +129,18 @@ struct SyncWarp {
   }
 };
 
-// Shared-memory slot of element p: with PAD one spare slot per E elements, which makes the
-// stride-E writes of stage 0 bank-conflict free for row buffers (sstride = 1).
-template <int E, bool PAD> __device__ __forceinline__ int sidx(int p) {
-  return PAD ? p + (p >> ilog2(E)) : p;
+// Shared-memory slot of element p of a row buffer (sstride = 1) when PAD is set.
+//   8-byte elements (complex float): p ^ ((p >> 4) & 15), a permutation inside each 128-byte line
+//   (16 elements) keyed by the line index: the contiguous reads of every stage stay on whole
+//   lines (two wavefronts per warp) and the stride-E writes of stage 0 and the grouped writes of
+//   the middle stages spread over all 32 banks (two wavefronts for N = 256, E = 8).
+//   16-byte elements (complex double): one spare slot per E elements (p + p / E), which spreads
+//   the stride-E writes; a warp needs four wavefronts for these anyway.
+// Without PAD: p (column buffers, sstride = columns per block).
+template <typename T, int E, bool PAD> __device__ __forceinline__ int sidx(int p) {
+  if constexpr (!PAD) return p;
+  else if constexpr (sizeof(T) == 4) return p ^ ((p >> 4) & 15);
+  else return p + (p >> ilog2(E));
 }
 
 // Stage s >= 1 of the Stockham pipeline (compile-time recursion over the stages).
@@ -150,7 +158,7 @@ __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride
   for (int q = 0; q < Q; ++q) {
     const int b = j + NT * q;
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<E, PAD>(b + r * (N / R)) * sstride];
+    for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, E, PAD>(b + r * (N / R)) * sstride];
   }
   sync();
 #pragma unroll
@@ -163,7 +171,7 @@ __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride
     if constexpr (s < S - 1) {
       const int base = (b / Ns) * Ns * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sbuf[sidx<E, PAD>(base + r * Ns) * sstride] = x[q * R + r];
+      for (int r = 0; r < R; ++r) sbuf[sidx<T, E, PAD>(base + r * Ns) * sstride] = x[q * R + r];
     } else {
 #pragma unroll
       for (int r = 0; r < R; ++r) a[q + r * Q] = x[q * R + r];
@@ -184,7 +192,7 @@ __device__ __forceinline__ void fft_run(cplx<T>* a, cplx<T>* sbuf, int sstride, 
   dft<T, E, INV>(a);  // stage 0: radix E, Ns = 1, no twiddles
   if constexpr (Sh::S > 1) {
 #pragma unroll
-    for (int r = 0; r < E; ++r) sbuf[sidx<E, PAD>(j * E + r) * sstride] = a[r];
+    for (int r = 0; r < E; ++r) sbuf[sidx<T, E, PAD>(j * E + r) * sstride] = a[r];
     sync();
     fft_stage<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
   }

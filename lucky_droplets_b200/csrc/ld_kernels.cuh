@@ -389,8 +389,9 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
 // block-wide when several row units share a warp (the warp-level form gave wrong results for
 // N <= 32 in the fused pass; the block-wide form is verified at every size).
 template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ >= 32), SyncWarp, SyncBlock>::type;
+// Row-buffer slot of element i: the same map as the FFT exchange of the row (sidx with PAD).
 template <typename T, int N> struct ZIdx {
-  static __device__ __forceinline__ int p(int i) { return i + (i >> Cfg<N>::LOGEZ); }
+  static __device__ __forceinline__ int p(int i) { return sidx<T, Cfg<N>::EZ, true>(i); }
 };
 
 // Hermitian-extended load of Y[k] = A[k] + i B[k] (k = j + NT m), A/B spectral rows with Kin

@@ -157,13 +157,16 @@ __device__ __forceinline__ int make_frame(const float* toff, float* tc) {
     r[d] = rf ? 1.f - toff[d] : toff[d];
     code |= (rf ? 1 : 0) << (6 + d);
   }
+  // sort the offsets descending, carrying their axes (values move with the indices, so nothing
+  // is indexed at run time)
   int p0 = 0, p1 = 1, p2 = 2, x;
-  if (r[p1] > r[p0]) { x = p0; p0 = p1; p1 = x; }
-  if (r[p2] > r[p1]) { x = p1; p1 = p2; p2 = x; }
-  if (r[p1] > r[p0]) { x = p0; p0 = p1; p1 = x; }
-  tc[0] = r[p0];
-  tc[1] = r[p1];
-  tc[2] = r[p2];
+  float a = r[0], b = r[1], c = r[2], y;
+  if (b > a) { x = p0; p0 = p1; p1 = x; y = a; a = b; b = y; }
+  if (c > b) { x = p1; p1 = p2; p2 = x; y = b; b = c; c = y; }
+  if (b > a) { x = p0; p0 = p1; p1 = x; y = a; a = b; b = y; }
+  tc[0] = a;
+  tc[1] = b;
+  tc[2] = c;
   return code | p0 | (p1 << 2) | (p2 << 4);
 }
 
@@ -182,9 +185,7 @@ __device__ __forceinline__ void point_frame(double px, double py, double pz, int
   for (int d = 0; d < 3; ++d) {
     const double fl = floor(q[d]);
     toff[d] = float(q[d] - fl);
-    long long ii = (long long)fl % N;
-    if (ii < 0) ii += N;
-    f.i[d] = int(ii);
+    f.i[d] = int((long long)fl & (long long)(N - 1));  // periodic cell; N is a power of two
   }
   f.code = make_frame(toff, f.tc);
 }
@@ -227,13 +228,16 @@ struct CompSums {
   float ss, sh, tr;
 };
 
-__device__ __forceinline__ CompSums comp_sums(const float (&v)[64], const float (&wh)[3][4]) {
+// need_ss: also the sum of all squares (scale mode 0); mode 1 needs only sh.
+__device__ __forceinline__ CompSums comp_sums(const float (&v)[64], const float (&wh)[3][4], bool need_ss = true) {
   CompSums p{0.f, 0.f, 0.f};
+  if (need_ss) {
 #pragma unroll
-  for (int j = 0; j < 64; ++j) {
-    p.ss = fmaf(v[j], v[j], p.ss);
-    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh = fmaf(v[j], v[j], p.sh);
+    for (int j = 0; j < 64; ++j) p.ss = fmaf(v[j], v[j], p.ss);
   }
+#pragma unroll
+  for (int j = 0; j < 64; ++j)
+    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh = fmaf(v[j], v[j], p.sh);
   // tricubic value by separable contraction: z, then y, then x
   float t1[16];
 #pragma unroll
@@ -263,6 +267,16 @@ __device__ __forceinline__ void comp_features(const float (&v)[64], const float*
     w[j] = pack2(v[2 * j] * inv * fs[2 * j], v[2 * j + 1] * inv * fs[2 * j + 1]);
 }
 
+// The same, with the scales read four at a time (16-byte aligned copy in shared memory).
+__device__ __forceinline__ void comp_features4(const float (&v)[64], const float4* fs4, float inv, unsigned (&w)[32]) {
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const float4 f = fs4[q];
+    w[2 * q] = pack2(v[4 * q] * inv * f.x, v[4 * q + 1] * inv * f.y);
+    w[2 * q + 1] = pack2(v[4 * q + 2] * inv * f.z, v[4 * q + 3] * inv * f.w);
+  }
+}
+
 // The offset part of a row (columns 192..207): t - 1/2 for the three canonical offsets, zeros.
 __device__ __forceinline__ void tail_features(const float* tc, unsigned (&w)[8]) {
   w[0] = pack2(tc[0] - 0.5f, tc[1] - 0.5f);
@@ -271,13 +285,14 @@ __device__ __forceinline__ void tail_features(const float* tc, unsigned (&w)[8])
   for (int j = 2; j < 8; ++j) w[j] = 0u;
 }
 
-// Grid-memory offset (in vec4 elements) of canonical index j along canonical axis k of a point
-// (cell ci, frame code): along grid axis p[k], reversed when that axis is reflected.
-__device__ __forceinline__ long long canon_offset(const int* ci, int code, int N, int k, int j) {
+// Grid-memory offset (in vec4 elements; N <= 1024, so N^3 fits an int) of canonical index j
+// along canonical axis k of a point (cell ci, frame code): along grid axis p[k], reversed when
+// that axis is reflected.
+__device__ __forceinline__ int canon_offset(const int* ci, int code, int N, int k, int j) {
   const int d = frame_perm(code, k);
   const int o = (code >> (6 + d)) & 1 ? 3 - j : j;
   const int cid = d == 0 ? ci[0] : (d == 1 ? ci[1] : ci[2]);
-  const long long g = (cid - 1 + o + N) & (N - 1);
+  const int g = (cid - 1 + o + N) & (N - 1);
   return d == 0 ? g * N * N : (d == 1 ? g * N : g);
 }
 
@@ -286,7 +301,7 @@ __device__ __forceinline__ long long canon_offset(const int* ci, int code, int N
 template <typename T>
 __device__ __forceinline__ void gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
                                                  float (&v)[64]) {
-  long long o0[4], o1[4], o2[4];
+  int o0[4], o1[4], o2[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     o0[j] = canon_offset(f.i, f.code, N, 0, j);
@@ -299,10 +314,12 @@ __device__ __forceinline__ void gather_component(const vec4<T>* __restrict__ u4,
 #pragma unroll
   for (int j0 = 0; j0 < 4; ++j0)
 #pragma unroll
-    for (int j1 = 0; j1 < 4; ++j1)
+    for (int j1 = 0; j1 < 4; ++j1) {
+      const int o01 = o0[j0] + o1[j1];
 #pragma unroll
       for (int j2 = 0; j2 < 4; ++j2)
-        v[16 * j0 + 4 * j1 + j2] = sg * float(__ldg(base + 4 * (o0[j0] + o1[j1] + o2[j2])));
+        v[16 * j0 + 4 * j1 + j2] = sg * float(__ldg(base + (size_t)(unsigned)(o01 + o2[j2]) * 4));
+    }
 }
 
 // Thread-per-point features (training samples): st is a 192-float scratch.  Returns the scale;
@@ -461,7 +478,9 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
   const long long nw = ((long long)gridDim.x * FTHREADS) >> 5;
   const int r = lane < 3 * FDROP ? lane / 3 : FDROP - 1;
   const int c = lane < 3 * FDROP ? lane - 3 * r : 0;
-  const float* fs = params + OFF_FS;
+  __shared__ __align__(16) float fs[64];  // feature scales, read as warp-uniform float4
+  if (threadIdx.x < 64) fs[threadIdx.x] = params[OFF_FS + threadIdx.x];
+  __syncthreads();
   const float mode = params[OFF_OS + 1];
   const long long ngroups = (n + FDROP - 1) / FDROP;
   for (long long grp = wg; grp < ngroups; grp += nw) {
@@ -474,7 +493,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
     comp_transform(v);
     float wh[3][4];
     tric_weights(f.tc, wh);
-    const CompSums cs = comp_sums(v, wh);
+    const CompSums cs = comp_sums(v, wh, mode == 0.f);
     const int b0 = 3 * r;
     const float ss0 = __shfl_sync(0xffffffffu, cs.ss, b0), ss1 = __shfl_sync(0xffffffffu, cs.ss, b0 + 1),
                 ss2 = __shfl_sync(0xffffffffu, cs.ss, b0 + 2);
@@ -484,7 +503,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
     const float scale = scale_of(ss0, ss1, ss2, sh0, sh1, sh2, mode);
     if (lane < 3 * FDROP && i < n) {
       unsigned w[32];
-      comp_features(v, fs, 1.f / scale, w);
+      comp_features4(v, reinterpret_cast<const float4*>(fs), 1.f / scale, w);
       unsigned char* tb = reinterpret_cast<unsigned char*>(Xg) + (i / TM) * TILE_X_BYTES;
       const int rr = (int)(i % TM);
 #pragma unroll
@@ -1012,6 +1031,7 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
                  void* out, void* stream) {
   if (!p || !u4 || !packed || !params || n < 0 || (n > 0 && (!pos || !out)))
     return ld_fail(LD_ERR_ARG, "ld_mlp_infer: bad arguments");
+  if (p->N > 1024) return ld_fail(LD_ERR_ARG, "ld_mlp_infer: N > 1024 (stencil offsets are 32-bit)");
   if (n == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;
@@ -1078,6 +1098,7 @@ int ld_mlp_samples(ld_plan* p, const void* u4, const void* ue, const int64_t* id
                    double sz, const float* params, void* X, float* T, float* aux, void* stream) {
   if (!p || !u4 || !ue || ns < 0 || (ns > 0 && (!idx || !params || !X || !T || !aux)))
     return ld_fail(LD_ERR_ARG, "ld_mlp_samples: bad arguments");
+  if (p->N > 1024) return ld_fail(LD_ERR_ARG, "ld_mlp_samples: N > 1024 (stencil offsets are 32-bit)");
   if (ns == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;

@@ -176,52 +176,99 @@ class ForcedDNS:
 
     # ---- stepping ---------------------------------------------------------------------------------
     def step(self, nsteps=1, stream=None):
+        for k in range(nsteps):
+            self._step_one(stream)
+
+    def _step_one(self, stream, before_droplets=None, before_collide=None):
+        """One time step on `stream`.  `before_droplets()` is called just before the first droplet
+        stage is enqueued, `before_collide()` after the state is final (update, epilogue and any
+        re-sorting enqueued) and before the collision search: the hooks of `step_host` that
+        overlap host copies with the flow transforms and the collision search."""
         L = _lib.lib()
         h = self.plan.handle
         st = stream_ptr(stream)
         prm = ctypes.byref(self.prm)
         d = self.droplets
         up = ptr(self.u_phys) if d is not None else None
-        for _ in range(nsteps):
-            if self.integrator == "rk2if":
-                check(L.ld_rk2if_stage(h, 1, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
-                if d is not None:
-                    d.stage(1, self.u_phys, self.dt, stream)
-                check(L.ld_rk2if_stage(h, 2, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
-                if d is not None:
-                    d.stage(2, self.u_phys, self.dt, stream)
-            else:
-                for s in (1, 2, 3, 4):
-                    check(L.ld_rk4_stage(h, s, ptr(self.uk), ptr(self.aux), ptr(self.acc), None, prm, st))
-            if self.epilogue:
-                check(L.ld_step_epilogue(h, ptr(self.uk), st))
-            self.t += self.dt
-            self.nstep += 1
-            if d is not None and self.sort_every > 0 and self.nstep % self.sort_every == 0:
-                d.sort(self._sorter, stream)
-            if d is not None and self.collider is not None:
-                d.collide(self.collider, self.pairs, stream)
+        hooks = [before_droplets]
+
+        def droplets_ready():
+            if hooks[0] is not None:
+                hooks[0]()
+                hooks[0] = None
+
+        if self.integrator == "rk2if":
+            check(L.ld_rk2if_stage(h, 1, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
+            if d is not None:
+                droplets_ready()
+                d.stage(1, self.u_phys, self.dt, stream)
+            check(L.ld_rk2if_stage(h, 2, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
+            if d is not None:
+                d.stage(2, self.u_phys, self.dt, stream)
+        else:
+            for s in (1, 2, 3, 4):
+                check(L.ld_rk4_stage(h, s, ptr(self.uk), ptr(self.aux), ptr(self.acc), None, prm, st))
+        if self.epilogue:
+            check(L.ld_step_epilogue(h, ptr(self.uk), st))
+        self.t += self.dt
+        self.nstep += 1
+        droplets_ready()
+        if d is not None and self.sort_every > 0 and self.nstep % self.sort_every == 0:
+            d.sort(self._sorter, stream)
+        if before_collide is not None:
+            before_collide()
+        if d is not None and self.collider is not None:
+            d.collide(self.collider, self.pairs, stream)
 
     def step_host(self, uk_host, pos_host=None, vel_host=None, nsteps=1, stream=None):
         """Drop-in for one call of the reference's time-loop body with host state (F:582-610):
         copies the cube-layout spectrum (and droplet positions/velocities) from host memory,
         advances ``nsteps`` steps and copies the new state back into the same host arrays.
-        Host tensors should be pinned for asynchronous copies.  Returns the host tensors."""
+        Host tensors should be pinned for asynchronous copies.  Returns the host tensors.
+
+        The spectrum is needed by the first kernel, so its copy precedes the step; the droplet
+        copies run on a side stream under the first stage's flow transforms (the droplets are
+        first read by the droplet stage), and the copies back run on a side stream under the
+        collision search of the last step, which reads the positions but writes no state."""
         torch = _torch()
         s = torch.cuda.current_stream() if stream is None else stream
+        d = self.droplets if pos_host is not None else None
+        side = self._copy_streams()
         with torch.cuda.stream(s):
             self.uk.copy_(uk_host, non_blocking=True)
-            d = self.droplets
-            if d is not None and pos_host is not None:
+        if d is not None:
+            side[0].wait_stream(s)  # earlier users of pos/vel are done before they are overwritten
+            with torch.cuda.stream(side[0]):
                 d.pos.copy_(pos_host, non_blocking=True)
                 d.vel.copy_(vel_host, non_blocking=True)
-            self.step(nsteps, stream=s)
-            uk_host.copy_(self.uk, non_blocking=True)
-            if d is not None and pos_host is not None:
-                pos_host.copy_(d.pos, non_blocking=True)
-                vel_host.copy_(d.vel, non_blocking=True)
+
+        def droplets_in():
+            s.wait_stream(side[0])
+
+        def state_out():
+            side[1].wait_stream(s)
+            with torch.cuda.stream(side[1]):
+                uk_host.copy_(self.uk, non_blocking=True)
+                if d is not None:
+                    pos_host.copy_(d.pos, non_blocking=True)
+                    vel_host.copy_(d.vel, non_blocking=True)
+
+        with torch.cuda.stream(s):
+            for k in range(nsteps):
+                self._step_one(s, droplets_in if (k == 0 and d is not None) else None,
+                               state_out if k == nsteps - 1 else None)
+            if nsteps == 0:
+                droplets_in()
+                state_out()
+        s.wait_stream(side[1])
         s.synchronize()
         return uk_host, pos_host, vel_host
+
+    def _copy_streams(self):
+        torch = _torch()
+        if getattr(self, "_side", None) is None:
+            self._side = (torch.cuda.Stream(device=self.plan.device), torch.cuda.Stream(device=self.plan.device))
+        return self._side
 
     def check(self, stream=None):
         """Host check of the device status word (the blow-up abort of F:618-620)."""

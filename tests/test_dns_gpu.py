@@ -177,3 +177,46 @@ def test_sorted_droplets_with_collisions_match_oracle(torch):
     got = got[np.lexsort((got[:, 1], got[:, 0]))]
     ref = K.collide(d.by_id(d.pos), rad, 2 * rad.max())
     assert np.array_equal(got, ref)
+
+
+def test_step_host_matches_device_steps(torch):
+    """step_host (host state in/out, droplet copies overlapped with the flow transforms and the
+    copies back with the collision search) leaves exactly the state of device-resident steps,
+    including a re-sort (sort_every=2) and the collision pairs of the last step."""
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    from lucky_droplets_b200.collide import Collider
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3, g=0.1)
+    uk0, u0 = C.init_flow(C.ConfigGrid(N), prm, seed=8)
+    pos, tau, rad = C.init_droplets(prm, 8, "uniform_tau", nd=4000)
+    rad = rad * 5.0
+    vel = C.gather(u0, pos, "tricubic")
+    runs = []
+    for _ in range(2):
+        dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision="f32")
+        dns.set_uk_full(uk0)
+        d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g, radius=rad)
+        dns.attach(d, collider=Collider(d.n, 2 * rad.max()), sort_every=2)
+        runs.append((dns, d))
+    (a, da), (b, db) = runs
+    a.step(5)
+    uk_h = b.uk.cpu().pin_memory()
+    pos_h = db.pos.cpu().pin_memory()
+    vel_h = db.vel.cpu().pin_memory()
+    for _ in range(5):
+        b.step_host(uk_h, pos_h, vel_h)
+    torch.cuda.synchronize()
+    assert torch.equal(uk_h, a.uk.cpu())
+    assert torch.equal(pos_h, da.pos.cpu())
+    assert torch.equal(vel_h, da.vel.cpu())
+    assert torch.equal(db.ids, da.ids)
+    assert int(b.collider.count.item()) == int(a.collider.count.item())
+    m = int(a.collider.count.item())
+
+    def pair_set(dns, d):
+        ids = d.ids.cpu().numpy()
+        p = ids[dns.pairs[:m].cpu().numpy().astype(np.int64)]
+        p = np.stack([p.min(axis=1), p.max(axis=1)], axis=1)
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+    assert m > 0 and np.array_equal(pair_set(b, db), pair_set(a, da))
