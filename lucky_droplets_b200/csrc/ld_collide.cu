@@ -1,10 +1,13 @@
-// Cell-list collision detection and the stable LSD radix sort it uses.
+// Cell-list collision detection, the counting sort by cell it uses, and a stable LSD radix sort.
 //
 // Pipeline (one call of ld_collide):
-//   keys      key[i] = cell of the wrapped position of droplet i, val[i] = i
-//   sort      stable LSD radix sort of (key, val), 8-bit digits
-//   starts    cs[k] = first sorted index of cell k (k = 0..ncell; cs[ncell] = n)
-//   reorder   sorted copies of wrapped positions and radii (FP64, and an FP32 copy for the filter)
+//   sort      counting sort by cell: key[i] = cell of the wrapped position of droplet i;
+//             occupancies by atomics, cs[k] = first sorted index of cell k (k = 0..ncell,
+//             cs[ncell] = n) by a scan, an unordered scatter, then every droplet placed at its
+//             cell's start plus its rank by index within the cell, which is exactly the order of a
+//             stable sort of (key, i); sorted copies of the wrapped positions and radii (FP64,
+//             and an FP32 copy for the pre-test) written alongside.  (More than 2^24 cells: LSD
+//             radix sort with 8-bit digits and binary-searched starts instead.)
 //   count     per sorted droplet: partners among the cell itself and its 13 forward neighbours
 //             (the first KEEP of them recorded)
 //   scan      exclusive scan of the counts in sorted order -> offsets, total
@@ -42,6 +45,100 @@ __global__ void k_cell_keys(const double* __restrict__ pos, long long n, double 
     const int cz = cell_of(wrapL(pos[3 * i + 2], L), cw, nc);
     key[i] = (unsigned)((cx * nc + cy) * nc + cz);
     val[i] = (unsigned)i;
+  }
+}
+
+// ---- counting sort by cell (the sort of ld_collide) -------------------------------------------
+__global__ void k_cell_count(const double* __restrict__ pos, long long n, double L, double cw, int nc,
+                             unsigned* __restrict__ key, unsigned* __restrict__ rank, unsigned* __restrict__ occ) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int cx = cell_of(wrapL(pos[3 * i], L), cw, nc);
+    const int cy = cell_of(wrapL(pos[3 * i + 1], L), cw, nc);
+    const int cz = cell_of(wrapL(pos[3 * i + 2], L), cw, nc);
+    const unsigned k = (unsigned)((cx * nc + cy) * nc + cz);
+    key[i] = k;
+    rank[i] = atomicAdd(&occ[k], 1u);  // arrival order: unordered
+  }
+}
+
+__global__ void k_cell_scatter(const unsigned* __restrict__ key, const unsigned* __restrict__ rank,
+                               const int* __restrict__ cs, long long n, unsigned* __restrict__ run) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    run[cs[key[i]] + rank[i]] = (unsigned)i;
+}
+
+// Sorted copies of one sorted slot: cell key, wrapped FP64 position + radius, FP32 copy.
+__device__ __forceinline__ void sorted_slot(long long s, unsigned k, unsigned i, const double* __restrict__ pos,
+                                            const double* __restrict__ rad, double L, unsigned* __restrict__ skey,
+                                            double4* __restrict__ sp, float4* __restrict__ spf) {
+  double4 q;
+  q.x = wrapL(pos[3 * (long long)i], L);
+  q.y = wrapL(pos[3 * (long long)i + 1], L);
+  q.z = wrapL(pos[3 * (long long)i + 2], L);
+  q.w = rad[i];
+  skey[s] = k;
+  sp[s] = q;
+  spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+}
+
+constexpr int kSmallCell = 64;  // cells up to this occupancy are placed by rank counting
+
+// Thread per droplet (index order): its place in the sorted order is its cell's start plus the
+// number of the cell's droplets with a smaller index, counted over the cell's unordered run;
+// writes the sorted index, key and copies there.  Cells above kSmallCell droplets are left to
+// k_cell_big (the droplet in the run's first slot appends the cell to `big`).
+__global__ void k_cell_place(const unsigned* __restrict__ key, const int* __restrict__ cs,
+                             const unsigned* __restrict__ run, long long n, const double* __restrict__ pos,
+                             const double* __restrict__ rad, double L, unsigned* __restrict__ sval,
+                             unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf,
+                             unsigned* __restrict__ big, unsigned* __restrict__ nbig) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned k = key[i];
+    const int s0 = cs[k], s1 = cs[k + 1];
+    if (s1 - s0 > kSmallCell) {
+      if (run[s0] == (unsigned)i) big[atomicAdd(nbig, 1u)] = k;
+      continue;
+    }
+    int r = 0;
+    for (int j = s0; j < s1; ++j) r += run[j] < (unsigned)i ? 1 : 0;
+    const int s = s0 + r;
+    sval[s] = (unsigned)i;
+    sorted_slot(s, k, (unsigned)i, pos, rad, L, skey, sp, spf);
+  }
+}
+
+// Block per large cell (grid-stride over the list): a bitonic network in global memory over the
+// cell's unordered run (virtual +inf padding to a power of two; every compare-exchange puts the
+// smaller index first, so padded slots never move), then the sorted index, key and copies.
+__global__ void __launch_bounds__(512)
+k_cell_big(const int* __restrict__ cs, const unsigned* __restrict__ big, const unsigned* __restrict__ nbig,
+           unsigned* __restrict__ run, const double* __restrict__ pos, const double* __restrict__ rad, double L,
+           unsigned* __restrict__ sval, unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf) {
+  const unsigned nb = *nbig;
+  for (unsigned b = blockIdx.x; b < nb; b += gridDim.x) {
+    const unsigned k = big[b];
+    const int s0 = cs[k], m = cs[k + 1] - s0;
+    unsigned* v = run + s0;
+    int P = 1;
+    while (P < m) P <<= 1;
+    for (int kk = 2; kk <= P; kk <<= 1) {
+      for (int d = kk >> 1; d >= 1; d >>= 1) {
+        for (int t = threadIdx.x; t < P / 2; t += blockDim.x) {
+          const int i = ((t & ~(d - 1)) << 1) | (t & (d - 1));  // insert a 0 bit at position log2(d)
+          const int j = d == (kk >> 1) ? (i ^ (kk - 1)) : (i | d);  // flip step first, then half-cleaners
+          if (j < m) {
+            const unsigned x = v[i], y = v[j];
+            if (x > y) { v[i] = y; v[j] = x; }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int x = threadIdx.x; x < m; x += blockDim.x) {
+      sval[s0 + x] = v[x];
+      sorted_slot(s0 + x, k, v[x], pos, rad, L, skey, sp, spf);
+    }
+    __syncthreads();
   }
 }
 
@@ -269,95 +366,113 @@ __device__ __forceinline__ bool near_f(const float4 a, const float4 b, float L, 
   return dx * dx + dy * dy + dz * dz < r * r;
 }
 
-// Block per (column, part), nc >= 3.  Column (cx, cy) holds cells (cx, cy, 0..nc-1), contiguous
-// in the sorted order.  Its droplets are tested against its own column (the same cell, partners
-// after them; the cell z+1) and the four forward columns (0,+1), (+1,-1), (+1,0), (+1,+1) at
-// cells z-1, z, z+1: the cell itself and its 13 forward neighbours, so every unordered pair is
-// tested exactly once.  The FP32 copies of the five columns are staged in shared memory (read
-// from global memory when they exceed cap_smem).  Each droplet visits its partners in a fixed
-// order, stores its partner count per sorted index and records its first KEEP partners (sorted
-// indices) in scr; k_emit_pairs then writes the pairs from the scanned counts, searching again
-// only for the rare droplets with more than KEEP partners.
+// Block per (cell column (cx, cy), part), nc >= 3; thread per droplet of the column (the part's
+// share of them).  Its partners are searched among the cell itself (partners after it in the
+// sorted order) and the 13 forward neighbours, visited in a fixed order r = 0..13:
+//   r = 0: the cell itself; r = 1: (0, 0, +1); r = 2..13: columns q = 1..4 (offsets (0,+1),
+//   (+1,-1), (+1,0), (+1,+1)) at dz = -1, 0, +1,
+// and in sorted order inside each target cell, so every unordered pair is tested exactly once.
+// The five columns' cell starts, their periodic shifts and (when they fit in cap_smem rows) their
+// FP32 positions are staged in shared memory; the home cell comes from the sorted key and the
+// neighbour cells by compare-and-wrap, so the visit needs no integer division.  The periodic
+// image of a neighbour cell is fixed (a colliding pair is closer than one cell, nc >= 3): the
+// home position is shifted once per target cell; a wrong image only lengthens the distance (the
+// FP64 rule decides).  Each droplet stores its partner count and its first KEEP partners (sorted
+// indices) in scr; k_emit_pairs writes the pairs from the scanned counts, searching again only
+// for droplets with more than KEEP partners.
 constexpr int COL_THREADS = 256;
 constexpr int KEEP = 4;
 constexpr int kColSmemRows = 12288;  // 192 KB of staged FP32 rows per block at most
+
+__device__ __forceinline__ void col_offset(int q, int& ox, int& oy) {
+  ox = q < 2 ? 0 : 1;
+  oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+}
+
+// The visit of one droplet (sorted index i, t-th of its column); STAGED: positions from colbuf.
+template <bool STAGED>
+__device__ __forceinline__ void col_visit(int i, int t, const double4* __restrict__ sp, const float4* __restrict__ spf,
+                                          const float4* colbuf, const int* cst, const int* dl, const float* shx,
+                                          const float* shy, int cz, int nc, double L, float Lf, float margin,
+                                          unsigned* __restrict__ cnt, int* __restrict__ scr) {
+  const float4 mf = STAGED ? colbuf[t] : spf[i];
+  const float mar = margin + 1e-6f * mf.w;
+  unsigned c = 0;
+#pragma unroll 1
+  for (int r = 0; r < 14; ++r) {
+    const int q = r < 2 ? 0 : 1 + (r - 2) / 3;
+    const int dz = r < 2 ? r : (r - 2) % 3 - 1;
+    const int zr = cz + dz;
+    const int zz = zr < 0 ? zr + nc : (zr >= nc ? zr - nc : zr);
+    const float sz = zr >= nc ? -Lf : (zr < 0 ? Lf : 0.f);
+    const float ax = mf.x + shx[q], ay = mf.y + shy[q], az = mf.z + sz;
+    const int g1 = cst[q * (nc + 1) + zz + 1];
+    const int d = dl[q];
+    for (int g = r == 0 ? i + 1 : cst[q * (nc + 1) + zz]; g < g1; ++g) {
+      const float4 b = STAGED ? colbuf[g - d] : spf[g];
+      const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
+      const float rr = mf.w + b.w + mar;
+      if (dxf * dxf + dyf * dyf + dzf * dzf >= rr * rr) continue;
+      if (!overlap(sp[i], sp[g], L)) continue;
+      if (c < KEEP) scr[(long long)KEEP * i + c] = g;
+      ++c;
+    }
+  }
+  cnt[i] = c;
+}
 
 __global__ void __launch_bounds__(COL_THREADS)
 k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
             const int* __restrict__ cs, int nc, int parts, double L, int cap_smem, unsigned* __restrict__ cnt,
             int* __restrict__ scr) {
-  extern __shared__ float4 colbuf[];
-  __shared__ int lo[5], len[5], so[6];
+  extern __shared__ __align__(16) unsigned char cp_smem[];
+  float4* colbuf = reinterpret_cast<float4*>(cp_smem);
+  int* cst = reinterpret_cast<int*>(cp_smem + sizeof(float4) * (size_t)cap_smem);  // 5 x (nc + 1) cell starts
+  __shared__ long long kq[5];
+  __shared__ int lo[5], so[6], dl[5];
+  __shared__ float shx[5], shy[5];
   const long long col = blockIdx.x / parts;
   const int part = (int)(blockIdx.x % parts);
   const int cx = (int)(col / nc), cy = (int)(col % nc);
+  const float Lf = (float)L, margin = (float)(1e-6 * L);
+  if (threadIdx.x < 5) {
+    int ox, oy;
+    col_offset(threadIdx.x, ox, oy);
+    kq[threadIdx.x] = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
+    shx[threadIdx.x] = (cx + ox >= nc) ? -Lf : 0.f;
+    shy[threadIdx.x] = (cy + oy >= nc) ? -Lf : ((cy + oy < 0) ? Lf : 0.f);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 5 * (nc + 1); e += COL_THREADS) {
+    const int q = e / (nc + 1), z = e - q * (nc + 1);
+    cst[e] = cs[kq[q] + z];
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     int acc = 0;
     for (int q = 0; q < 5; ++q) {
-      const int ox = q < 2 ? 0 : 1;
-      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
-      const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
-      lo[q] = cs[k];
-      len[q] = cs[k + nc] - cs[k];
+      lo[q] = cst[q * (nc + 1)];
       so[q] = acc;
-      acc += len[q];
+      acc += cst[q * (nc + 1) + nc] - lo[q];
     }
     so[5] = acc;
   }
   __syncthreads();
-  const bool staged = so[5] <= cap_smem;
+  const bool staged = so[5] <= cap_smem;  // block-uniform
+  if (threadIdx.x < 5) dl[threadIdx.x] = staged ? lo[threadIdx.x] - so[threadIdx.x] : 0;
   if (staged) {
-    for (int q = 0; q < 5; ++q)
-      for (int t = threadIdx.x; t < len[q]; t += COL_THREADS) colbuf[so[q] + t] = spf[lo[q] + t];
+    for (int q = 0; q < 5; ++q) {
+      const int n_q = so[q + 1] - so[q];
+      for (int t = threadIdx.x; t < n_q; t += COL_THREADS) colbuf[so[q] + t] = spf[lo[q] + t];
+    }
   }
   __syncthreads();
-  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
-  const long long ncol_cells = (long long)nc;
-  for (int t = part * COL_THREADS + threadIdx.x; t < len[0]; t += parts * COL_THREADS) {
+  const int len0 = so[1] - so[0];
+  for (int t = part * COL_THREADS + threadIdx.x; t < len0; t += parts * COL_THREADS) {
     const int i = lo[0] + t;
-    const float4 mf = staged ? colbuf[t] : spf[i];
-    const float mar = margin + 1e-6f * mf.w;
-    const int cz = (int)(skey[i] % (unsigned)nc);
-    unsigned c = 0;
-    double4 me;
-    bool have_me = false;
-    // target q, cell z: the sorted range [g0, g1).  The periodic image of a neighbour cell is
-    // fixed (nc >= 3: a colliding pair is closer than one cell, so its minimum image is the
-    // adjacent-cell image): the home droplet is shifted once per target cell instead of folding
-    // every candidate difference; a wrong image only lengthens the distance (the FP64 rule decides).
-    const float Lfs = Lf;
-    for (int r = 0; r < 14; ++r) {
-      int q, dz;
-      if (r < 2) { q = 0; dz = r; }
-      else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
-      const int ox = q < 2 ? 0 : 1;
-      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
-      const int zr = cz + dz;
-      const int z = (zr + nc) % nc;
-      const float sx = (cx + ox >= nc) ? -Lfs : 0.f;
-      const float sy = (cy + oy >= nc) ? -Lfs : ((cy + oy < 0) ? Lfs : 0.f);
-      const float sz = (zr >= nc) ? -Lfs : ((zr < 0) ? Lfs : 0.f);
-      const float ax = mf.x + sx, ay = mf.y + sy, az = mf.z + sz;
-      const int base_cell = lo[q];
-      int g0, g1;
-      {
-        const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * ncol_cells + z;
-        g0 = cs[k];
-        g1 = cs[k + 1];
-      }
-      if (r == 0) g0 = i + 1;
-      for (int g = g0; g < g1; ++g) {
-        const float4 b = staged ? colbuf[so[q] + (g - base_cell)] : spf[g];
-        const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
-        const float rr = mf.w + b.w + mar;
-        if (dxf * dxf + dyf * dyf + dzf * dzf >= rr * rr) continue;
-        if (!have_me) { me = sp[i]; have_me = true; }
-        if (!overlap(me, sp[g], L)) continue;
-        if (c < KEEP) scr[(long long)KEEP * i + c] = g;
-        ++c;
-      }
-    }
-    cnt[i] = c;
+    const int cz = (int)(skey[i] - (unsigned)kq[0]);
+    if (staged) col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, Lf, margin, cnt, scr);
+    else col_visit<false>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, Lf, margin, cnt, scr);
   }
 }
 
@@ -448,6 +563,7 @@ struct ld_collider {
   float4* spf = nullptr;
   int* scr = nullptr;  // first KEEP partners of each sorted droplet
   unsigned* status = nullptr;
+  unsigned* nbig = nullptr;  // number of cells above kSmallCell droplets (counting sort)
   unsigned* sums = nullptr;  // scan tile totals
   int nblocks = 0;
   ld_plan* trace = nullptr;  // plan whose event trace records this collider's launches
@@ -494,6 +610,7 @@ int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
   A((void**)&c->spf, sizeof(float4) * nmax);
   A((void**)&c->scr, sizeof(int) * KEEP * nmax);
   A((void**)&c->status, sizeof(unsigned));
+  A((void**)&c->nbig, sizeof(unsigned));
   {
     long long m = (nmax + 1) > (long long)RADIX * c->nblocks ? (nmax + 1) : (long long)RADIX * c->nblocks;
     if (ncell + 1 > m) m = ncell + 1;
@@ -513,6 +630,7 @@ int ld_collider_destroy(ld_collider* c) {
   if (!c) return LD_OK;
   cudaFree(c->key); cudaFree(c->val); cudaFree(c->key2); cudaFree(c->val2); cudaFree(c->hist);
   cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->scr); cudaFree(c->status);
+  cudaFree(c->nbig);
   cudaFree(c->sums);
   delete c;
   return LD_OK;
@@ -557,30 +675,51 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
   }
   {
     ProfScope ps(c->trace, KID_COLL_SORT, s);
-    k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val);
-    int bits = 1;
-    while ((1LL << bits) < ncell) ++bits;
-    if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
+    if (ncell + 1 > (long long)SCAN_TILE * SCAN_TILE) {
+      // more cells than one scan handles: stable radix sort of the keys, starts by binary search
+      k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val);
+      int bits = 1;
+      while ((1LL << bits) < ncell) ++bits;
+      if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
+      k_cell_starts<<<gridn(ncell + 1, 256), 256, 0, s>>>(c->key, n, ncell, c->start);
+      k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf);
+    } else {
+      // counting sort by cell (the same order): keys (c->key2) and arrival ranks (c->val2),
+      // occupancies -> starts in c->start, unordered runs scattered into c->cnt, then every
+      // droplet placed by its rank within its cell into c->val with the sorted keys (c->key) and
+      // copies (cells above kSmallCell: listed in c->val2, sorted by k_cell_big)
+      unsigned* occ = reinterpret_cast<unsigned*>(c->start);
+      LD_CUDA_CHECK(cudaMemsetAsync(occ, 0, sizeof(unsigned) * (size_t)(ncell + 1), s));
+      LD_CUDA_CHECK(cudaMemsetAsync(c->nbig, 0, sizeof(unsigned), s));
+      k_cell_count<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key2, c->val2, occ);
+      if (int rc = scan_u32(c, occ, ncell + 1, s)) return rc;
+      k_cell_scatter<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->val2, c->start, n, c->cnt);
+      k_cell_place<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->start, c->cnt, n, pos, radius, L, c->val, c->key, c->sp,
+                                                 c->spf, c->val2, c->nbig);
+      k_cell_big<<<148, 512, 0, s>>>(c->start, c->val2, c->nbig, c->cnt, pos, radius, L, c->val, c->key, c->sp,
+                                     c->spf);
+    }
   }
   ProfScope ps(c->trace, KID_COLL_PAIRS, s);
-  k_cell_starts<<<gridn(ncell + 1, 256), 256, 0, s>>>(c->key, n, ncell, c->start);
-  k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf);
   LD_CUDA_CHECK(cudaMemsetAsync(c->cnt + n, 0, 4, s));
   if (nc >= 3) {
-    // block per cell column; pairs come out as sorted-array indices and are mapped back to
-    // droplet indices by k_map_pairs
+    // block per cell column (and part); pairs come out as sorted-array indices and are mapped
+    // back to droplet indices by k_map_pairs
     const long long ncol = (long long)nc * nc;
     const long long per_col = (n + ncol - 1) / ncol;
     const long long parts = per_col > 512 ? (per_col + 511) / 512 : 1;
+    const size_t starts_bytes = sizeof(int) * 5 * (size_t)(nc + 1);
+    if (ncol * parts > 0x7fffffffLL || starts_bytes > 64 * 1024)
+      return ld_fail(LD_ERR_UNSUPPORTED, "ld_collide: too many cells per side (%d)", nc);
     long long want = 5 * per_col + (5 * per_col) / 4 + 256;  // typical staged rows, with headroom
+    const long long room = (long long)((220 * 1024 - starts_bytes) / sizeof(float4));
     if (want > kColSmemRows) want = kColSmemRows;
+    if (want > room) want = room;
     const int cap_smem = (int)want;
-    const size_t smem = sizeof(float4) * (size_t)cap_smem;
-    if (ncol * parts > 0x7fffffffLL) return ld_fail(LD_ERR_UNSUPPORTED, "ld_collide: too many cell columns");
+    const size_t smem = sizeof(float4) * (size_t)cap_smem + starts_bytes;
     LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const unsigned gb = (unsigned)(ncol * parts);
-    k_col_pairs<<<gb, COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem, c->cnt,
-                                              c->scr);
+    k_col_pairs<<<(unsigned)(ncol * parts), COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts,
+                                                                    L, cap_smem, c->cnt, c->scr);
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
     k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, n, c->cnt, c->scr, pairs,
                                                cap);

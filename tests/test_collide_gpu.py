@@ -177,3 +177,25 @@ def test_dense_cluster_many_partners(torch):
     ref = K.collide(pos, rad, 0.06)
     assert len(ref) > 20000
     assert got.shape == ref.shape and np.array_equal(got, ref)
+
+
+def test_crowded_cell_beside_sparse_cells(torch):
+    """One cell holding 2500 droplets among sparse cells (nc >= 3): the counting sort's
+    large-cell path and partner lists far longer than the recorded KEEP, against the FP64 rule;
+    two calls give the identical list."""
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng(33)
+    dense = rng.uniform(1.1, 1.4, (2500, 3))
+    sparse = rng.uniform(0.0, TWO_PI, (6000, 3))
+    pos = np.concatenate([sparse[:3000], dense, sparse[3000:]])
+    rad = np.full(pos.shape[0], 0.006)
+    cell = 0.5  # 12 cells per side
+    got, _ = gpu_pairs(torch, pos, rad, cell)
+    ref = K.collide(pos, rad, cell)
+    assert len(ref) > 100
+    assert got.shape == ref.shape and np.array_equal(got, ref)
+    c = Collider(pos.shape[0], cell)
+    p, r = torch.as_tensor(pos).cuda(), torch.as_tensor(rad).cuda()
+    a = c.collide(p, r, cap=100000).cpu().numpy()
+    b = c.collide(p, r, cap=100000).cpu().numpy()
+    assert np.array_equal(a, b)
