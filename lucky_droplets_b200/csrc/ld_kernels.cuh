@@ -256,10 +256,14 @@ template <typename T> struct UpdArgs {
   // vk = y + tps (k (k . rhs) / k^2 + visc nu k^2 y), minus vg = tps g N^3 on the mean of w
   cplx<T>* vk;
   T tps, vg;
+  // RK2 stages: stage the cube rows of the CTA's columns that the update reads (s1 in stage 1,
+  // s2 in stage 2) into shared memory with cp.async while the x transforms run; the launcher
+  // sets it when the (3, Mx, TB) buffer fits beside the exchange buffer at 2 CTAs per SM
+  int prefetch;
 };
 
 template <typename T, int N, int MODE>
-__global__ void __launch_bounds__(Cfg<N>::COL_THREADS)
+__global__ void __launch_bounds__(Cfg<N>::COL_THREADS, (N == 256 && sizeof(T) == 4) ? 2 : 1)
 k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
   constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -267,6 +271,27 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
   const int c = threadIdx.x % TB, j = threadIdx.x / TB;
   const int col = blockIdx.x * TB + c;
   const bool ok = col < ncols;
+  constexpr bool RK2 = MODE == UPD_RK2_1 || MODE == UPD_RK2_2;
+  const int Mx = 2 * A.kc + 1;
+  cplx<T>* ybuf = sbuf + N * TB;  // (3, Mx, TB) staged rows of s1 (stage 1) or s2 (stage 2)
+  const bool pre = RK2 && A.prefetch;
+  if (pre) {
+    constexpr int PER = 16 / (int)sizeof(cplx<T>);  // elements per 16-byte chunk
+    const cplx<T>* src = MODE == UPD_RK2_1 ? A.s1 : A.s2;
+    const int col0 = blockIdx.x * TB;
+    const int w = ncols - col0 < TB ? ncols - col0 : TB;  // a multiple of 8 (Mzp is)
+    const int cpr = w / PER;
+    const long long rs = (long long)A.My * A.Mzp;
+    for (int q = threadIdx.x; q < 3 * Mx * (TB / PER); q += blockDim.x) {
+      const int row = q / (TB / PER), k = q - row * (TB / PER);  // row = cc * Mx + r
+      if (k >= cpr) continue;
+      const int cc = row / Mx, r = row - cc * Mx;
+      const cplx<T>* g = src + cc * A.cs + r * rs + col0 + k * PER;
+      const unsigned d = (unsigned)__cvta_generic_to_shared(ybuf + row * TB + k * PER);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   cplx<T> res[3][E];
 #pragma unroll
   for (int f = 0; f < 3; ++f) {
@@ -275,6 +300,10 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
       res[f][m] = ok ? A.nl[f * A.nls + (long long)(j + NT * m) * ncols + col] : czero<cplx<T>>();
     if (f) __syncthreads();
     fft_run<T, N, E, false, false>(res[f], sbuf + c, TB, j, tw, SyncBlock());
+  }
+  if (pre) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    __syncthreads();
   }
   if (!ok) return;
   const int iy = col / A.Mzp;
@@ -293,19 +322,23 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     const int k2 = kxi * kxi + kyi * kyi + kzi * kzi;
     const long long idx = (long long)r * A.My * A.Mzp + col;
     const bool keep = (kzi <= kc) && (k2 <= kc * kc + kc);  // round(|k|) <= kc  (F:129)
-    cplx<T> y[3];  // the stage input
+    // forcing on shells kf_lo..kf_hi: factor[kint] * y  (F:253-264)
+    T fac = T(0);
+    if (keep && k2 <= A.kf_hi * A.kf_hi + A.kf_hi) {
+      int s = 0;
+      while (s * s + s < k2) ++s;  // s = round(sqrt(k2))
+      if (s >= A.kf_lo) fac = T(A.factor[s]);
+    }
+    // the stage input; the second RK2 stage reads it only for the forcing and the slow manifold
+    const bool need_y = MODE != UPD_RK2_2 || A.vk != nullptr || fac != T(0);
+    cplx<T> y[3];
 #pragma unroll
-    for (int cc = 0; cc < 3; ++cc) y[cc] = A.s1[cc * A.cs + idx];
+    for (int cc = 0; cc < 3; ++cc)
+      y[cc] = !need_y ? czero<cplx<T>>()
+                      : ((MODE == UPD_RK2_1 && pre) ? ybuf[(cc * Mx + r) * TB + c] : A.s1[cc * A.cs + idx]);
     cplx<T> rhs[3];
     cplx<T> kd = czero<cplx<T>>();  // (k . rhs) / k^2 before the projection
     if (keep) {
-      // forcing on shells kf_lo..kf_hi: factor[kint] * y  (F:253-264)
-      T fac = T(0);
-      if (k2 <= A.kf_hi * A.kf_hi + A.kf_hi) {
-        int s = 0;
-        while (s * s + s < k2) ++s;  // s = round(sqrt(k2))
-        if (s >= A.kf_lo) fac = T(A.factor[s]);
-      }
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) rhs[cc] = cadd(res[cc][m], cscale(y[cc], fac));
       if (k2 > 0) {  // pressure projection, invlap = -1/k^2 (F:309-316)
@@ -349,7 +382,8 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     } else if (MODE == UPD_RK2_2) {
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
-        cplx<T> v = cadd(A.s2[cc * A.cs + idx], cscale(rhs[cc], T(0.5) * h));
+        const cplx<T> acc = pre ? ybuf[(cc * Mx + r) * TB + c] : A.s2[cc * A.cs + idx];
+        cplx<T> v = cadd(acc, cscale(rhs[cc], T(0.5) * h));
         if (!keep) v = czero<cplx<T>>();
         if (!(isfinite(v.x) && isfinite(v.y))) flags |= LD_STATUS_NONFINITE;
         A.s0[cc * A.cs + idx] = v;

@@ -483,11 +483,20 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
   __syncthreads();
   const float mode = params[OFF_OS + 1];
   const long long ngroups = (n + FDROP - 1) / FDROP;
+  // positions of the warp's next group are loaded while the current one is processed
+  double px = 0.0, py = 0.0, pz = 0.0;
+  if (wg < ngroups) {
+    const long long i0 = wg * FDROP + r, ii0 = i0 < n ? i0 : n - 1;
+    px = pos[3 * ii0]; py = pos[3 * ii0 + 1]; pz = pos[3 * ii0 + 2];
+  }
   for (long long grp = wg; grp < ngroups; grp += nw) {
     const long long i = grp * FDROP + r;
-    const long long ii = i < n ? i : n - 1;
     PtFrame f;
-    point_frame(pos[3 * ii], pos[3 * ii + 1], pos[3 * ii + 2], N, L, f);
+    point_frame(px, py, pz, N, L, f);
+    if (grp + nw < ngroups) {
+      const long long i1 = (grp + nw) * FDROP + r, ii1 = i1 < n ? i1 : n - 1;
+      px = pos[3 * ii1]; py = pos[3 * ii1 + 1]; pz = pos[3 * ii1 + 2];
+    }
     float v[64];
     gather_component<T>(u4, N, f, c, v);
     comp_transform(v);

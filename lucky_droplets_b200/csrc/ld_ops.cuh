@@ -319,10 +319,15 @@ template <typename T, int N> struct Ops {
     A.h = T(prm->dt); A.nu = T(prm->nu); A.visc = T(visc);
     A.kc = kc; A.My = My; A.Mzp = Mzp; A.status = p->status;
     A.vk = (C*)p->sm_vk; A.tps = T(p->sm_tps); A.vg = T(p->sm_tps * p->sm_g * (double)N * N * N);
+    // RK2 stages stage their cube rows in shared memory when that keeps 2 CTAs per SM
+    const size_t pre_bytes = sizeof(C) * 3 * (size_t)(2 * kc + 1) * TB;
+    constexpr bool RK2 = MODE == UPD_RK2_1 || MODE == UPD_RK2_2;
+    A.prefetch = (RK2 && COL_SMEM + pre_bytes <= 112 * 1024) ? 1 : 0;
+    const size_t smem = COL_SMEM + (A.prefetch ? pre_bytes : 0);
     ProfScope ps(p, KID_XFWD_UPD, s);
     auto k = k_xfwd_update<T, N, MODE>;
-    if (int rc = set_smem(k, COL_SMEM)) return rc;
-    k<<<(unsigned)cdiv((long long)My * Mzp, TB), Cfg<N>::COL_THREADS, COL_SMEM, s>>>(A, My * Mzp, tw);
+    if (int rc = set_smem(k, smem)) return rc;
+    k<<<(unsigned)cdiv((long long)My * Mzp, TB), Cfg<N>::COL_THREADS, smem, s>>>(A, My * Mzp, tw);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
