@@ -297,10 +297,12 @@ __device__ __forceinline__ int canon_offset(const int* ci, int code, int N, int 
 }
 
 // Canonical component c of the point's 64-tap stencil, straight from the interleaved field into
-// registers (canonical tap order j0*16 + j1*4 + j2).
+// registers (canonical tap order j0*16 + j1*4 + j2), without the frame's sign of the component,
+// which is returned: the transform and the sums are odd or even in the sign and round
+// symmetrically, so callers apply it exactly where it matters (features, canonical tricubic).
 template <typename T>
-__device__ __forceinline__ void gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
-                                                 float (&v)[64]) {
+__device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
+                                                  float (&v)[64]) {
   int o0[4], o1[4], o2[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
@@ -318,8 +320,9 @@ __device__ __forceinline__ void gather_component(const vec4<T>* __restrict__ u4,
       const int o01 = o0[j0] + o1[j1];
 #pragma unroll
       for (int j2 = 0; j2 < 4; ++j2)
-        v[16 * j0 + 4 * j1 + j2] = sg * float(__ldg(base + (size_t)(unsigned)(o01 + o2[j2]) * 4));
+        v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (size_t)(unsigned)(o01 + o2[j2]) * 4));
     }
+  return sg;
 }
 
 // Thread-per-point features (training samples): st is a 192-float scratch.  Returns the scale;
@@ -334,9 +337,10 @@ __device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, 
   float wh[3][4];
   tric_weights(f.tc, wh);
   CompSums cs[3];
+  float sgc[3];
   for (int c = 0; c < 3; ++c) {
     float v[64];
-    gather_component<T>(u4, N, f, c, v);
+    sgc[c] = gather_component<T>(u4, N, f, c, v);
     comp_transform(v);
     cs[c] = comp_sums(v, wh);
 #pragma unroll
@@ -351,7 +355,7 @@ __device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, 
 #pragma unroll
     for (int j = 0; j < 64; ++j) v[j] = st[64 * c + j];
     unsigned w[32];
-    comp_features(v, fs, inv, w);
+    comp_features(v, fs, sgc[c] * inv, w);
 #pragma unroll
     for (int j = 0; j < 32; ++j) rw[32 * c + j] = w[j];
   }
@@ -362,9 +366,8 @@ __device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, 
   code = f.code;
 #pragma unroll
   for (int cc = 0; cc < 3; ++cc) {
-    tric_can[cc] = cs[cc].tr;
-    const int d = frame_perm(code, cc);
-    tric_grid[d] = frame_sign(code, d) * cs[cc].tr;
+    tric_can[cc] = sgc[cc] * cs[cc].tr;  // cs.tr is the unsigned (grid-frame) value
+    tric_grid[frame_perm(code, cc)] = cs[cc].tr;
   }
   return scale;
 }
@@ -498,7 +501,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
       px = pos[3 * ii1]; py = pos[3 * ii1 + 1]; pz = pos[3 * ii1 + 2];
     }
     float v[64];
-    gather_component<T>(u4, N, f, c, v);
+    const float sg = gather_component<T>(u4, N, f, c, v);
     comp_transform(v);
     float wh[3][4];
     tric_weights(f.tc, wh);
@@ -512,7 +515,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
     const float scale = scale_of(ss0, ss1, ss2, sh0, sh1, sh2, mode);
     if (lane < 3 * FDROP && i < n) {
       unsigned w[32];
-      comp_features4(v, reinterpret_cast<const float4*>(fs), 1.f / scale, w);
+      comp_features4(v, reinterpret_cast<const float4*>(fs), sg * (1.f / scale), w);
       unsigned char* tb = reinterpret_cast<unsigned char*>(Xg) + (i / TM) * TILE_X_BYTES;
       const int rr = (int)(i % TM);
 #pragma unroll
@@ -529,7 +532,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
 #pragma unroll
         for (int cc = 0; cc < 3; ++cc) {
           const int d = frame_perm(f.code, cc);
-          const float val = frame_sign(f.code, d) * trc[cc];
+          const float val = trc[cc];  // unsigned: already the grid-frame tricubic value
           if (d == 0) ax[0] = val;
           else if (d == 1) ax[1] = val;
           else ax[2] = val;
