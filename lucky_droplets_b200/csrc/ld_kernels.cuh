@@ -173,13 +173,20 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
   cplx<T>* buf0 = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* buf1 = buf0 + N * TB;
   const int c = threadIdx.x % TB, j = threadIdx.x / TB;
-  const int ncb = (ncols + TB - 1) / TB;
-  const long long nitems = (long long)ncb * nf * nouter;
-  auto prefetch = [&](long long it, cplx<T>* dst) {
-    const int cb = (int)(it % ncb);
-    const long long rest = it / ncb;
-    const int f = (int)(rest % nf), o = (int)(rest / nf);
-    const int col0 = cb * TB;
+  // item = (column block cb, field f, outer o), cb fastest; the launcher keeps the item count
+  // below 2^31, so items are split with 32-bit unsigned division
+  const unsigned ncb = (unsigned)((ncols + TB - 1) / TB);
+  const unsigned nitems = ncb * (unsigned)nf * (unsigned)nouter;
+  struct Item {
+    int cb, f, o;
+  };
+  auto split = [&](unsigned it) {
+    const unsigned rest = it / ncb;
+    const unsigned fo = rest / (unsigned)nf;
+    return Item{(int)(it - rest * ncb), (int)(rest - fo * (unsigned)nf), (int)fo};
+  };
+  auto prefetch = [&](const Item& itm, cplx<T>* dst) {
+    const int col0 = itm.cb * TB;
     const int w = ncols - col0 < TB ? ncols - col0 : TB;
     const int cpr = w * (int)sizeof(cplx<T>) / 16;
     for (int q = threadIdx.x; q < N * CPR; q += blockDim.x) {
@@ -187,23 +194,22 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
       if (k >= cpr) continue;
       const int r = in.kc < 0 ? n : crow(n, N, in.kc);
       if (r < 0) continue;
-      const char* src = reinterpret_cast<const char*>(in.p + in.at(f, o, r, col0)) + 16 * k;
+      const char* src = reinterpret_cast<const char*>(in.p + in.at(itm.f, itm.o, r, col0)) + 16 * k;
       const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst + n * TB) + 16 * k);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  long long it = blockIdx.x;
-  if (it < nitems) prefetch(it, buf0);
+  unsigned it = blockIdx.x;
+  Item cur_item = split(it);
+  if (it < nitems) prefetch(cur_item, buf0);
   int b = 0;
   for (; it < nitems; it += gridDim.x) {
     cplx<T>* cur = b ? buf1 : buf0;
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
-    const int cb = (int)(it % ncb);
-    const long long rest = it / ncb;
-    const int f = (int)(rest % nf), o = (int)(rest / nf);
-    const int col = cb * TB + c;
+    const int f = cur_item.f, o = cur_item.o;
+    const int col = cur_item.cb * TB + c;
     const bool ok = col < ncols;
     cplx<T> a[E];
 #pragma unroll
@@ -213,7 +219,9 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
       a[m] = (ok && r >= 0) ? cscale(cur[n * TB + c], in.scale) : czero<cplx<T>>();
     }
     __syncthreads();  // every value is in registers: cur becomes the exchange buffer
-    if (it + gridDim.x < nitems) prefetch(it + gridDim.x, b ? buf0 : buf1);
+    const unsigned nx = it + gridDim.x;
+    const Item next_item = split(nx);
+    if (nx < nitems) prefetch(next_item, b ? buf0 : buf1);
     fft_run<T, N, E, INV, false>(a, cur + c, TB, j, tw, SyncBlock());
     if (ok) {
 #pragma unroll
@@ -221,6 +229,7 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
     }
     __syncthreads();
     b ^= 1;
+    cur_item = next_item;
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
 }

@@ -477,8 +477,6 @@ __global__ void __launch_bounds__(FTHREADS, 2)
 k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __restrict__ pos, long long n,
                const float* __restrict__ params, bf16* __restrict__ Xg, float* __restrict__ auxg) {
   const int lane = threadIdx.x & 31;
-  const long long wg = ((long long)blockIdx.x * FTHREADS + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * FTHREADS) >> 5;
   const int r = lane < 3 * FDROP ? lane / 3 : FDROP - 1;
   const int c = lane < 3 * FDROP ? lane - 3 * r : 0;
   __shared__ __align__(16) float fs[64];  // feature scales, read as warp-uniform float4
@@ -486,17 +484,26 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
   __syncthreads();
   const float mode = params[OFF_OS + 1];
   const long long ngroups = (n + FDROP - 1) / FDROP;
+  // each CTA takes a contiguous range of groups (its warps interleaved inside it): CTAs run in
+  // launch order, so the resident ones work on one contiguous window of the (cell-sorted)
+  // droplets and the field lines their stencils share stay in L2
+  constexpr int WPB = FTHREADS / 32;
+  const long long per = (ngroups + gridDim.x - 1) / gridDim.x;
+  const long long g_lo = (long long)blockIdx.x * per;
+  const long long g_hi = g_lo + per < ngroups ? g_lo + per : ngroups;
+  const long long wg = g_lo + (threadIdx.x >> 5);
+  constexpr long long nw = WPB;
   // positions of the warp's next group are loaded while the current one is processed
   double px = 0.0, py = 0.0, pz = 0.0;
-  if (wg < ngroups) {
+  if (wg < g_hi) {
     const long long i0 = wg * FDROP + r, ii0 = i0 < n ? i0 : n - 1;
     px = pos[3 * ii0]; py = pos[3 * ii0 + 1]; pz = pos[3 * ii0 + 2];
   }
-  for (long long grp = wg; grp < ngroups; grp += nw) {
+  for (long long grp = wg; grp < g_hi; grp += nw) {
     const long long i = grp * FDROP + r;
     PtFrame f;
     point_frame(px, py, pz, N, L, f);
-    if (grp + nw < ngroups) {
+    if (grp + nw < g_hi) {
       const long long i1 = (grp + nw) * FDROP + r, ii1 = i1 < n ? i1 : n - 1;
       px = pos[3 * ii1]; py = pos[3 * ii1 + 1]; pz = pos[3 * ii1 + 2];
     }

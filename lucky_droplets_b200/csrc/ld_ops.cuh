@@ -57,7 +57,8 @@ template <typename T, int N> struct Ops {
     if constexpr (!PIPE) {
       return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
     } else {
-      if (choice == 0) return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
+      if (choice == 0 || cdiv(ncols, TB) * (long long)nf * nouter >= (1LL << 31))
+        return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
       ProfScope ps(p, kid, s);
       auto k = k_colfft_pipe<T, N, INV, St>;
       if (int rc = set_smem(k, 2 * COL_SMEM)) return rc;
