@@ -179,6 +179,14 @@ class ForcedDNS:
         for k in range(nsteps):
             self._step_one(stream)
 
+    def capture(self, nsteps):
+        """Capture `nsteps` steps from the current step count into a CUDA graph (nothing runs
+        during the capture; the step counters are left as they were).  Returns a StepGraph whose
+        replay() advances the state by nsteps steps with one graph launch.  The re-sorting of the
+        droplets every sort_every steps is part of the graph, at the positions the current step
+        count gives, so a replay must start at the same step count modulo sort_every."""
+        return StepGraph(self, nsteps)
+
     def _step_one(self, stream, before_droplets=None, before_collide=None):
         """One time step on `stream`.  `before_droplets()` is called just before the first droplet
         stage is enqueued, `before_collide()` after the state is final (update, epilogue and any
@@ -276,6 +284,39 @@ class ForcedDNS:
         if flags & (_lib.STATUS_BLOWUP | _lib.STATUS_NONFINITE):
             raise BlowUpError(f"threshold exceeded or non-finite state at t={self.t:.6g} (flags={flags})")
         return flags
+
+
+class StepGraph:
+    """`nsteps` steps of a ForcedDNS captured as one CUDA graph (see ForcedDNS.capture).  The
+    buffers the steps use must stay where they are (they do: every operation works in place)."""
+
+    def __init__(self, dns, nsteps):
+        torch = _torch()
+        self.dns = dns
+        self.nsteps = int(nsteps)
+        self.period = dns.sort_every if (dns.droplets is not None and dns.sort_every > 0) else 0
+        self.phase = dns.nstep % self.period if self.period else 0
+        saved = (dns.t, dns.nstep)
+        self.graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(device=dns.plan.device)
+        cap.wait_stream(torch.cuda.current_stream())
+        try:
+            with torch.cuda.graph(self.graph, stream=cap, capture_error_mode="thread_local"):
+                dns.step(self.nsteps, stream=cap)
+        finally:
+            dns.t, dns.nstep = saved
+
+    def replay(self, n=1):
+        """Advance the state by n * nsteps steps (graph launches on the current stream)."""
+        dns = self.dns
+        for _ in range(n):
+            if self.period and dns.nstep % self.period != self.phase:
+                raise RuntimeError(f"step graph captured at step phase {self.phase} (mod {self.period}), "
+                                   f"replayed at step {dns.nstep}")
+            self.graph.replay()
+            for _ in range(self.nsteps):  # the same sum as stepping one by one
+                dns.t += dns.dt
+            dns.nstep += self.nsteps
 
 
 class Droplets:

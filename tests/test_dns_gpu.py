@@ -220,3 +220,47 @@ def test_step_host_matches_device_steps(torch):
         return p[np.lexsort((p[:, 1], p[:, 0]))]
 
     assert m > 0 and np.array_equal(pair_set(b, db), pair_set(a, da))
+
+
+def test_step_graph_replay_matches_eager_steps(torch):
+    """Steps replayed from a CUDA graph (ForcedDNS.capture) leave exactly the state of steps
+    launched one by one, re-sorting (every 4 steps, inside the graph) and collisions included; a
+    replay at another step phase of the re-sorting is refused."""
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    from lucky_droplets_b200.collide import Collider
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3, g=0.1)
+    uk0, u0 = C.init_flow(C.ConfigGrid(N), prm, seed=9)
+    pos, tau, rad = C.init_droplets(prm, 9, "uniform_tau", nd=3000)
+    rad = rad * 5.0
+    vel = C.gather(u0, pos, "tricubic")
+    runs = []
+    for _ in range(2):
+        dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision="f32")
+        dns.set_uk_full(uk0)
+        d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g, radius=rad)
+        dns.attach(d, collider=Collider(d.n, 2 * rad.max()), sort_every=4)
+        dns.step(2)
+        runs.append((dns, d))
+    (a, da), (b, db) = runs
+    g = b.capture(8)  # at step 2: phase 2 of the re-sorting period
+    assert b.nstep == 2
+    g.replay(2)
+    a.step(16)
+    torch.cuda.synchronize()
+    assert a.nstep == b.nstep == 18 and a.t == b.t
+    assert torch.equal(a.uk, b.uk)
+    assert torch.equal(da.pos, db.pos) and torch.equal(da.vel, db.vel) and torch.equal(da.ids, db.ids)
+    m = int(a.collider.count.item())
+    assert m > 0 and m == int(b.collider.count.item())
+
+    def pair_set(dns, d):
+        ids = d.ids.cpu().numpy()
+        p = ids[dns.pairs[:m].cpu().numpy().astype(np.int64)]
+        p = np.stack([p.min(axis=1), p.max(axis=1)], axis=1)
+        return p[np.lexsort((p[:, 1], p[:, 0]))]
+
+    assert np.array_equal(pair_set(a, da), pair_set(b, db))
+    b.step(1)
+    with pytest.raises(RuntimeError):
+        g.replay()
