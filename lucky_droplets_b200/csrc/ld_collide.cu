@@ -381,7 +381,7 @@ __device__ __forceinline__ bool near_f(const float4 a, const float4 b, float L, 
 // indices) in scr; k_emit_pairs writes the pairs from the scanned counts, searching again only
 // for droplets with more than KEEP partners.
 constexpr int COL_THREADS = 256;
-constexpr int KEEP = 4;
+constexpr int KEEP = 16;  // partners recorded per droplet (more: searched again by k_emit_pairs)
 constexpr int kColSmemRows = 12288;  // 192 KB of staged FP32 rows per block at most
 
 __device__ __forceinline__ void col_offset(int q, int& ox, int& oy) {

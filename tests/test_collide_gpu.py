@@ -168,8 +168,7 @@ def test_contact_distance_boundary(torch, rel_gap):
 
 
 def test_dense_cluster_many_partners(torch):
-    """About 7 partners per droplet (most beyond the recorded first four, nc >= 3): the emitted
-    list still equals the FP64 rule's."""
+    """About 7 partners per droplet (nc >= 3): the emitted list still equals the FP64 rule's."""
     rng = np.random.default_rng(21)
     pos = rng.uniform(0.0, 1.0, (8000, 3))
     rad = np.full(8000, 0.03)
@@ -199,3 +198,16 @@ def test_crowded_cell_beside_sparse_cells(torch):
     a = c.collide(p, r, cap=100000).cpu().numpy()
     b = c.collide(p, r, cap=100000).cpu().numpy()
     assert np.array_equal(a, b)
+
+
+def test_partners_beyond_the_record_are_searched_again(torch):
+    """About 100 partners per droplet, far beyond the sixteen the count pass records: every
+    droplet's pairs come from the emit pass's second search, and the list equals the FP64
+    rule's."""
+    rng = np.random.default_rng(44)
+    pos = rng.uniform(2.0, 2.5, (3000, 3))
+    rad = np.full(3000, 0.05)
+    got, _ = gpu_pairs(torch, pos, rad, 0.1, cap=400000)
+    ref = K.collide(pos, rad, 0.1)
+    assert len(ref) > 100000
+    assert got.shape == ref.shape and np.array_equal(got, ref)
