@@ -161,6 +161,12 @@ LD_API int ld_plan_set_tuning(ld_plan* plan, const int32_t* choice);
  * (F:319-321); vk = NULL switches it off. */
 LD_API int ld_slow_manifold(ld_plan* plan, void* vk, double tps, double g);
 LD_API int ld_step_epilogue(ld_plan* plan, void* uk, void* stream);
+/* The same epilogue restricted to the kz = 0 plane (its reality symmetrisation, projection and
+ * checks, F:596-620): the last stage of ld_rk2if_stage (stage 2) and of ld_rk4_stage (stage 4)
+ * already applies the epilogue's projection and checks to the kz > 0 modes it writes, so after
+ * those stages this call completes the step epilogue (ld_step_epilogue there is also correct: it
+ * projects the kz > 0 modes a second time). */
+LD_API int ld_step_epilogue_plane0(ld_plan* plan, void* uk, void* stream);
 
 /* ---- droplets, P:52-111, P:435-511, P:817-837 ----------------------------------------- */
 /* Interpolate ncomp physical fields (ncomp, N, N, N) at n positions (n, 3) double:

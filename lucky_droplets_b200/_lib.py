@@ -49,6 +49,7 @@ SIGNATURES = {
     "ld_rk2if_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_p]),
     "ld_rk4_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_p]),
     "ld_step_epilogue": (_c_i, [_c_p, _c_p, _c_p]),
+    "ld_step_epilogue_plane0": (_c_i, [_c_p, _c_p, _c_p]),
     "ld_gather": (_c_i, [_c_p, _c_p, _c_i, _c_p, _c_i64, _c_i, _c_p, _c_p]),
     "ld_droplet_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_i, _c_d, _c_d, _c_p]),
     "ld_profile": (_c_i, [_c_p, _c_i]),

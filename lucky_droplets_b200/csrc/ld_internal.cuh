@@ -90,6 +90,7 @@ struct OpsTable {
   int (*rhs)(ld_plan*, int mode, void* s0, void* s1, void* s2, void* s3, void* uout,
              const ld_flow_params*, double visc, cudaStream_t);
   int (*epilogue)(ld_plan*, void* uk, cudaStream_t);
+  int (*epilogue0)(ld_plan*, void* uk, cudaStream_t);
   int (*gather)(ld_plan*, const void* f, int ncomp, const double* pos, long long n, int method, void* out,
                 cudaStream_t);
   int (*dstage)(ld_plan*, int stage, int method, const void* u, double* pos, void* vel, const void* tau,

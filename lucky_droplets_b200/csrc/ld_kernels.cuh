@@ -269,7 +269,32 @@ template <typename T> struct UpdArgs {
   // s2 in stage 2) into shared memory with cp.async while the x transforms run; the launcher
   // sets it when the (3, Mx, TB) buffer fits beside the exchange buffer at 2 CTAs per SM
   int prefetch;
+  // final stages (UPD_RK2_2, UPD_RK4_4): the step epilogue's work on the kz > 0 modes (projection
+  // and the non-finite / blow-up checks, as k_epilogue does them) is done here, so that the
+  // epilogue that follows needs only the kz = 0 plane (k_epilogue_plane0)
+  T blowup;
 };
+
+// The step epilogue of one kz > 0 mode (k_epilogue's arithmetic): projection with its own k
+// inside the mask, zero outside; flags for non-finite values and the blow-up threshold.
+template <typename T>
+__device__ __forceinline__ void epi_mode(cplx<T> (&v)[3], int kx, int ky, int kz, int kc, T blowup, unsigned& flags) {
+  const int k2 = kx * kx + ky * ky + kz * kz;
+  if (kz <= kc && k2 <= kc * kc + kc) {
+    const T qx = T(kx), qy = T(ky), qz = T(kz);
+    cplx<T> kd = cscale(cadd(cadd(cscale(v[0], qx), cscale(v[1], qy)), cscale(v[2], qz)), T(1) / T(k2));
+    v[0] = csub(v[0], cscale(kd, qx));
+    v[1] = csub(v[1], cscale(kd, qy));
+    v[2] = csub(v[2], cscale(kd, qz));
+  } else {
+    v[0] = v[1] = v[2] = czero<cplx<T>>();
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (!(isfinite(v[c].x) && isfinite(v[c].y))) flags |= LD_STATUS_NONFINITE;
+    if (v[c].x > blowup) flags |= LD_STATUS_BLOWUP;
+  }
+}
 
 template <typename T, int N, int MODE>
 __global__ void __launch_bounds__(Cfg<N>::COL_THREADS, (N == 256 && sizeof(T) == 4) ? 2 : 1)
@@ -389,35 +414,46 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
         A.s2[cc * A.cs + idx] = ac;
       }
     } else if (MODE == UPD_RK2_2) {
+      cplx<T> v[3];
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) {
         const cplx<T> acc = pre ? ybuf[(cc * Mx + r) * TB + c] : A.s2[cc * A.cs + idx];
-        cplx<T> v = cadd(acc, cscale(rhs[cc], T(0.5) * h));
-        if (!keep) v = czero<cplx<T>>();
-        if (!(isfinite(v.x) && isfinite(v.y))) flags |= LD_STATUS_NONFINITE;
-        A.s0[cc * A.cs + idx] = v;
+        v[cc] = cadd(acc, cscale(rhs[cc], T(0.5) * h));
+        if (!keep) v[cc] = czero<cplx<T>>();
+        if (!(isfinite(v[cc].x) && isfinite(v[cc].y))) flags |= LD_STATUS_NONFINITE;
       }
+      if (kzi > 0) epi_mode(v, kxi, kyi, kzi, kc, A.blowup, flags);
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) A.s0[cc * A.cs + idx] = v[cc];
     } else {
       // RK4 (F:341-360): ku = rhs - nu k^2 y ;  y = stage input
       const T lv = A.nu * T(k2);
       cplx<T> ku[3];
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) ku[cc] = csub(rhs[cc], cscale(y[cc], lv));
+      if (MODE == UPD_RK4_4) {
+        cplx<T> v[3];
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) {
-        const long long o = cc * A.cs + idx;
-        if (MODE == UPD_RK4_1) {
-          cplx<T> un = y[cc];
-          A.s2[o] = cadd(un, cscale(ku[cc], h / T(6)));
-          A.s3[o] = cadd(un, cscale(ku[cc], h / T(2)));
-        } else if (MODE == UPD_RK4_2 || MODE == UPD_RK4_3) {
-          cplx<T> un = A.s0[o];
-          A.s2[o] = cadd(A.s2[o], cscale(ku[cc], h / T(3)));
-          A.s3[o] = cadd(un, cscale(ku[cc], MODE == UPD_RK4_2 ? h / T(2) : h));
-        } else {
-          cplx<T> v = cadd(A.s2[o], cscale(ku[cc], h / T(6)));
-          if (!(isfinite(v.x) && isfinite(v.y))) flags |= LD_STATUS_NONFINITE;
-          A.s0[o] = v;
+        for (int cc = 0; cc < 3; ++cc) {
+          v[cc] = cadd(A.s2[cc * A.cs + idx], cscale(ku[cc], h / T(6)));
+          if (!(isfinite(v[cc].x) && isfinite(v[cc].y))) flags |= LD_STATUS_NONFINITE;
+        }
+        if (kzi > 0) epi_mode(v, kxi, kyi, kzi, kc, A.blowup, flags);
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) A.s0[cc * A.cs + idx] = v[cc];
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) {
+          const long long o = cc * A.cs + idx;
+          if (MODE == UPD_RK4_1) {
+            cplx<T> un = y[cc];
+            A.s2[o] = cadd(un, cscale(ku[cc], h / T(6)));
+            A.s3[o] = cadd(un, cscale(ku[cc], h / T(2)));
+          } else {  // UPD_RK4_2, UPD_RK4_3
+            cplx<T> un = A.s0[o];
+            A.s2[o] = cadd(A.s2[o], cscale(ku[cc], h / T(3)));
+            A.s3[o] = cadd(un, cscale(ku[cc], MODE == UPD_RK4_2 ? h / T(2) : h));
+          }
         }
       }
     }
@@ -852,6 +888,51 @@ __global__ void k_epilogue(cplx<T>* __restrict__ u, long long cs, int kc, int My
       u[c * cs + e] = v[c];
       if (!(isfinite(v[c].x) && isfinite(v[c].y))) flags |= LD_STATUS_NONFINITE;
       if (v[c].x > blowup) flags |= LD_STATUS_BLOWUP;
+    }
+  }
+  if (flags) atomicOr(status, flags);
+}
+
+// The step epilogue on the kz = 0 plane only (k_epilogue's kz = 0 branch): for a state whose
+// kz > 0 modes the final update stage has already projected and checked.
+template <typename T>
+__global__ void k_epilogue_plane0(cplx<T>* __restrict__ u, long long cs, int kc, int My, int Mzp, T blowup,
+                                  unsigned* status) {
+  const long long total = (long long)My * My;
+  unsigned flags = 0;
+  for (long long e2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; e2 < total; e2 += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(e2 / My), iy = (int)(e2 - (long long)ix * My);
+    const int kx = cfreq(ix, kc), ky = cfreq(iy, kc);
+    const long long e = e2 * Mzp;
+    const int jx = kx == 0 ? 0 : (-kx < 0 ? -kx + 2 * kc + 1 : -kx);
+    const int jy = ky == 0 ? 0 : (-ky < 0 ? -ky + 2 * kc + 1 : -ky);
+    const bool mine = (kx > 0) || (kx == 0 && ky >= 0);
+    if (!mine) continue;
+    const long long ep = ((long long)jx * My + jy) * Mzp;
+    cplx<T> v[3], w[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      cplx<T> a = u[c * cs + e], b = u[c * cs + ep];
+      v[c] = cmk(T(0.5) * (a.x + b.x), T(0.5) * (a.y - b.y));
+      w[c] = cconj(v[c]);
+    }
+    for (int side = 0; side < 2; ++side) {
+      cplx<T>* q = side ? w : v;
+      const T qx = T(side ? -kx : kx), qy = T(side ? -ky : ky);
+      const int k2 = kx * kx + ky * ky;
+      if (k2 > 0 && k2 <= kc * kc + kc) {
+        cplx<T> kd = cscale(cadd(cscale(q[0], qx), cscale(q[1], qy)), T(1) / T(k2));
+        q[0] = csub(q[0], cscale(kd, qx));
+        q[1] = csub(q[1], cscale(kd, qy));
+      }
+      if (k2 > kc * kc + kc) { q[0] = q[1] = q[2] = czero<cplx<T>>(); }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      u[c * cs + e] = v[c];
+      if (ep != e) u[c * cs + ep] = w[c];
+      if (!(isfinite(v[c].x) && isfinite(v[c].y))) flags |= LD_STATUS_NONFINITE;
+      if (v[c].x > blowup || w[c].x > blowup) flags |= LD_STATUS_BLOWUP;
     }
   }
   if (flags) atomicOr(status, flags);

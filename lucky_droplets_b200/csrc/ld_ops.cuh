@@ -320,6 +320,7 @@ template <typename T, int N> struct Ops {
     A.h = T(prm->dt); A.nu = T(prm->nu); A.visc = T(visc);
     A.kc = kc; A.My = My; A.Mzp = Mzp; A.status = p->status;
     A.vk = (C*)p->sm_vk; A.tps = T(p->sm_tps); A.vg = T(p->sm_tps * p->sm_g * (double)N * N * N);
+    A.blowup = T(100.0 * (double)N * N * N);  // the blow-up threshold of the step epilogue (F:618)
     // RK2 stages stage their cube rows in shared memory when that keeps 2 CTAs per SM
     const size_t pre_bytes = sizeof(C) * 3 * (size_t)(2 * kc + 1) * TB;
     constexpr bool RK2 = MODE == UPD_RK2_1 || MODE == UPD_RK2_2;
@@ -431,7 +432,16 @@ template <typename T, int N> struct Table {
     ld::k_epilogue<T><<<grid1d(total, 256), 256, 0, s>>>((C*)uk, total, p->kc, p->My, p->Mzp, T(blow), p->status);
     LD_LAUNCH_CHECK();
     return LD_OK;
+  }  static int epilogue0(ld_plan* p, void* uk, cudaStream_t s) {
+    ProfScope ps(p, KID_EPILOGUE, s);
+    const double blow = 100.0 * (double)N * N * N;
+    const long long plane = (long long)p->My * p->My;
+    ld::k_epilogue_plane0<T><<<grid1d(plane, 256), 256, 0, s>>>((C*)uk, p->cube_elems(), p->kc, p->My, p->Mzp,
+                                                                 T(blow), p->status);
+    LD_LAUNCH_CHECK();
+    return LD_OK;
   }
+
   static int gather(ld_plan* p, const void* f, int nc, const double* pos, long long n, int method, void* out,
                     cudaStream_t s) {
     return O::gather(p, (const T*)f, nc, pos, n, method, (T*)out, s);
@@ -442,7 +452,7 @@ template <typename T, int N> struct Table {
   }
   static const OpsTable* get() {
     static const OpsTable t = {rfft_full, irfft_full, irfft_cube, rfft_cube, to_cube, from_cube,
-                               shell_spectrum, rhs, epilogue, gather, dstage, autotune};
+                               shell_spectrum, rhs, epilogue, epilogue0, gather, dstage, autotune};
     return &t;
   }
 };

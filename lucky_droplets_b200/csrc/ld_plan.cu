@@ -288,6 +288,12 @@ int ld_step_epilogue(ld_plan* p, void* uk, void* stream) {
   return table_of(p)->epilogue(p, uk, S(stream));
 }
 
+int ld_step_epilogue_plane0(ld_plan* p, void* uk, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!uk) return ld_fail(LD_ERR_ARG, "ld_step_epilogue_plane0: bad arguments");
+  return table_of(p)->epilogue0(p, uk, S(stream));
+}
+
 int ld_gather(ld_plan* p, const void* field, int ncomp, const double* pos, int64_t n, int method, void* out,
               void* stream) {
   if (int rc = check_plan(p)) return rc;

@@ -217,7 +217,7 @@ class ForcedDNS:
             for s in (1, 2, 3, 4):
                 check(L.ld_rk4_stage(h, s, ptr(self.uk), ptr(self.aux), ptr(self.acc), None, prm, st))
         if self.epilogue:
-            check(L.ld_step_epilogue(h, ptr(self.uk), st))
+            check(L.ld_step_epilogue_plane0(h, ptr(self.uk), st))
         self.t += self.dt
         self.nstep += 1
         droplets_ready()

@@ -207,6 +207,6 @@ class ReferenceRun:
             if nd:
                 check(L.ld_copy_async(ptr(d.coord), ptr(self.sump), nd * 7 * 8, st))          # F:582
             self.clip_zero(self.n_new, self.n, False, stream)                                 # F:584
-            check(L.ld_step_epilogue(p.handle, ptr(dns.uk), st))                              # F:596-620
+            check(L.ld_step_epilogue_plane0(p.handle, ptr(dns.uk), st))                       # F:596-620
             dns.t += h
             dns.nstep += 1
