@@ -285,15 +285,16 @@ __device__ __forceinline__ void tail_features(const float* tc, unsigned (&w)[8])
   for (int j = 2; j < 8; ++j) w[j] = 0u;
 }
 
-// Grid-memory offset (in vec4 elements; N <= 1024, so N^3 fits an int) of canonical index j
-// along canonical axis k of a point (cell ci, frame code): along grid axis p[k], reversed when
-// that axis is reflected.
-__device__ __forceinline__ int canon_offset(const int* ci, int code, int N, int k, int j) {
+// Grid-memory offset, in scalar elements of the interleaved field (4 per grid point), of canonical
+// index j along canonical axis k of a point (cell ci, frame code): along grid axis p[k], reversed
+// when that axis is reflected.  Unsigned 32-bit: 4 N^3 <= 2^32 for N <= 1024.
+__device__ __forceinline__ unsigned canon_offset(const int* ci, int code, int N, int k, int j) {
   const int d = frame_perm(code, k);
   const int o = (code >> (6 + d)) & 1 ? 3 - j : j;
   const int cid = d == 0 ? ci[0] : (d == 1 ? ci[1] : ci[2]);
-  const int g = (cid - 1 + o + N) & (N - 1);
-  return d == 0 ? g * N * N : (d == 1 ? g * N : g);
+  const unsigned g = (unsigned)((cid - 1 + o + N) & (N - 1));
+  const unsigned n = (unsigned)N;
+  return 4u * (d == 0 ? g * n * n : (d == 1 ? g * n : g));
 }
 
 // Canonical component c of the point's 64-tap stencil, straight from the interleaved field into
@@ -303,24 +304,24 @@ __device__ __forceinline__ int canon_offset(const int* ci, int code, int N, int 
 template <typename T>
 __device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
                                                   float (&v)[64]) {
-  int o0[4], o1[4], o2[4];
+  const int d = frame_perm(f.code, c);
+  const float sg = frame_sign(f.code, d);
+  unsigned o0[4], o1[4], o2[4];
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    o0[j] = canon_offset(f.i, f.code, N, 0, j);
+    o0[j] = canon_offset(f.i, f.code, N, 0, j) + (unsigned)d;  // the component folded in once
     o1[j] = canon_offset(f.i, f.code, N, 1, j);
     o2[j] = canon_offset(f.i, f.code, N, 2, j);
   }
-  const int d = frame_perm(f.code, c);
-  const float sg = frame_sign(f.code, d);
-  const T* base = reinterpret_cast<const T*>(u4) + d;
+  // one warp-uniform base pointer and a 32-bit offset per tap
+  const T* base = reinterpret_cast<const T*>(u4);
 #pragma unroll
   for (int j0 = 0; j0 < 4; ++j0)
 #pragma unroll
     for (int j1 = 0; j1 < 4; ++j1) {
-      const int o01 = o0[j0] + o1[j1];
+      const unsigned o01 = o0[j0] + o1[j1];
 #pragma unroll
-      for (int j2 = 0; j2 < 4; ++j2)
-        v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (size_t)(unsigned)(o01 + o2[j2]) * 4));
+      for (int j2 = 0; j2 < 4; ++j2) v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (o01 + o2[j2])));
     }
   return sg;
 }
