@@ -328,17 +328,28 @@ def train_learned(a, seed):
 
 def judge_learned(dns, d, li, frac, seed):
     """The judge: exact spectral sum at a random fraction of the droplets against the learned and
-    the tricubic velocities of the current state; device time of the whole judge."""
+    the tricubic velocities of the current state.  The errors (and the network's enabled flag)
+    come from LearnedInterp.judge; its device time is taken on a second, identical pass of the
+    device work alone (interleaved field, exact sum, inference, tricubic gather), so that neither
+    first-use allocations nor the host reductions fall between the events."""
     import torch
+    from lucky_droplets_b200 import _lib
+    from lucky_droplets_b200._lib import check, ptr, stream_ptr
     n = max(1, int(round(frac * d.n)))
     g = torch.Generator(device="cpu").manual_seed(seed)
     sel = torch.randperm(d.n, generator=g)[:n].to(d.pos.device)
     pos = d.pos[sel].contiguous()
+    e_l, e_t = li.judge(dns.uk, li.interleaved(dns.uk), pos)
+    p = dns.plan
+    tric = torch.empty((n, 3), dtype=p.rdtype, device=p.device)
+    torch.cuda.synchronize()
     s = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(s)
     u4 = li.interleaved(dns.uk)
-    e_l, e_t = li.judge(dns.uk, u4, pos)
+    p.exact_sum(dns.uk, pos)
+    li.infer(u4, pos)
+    check(_lib.lib().ld_gather4(p.handle, ptr(u4), ptr(pos), n, _lib.LD_INTERP["tricubic"], ptr(tric), stream_ptr()))
     e1.record(s)
     torch.cuda.synchronize()
     return {"learned": e_l, "tricubic": e_t, "n_sample": n, "enabled": li.enabled, "judge_ms": e0.elapsed_time(e1)}
