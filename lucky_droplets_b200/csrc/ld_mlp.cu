@@ -664,6 +664,14 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   bool failed = false;
   for (long long i = g; i < mine && !failed; i += 2) {
     const long long tile = blockIdx.x + i * (long long)gridDim.x;
+    // the output warps' aux rows (tricubic xyz, scale, frame code) load while the layers run
+    const long long orow = tile * TM + 32 * gw + lane;
+    float4 ax0 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int code = 0;
+    if (gw < 4 && orow < n) {
+      ax0 = *reinterpret_cast<const float4*>(auxg + orow * 8);
+      code = __float_as_int(auxg[orow * 8 + 4]);
+    }
     // X of this tile (the i-th copy into the X buffer, on bar_x[g], the group's (i/2)-th wait);
     // failures are made group-uniform
     failed = group_or(g, !mbar_wait_bounded(&bar_x[g], (unsigned)((i >> 1) & 1), kWaitLimitMlp));
@@ -728,18 +736,16 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
           umma_commit(&bar_mma[g]);
         }
       } else if (gw < 4) {
-        const int row = 32 * gw + lane;
         float v[16];
         tmem_ld16(tmem + ((unsigned)(32 * gw) << 16) + 128u, v);
-        const long long ii = tile * TM + row;
-        if (ii < n) {
-          const float* ax = auxg + ii * 8;
-          const int code = __float_as_int(ax[4]);
+        if (orow < n) {
+          const float tg[3] = {ax0.x, ax0.y, ax0.z};
 #pragma unroll
           for (int c = 0; c < D_OUT; ++c) {
             const int cg = frame_perm(code, c);
             const float y = v[c] + bias[2 * H + c];
-            out[3 * ii + cg] = T(ax[cg] + ax[3] * (os * frame_sign(code, cg) * y));
+            const float t = cg == 0 ? tg[0] : (cg == 1 ? tg[1] : tg[2]);
+            out[3 * orow + cg] = T(t + ax0.w * (os * frame_sign(code, cg) * y));
           }
         }
       }
