@@ -193,20 +193,20 @@ __device__ __forceinline__ void point_frame(double px, double py, double pz, int
 // Tricubic weights of the canonical offsets in the polynomial basis (per canonical axis): with
 // U the basis above (row norms^2 4, 20, 4, 20), w.s = sum_i (U w)_i (U s)_i / |U_i|^2, so the
 // tricubic value is sum_i D_i wh0[i0] wh1[i1] wh2[i2] with wh = (U w) / |U|^2.
+__device__ __forceinline__ void tric_weight_axis(float t, float (&w)[4]) {
+  w[0] = -t * (t - 1.f) * (t - 2.f) / 6.f;
+  w[1] = (t + 1.f) * (t - 1.f) * (t - 2.f) / 2.f;
+  w[2] = -(t + 1.f) * t * (t - 2.f) / 2.f;
+  w[3] = (t + 1.f) * t * (t - 1.f) / 6.f;
+  poly4(w, 1);
+  w[0] *= 0.25f;
+  w[1] *= 0.05f;
+  w[2] *= 0.25f;
+  w[3] *= 0.05f;
+}
 __device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4]) {
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float t = tc[k];
-    wh[k][0] = -t * (t - 1.f) * (t - 2.f) / 6.f;
-    wh[k][1] = (t + 1.f) * (t - 1.f) * (t - 2.f) / 2.f;
-    wh[k][2] = -(t + 1.f) * t * (t - 2.f) / 2.f;
-    wh[k][3] = (t + 1.f) * t * (t - 1.f) / 6.f;
-    poly4(wh[k], 1);
-    wh[k][0] *= 0.25f;
-    wh[k][1] *= 0.05f;
-    wh[k][2] *= 0.25f;
-    wh[k][3] *= 0.05f;
-  }
+  for (int k = 0; k < 3; ++k) tric_weight_axis(tc[k], wh[k]);
 }
 
 // One component's 64 taps (canonical order, in registers) -> its polynomial coefficients, then
@@ -322,6 +322,25 @@ __device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4
       const unsigned o01 = o0[j0] + o1[j1];
 #pragma unroll
       for (int j2 = 0; j2 < 4; ++j2) v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (o01 + o2[j2])));
+    }
+  return sg;
+}
+
+// The same gather from the point's canonical offsets o[k][j] (canon_offset of axis k, index j),
+// computed elsewhere.
+template <typename T>
+__device__ __forceinline__ float gather_component_at(const vec4<T>* __restrict__ u4, const PtFrame& f, int c,
+                                                     const unsigned (&o)[3][4], float (&v)[64]) {
+  const int d = frame_perm(f.code, c);
+  const float sg = frame_sign(f.code, d);
+  const T* base = reinterpret_cast<const T*>(u4);
+#pragma unroll
+  for (int j0 = 0; j0 < 4; ++j0)
+#pragma unroll
+    for (int j1 = 0; j1 < 4; ++j1) {
+      const unsigned o01 = o[0][j0] + (unsigned)d + o[1][j1];
+#pragma unroll
+      for (int j2 = 0; j2 < 4; ++j2) v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (o01 + o[2][j2])));
     }
   return sg;
 }
@@ -508,13 +527,30 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
       const long long i1 = (grp + nw) * FDROP + r, ii1 = i1 < n ? i1 : n - 1;
       px = pos[3 * ii1]; py = pos[3 * ii1 + 1]; pz = pos[3 * ii1 + 2];
     }
-    float v[64];
-    const float sg = gather_component<T>(u4, N, f, c, v);
-    comp_transform(v);
-    float wh[3][4];
-    tric_weights(f.tc, wh);
-    const CompSums cs = comp_sums(v, wh, mode == 0.f);
+    // the three lanes of a droplet split the per-point work by canonical axis (lane 3r + c takes
+    // axis c's stencil offsets and tricubic weights) and exchange it by shuffles
     const int b0 = 3 * r;
+    unsigned o[3][4];
+    float wh[3][4];
+    {
+      unsigned oc[4];
+      float wc[4];
+      const float tcc = c == 0 ? f.tc[0] : (c == 1 ? f.tc[1] : f.tc[2]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) oc[j] = canon_offset(f.i, f.code, N, c, j);
+      tric_weight_axis(tcc, wc);
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          o[k][j] = __shfl_sync(0xffffffffu, oc[j], b0 + k);
+          wh[k][j] = __shfl_sync(0xffffffffu, wc[j], b0 + k);
+        }
+    }
+    float v[64];
+    const float sg = gather_component_at<T>(u4, f, c, o, v);
+    comp_transform(v);
+    const CompSums cs = comp_sums(v, wh, mode == 0.f);
     const float ss0 = __shfl_sync(0xffffffffu, cs.ss, b0), ss1 = __shfl_sync(0xffffffffu, cs.ss, b0 + 1),
                 ss2 = __shfl_sync(0xffffffffu, cs.ss, b0 + 2);
     const float sh0 = __shfl_sync(0xffffffffu, cs.sh, b0), sh1 = __shfl_sync(0xffffffffu, cs.sh, b0 + 1),
