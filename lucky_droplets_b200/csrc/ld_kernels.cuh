@@ -89,6 +89,17 @@ template <typename T, int N> struct StRows {
   }
 };
 
+// The same with the row map fixed at compile time (MAP: compact cube rows through crow, else the
+// identity), for the passes whose layout is known when they are instantiated.
+template <typename T, int N, bool MAP> struct StRowsC {
+  RowsIO<T> io;
+  __device__ __forceinline__ void operator()(int f, int o, int n, int col, cplx<T> v) const {
+    const int r = MAP ? crow(n, N, io.kc) : n;
+    if (r < 0) return;
+    io.p[io.at(f, o, r, col)] = v;
+  }
+};
+
 // Storer into the cube that also applies the spherical mask round(|k|) <= kc (F:129): the last
 // (x) pass of a forward cube transform.  Columns are the flat (ky, kz) index of a kx plane.
 template <typename T, int N> struct StCube {
@@ -164,7 +175,7 @@ k_colfft(Ld ld, St st, int ncols, int nf, const cplx<T>* __restrict__ tw) {
 // rows of the CTA's next item stream into the other shared buffer with 16-byte cp.async copies;
 // the buffer an item was staged in serves as its FFT exchange buffer once its values sit in
 // registers.  Rows the loader's row map drops (r < 0) and columns past ncols are not copied.
-template <typename T, int N, bool INV, class St>
+template <typename T, int N, bool INV, class St, bool IN_MAP>
 __global__ void __launch_bounds__(Cfg<N>::COL_THREADS, 3)
 k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>* __restrict__ tw) {
   constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
@@ -192,7 +203,7 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
     for (int q = threadIdx.x; q < N * CPR; q += blockDim.x) {
       const int n = q / CPR, k = q - n * CPR;
       if (k >= cpr) continue;
-      const int r = in.kc < 0 ? n : crow(n, N, in.kc);
+      const int r = IN_MAP ? crow(n, N, in.kc) : n;
       if (r < 0) continue;
       const char* src = reinterpret_cast<const char*>(in.p + in.at(itm.f, itm.o, r, col0)) + 16 * k;
       const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst + n * TB) + 16 * k);
@@ -215,7 +226,7 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const int n = j + NT * m;
-      const int r = in.kc < 0 ? n : crow(n, N, in.kc);
+      const int r = IN_MAP ? crow(n, N, in.kc) : n;
       a[m] = (ok && r >= 0) ? cscale(cur[n * TB + c], in.scale) : czero<cplx<T>>();
     }
     __syncthreads();  // every value is in registers: cur becomes the exchange buffer

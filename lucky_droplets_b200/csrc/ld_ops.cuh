@@ -50,7 +50,9 @@ template <typename T, int N> struct Ops {
 
   // Column pass over plain strided rows: the pipelined kernel where two staging buffers fit.
   static constexpr bool PIPE = 2 * COL_SMEM <= 72 * 1024;
-  template <bool INV, class St>
+  // IN_MAP: the input rows are compact cube rows (in.kc >= 0), fixed at compile time for the
+  // pipelined kernel
+  template <bool INV, bool IN_MAP, class St>
   static int colpass_rows(ld_plan* p, int kid, RowsIO<T> in, St st, int ncols, int nf, int nouter, const C* tw,
                           cudaStream_t s, int variant = -2) {
     const int choice = variant != -2 ? variant : p->tune_y[INV ? 0 : 1];
@@ -60,7 +62,7 @@ template <typename T, int N> struct Ops {
       if (choice == 0 || cdiv(ncols, TB) * (long long)nf * nouter >= (1LL << 31))
         return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
       ProfScope ps(p, kid, s);
-      auto k = k_colfft_pipe<T, N, INV, St>;
+      auto k = k_colfft_pipe<T, N, INV, St, IN_MAP>;
       if (int rc = set_smem(k, 2 * COL_SMEM)) return rc;
       static int occ = 0;
       if (occ == 0) {
@@ -249,10 +251,12 @@ template <typename T, int N> struct Ops {
         if (v >= nv) continue;
         auto run = [&]() -> int {
           if (pass == 0)
-            return colpass_rows<true>(p, KID_YINV, io(W1, w1s, (long long)My * Mzp, Mzp, kc),
-                                      StRows<T, N>{io(W2, w2s, (long long)N * Mzp, Mzp, -1)}, Mzp, 6, N, tw, s, v);
-          return colpass_rows<false>(p, KID_YFWD, io(W1, w2s, (long long)N * Mzp, Mzp, -1),
-                                     StRows<T, N>{io(W2, w1s, (long long)My * Mzp, Mzp, kc)}, Mzp, 3, N, tw, s, v);
+            return colpass_rows<true, true>(p, KID_YINV, io(W1, w1s, (long long)My * Mzp, Mzp, kc),
+                                            StRowsC<T, N, false>{io(W2, w2s, (long long)N * Mzp, Mzp, -1)}, Mzp, 6, N,
+                                            tw, s, v);
+          return colpass_rows<false, false>(p, KID_YFWD, io(W1, w2s, (long long)N * Mzp, Mzp, -1),
+                                            StRowsC<T, N, true>{io(W2, w1s, (long long)My * Mzp, Mzp, kc)}, Mzp, 3, N,
+                                            tw, s, v);
         };
         if (int rc = run()) return rc;  // warm-up
         LD_CUDA_CHECK(cudaEventRecord(a, s));
@@ -292,7 +296,7 @@ template <typename T, int N> struct Ops {
     // inverse y pass
     auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
     auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
-    if (int rc = colpass_rows<true>(p, KID_YINV, yin, StRows<T, N>{yout}, Mzp, 6, N, tw, s)) return rc;
+    if (int rc = colpass_rows<true, true>(p, KID_YINV, yin, StRowsC<T, N, false>{yout}, Mzp, 6, N, tw, s)) return rc;
     // fused z pass: u, w -> u x w  (W2 -> W1 as (3, N*N, Mzp))
     {
       ProfScope ps(p, KID_ZCROSS, s);
@@ -310,7 +314,7 @@ template <typename T, int N> struct Ops {
     // forward y pass (W1 -> W2 as (3, N, My, Mzp))
     auto fyin = io(W1, w2s, (long long)N * Mzp, Mzp, -1);
     auto fyout = io(W2, w1s, (long long)My * Mzp, Mzp, kc);
-    if (int rc = colpass_rows<false>(p, KID_YFWD, fyin, StRows<T, N>{fyout}, Mzp, 3, N, tw, s)) return rc;
+    if (int rc = colpass_rows<false, false>(p, KID_YFWD, fyin, StRowsC<T, N, true>{fyout}, Mzp, 3, N, tw, s)) return rc;
     // forward x pass + k-space update
     UpdArgs<T> A;
     A.nl = W2; A.nls = w1s;
