@@ -70,6 +70,9 @@ template <typename T> struct RowsIO {
   }
 };
 
+
+// Strided row loader and storer with the row map chosen at run time (io.kc < 0: rows as they are,
+// else compact cube rows through crow).
 template <typename T, int N> struct LdRows {
   RowsIO<T> io;
   __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
@@ -89,8 +92,21 @@ template <typename T, int N> struct StRows {
   }
 };
 
-// The same with the row map fixed at compile time (MAP: compact cube rows through crow, else the
-// identity), for the passes whose layout is known when they are instantiated.
+// Strided row loader: rows mapped to compact cube rows through crow (MAP) or taken as they are,
+// scaled by io.scale.
+template <typename T, int N, bool MAP> struct LdRowsC {
+  RowsIO<T> io;
+  __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
+    const int r = MAP ? crow(n, N, io.kc) : n;
+    if (r < 0) return czero<cplx<T>>();
+    cplx<T> v = io.p[io.at(f, o, r, col)];
+    return cscale(v, io.scale);
+  }
+};
+
+
+// Strided row storer: rows mapped to compact cube rows through crow (MAP; rows outside the cube
+// are not written) or taken as they are.
 template <typename T, int N, bool MAP> struct StRowsC {
   RowsIO<T> io;
   __device__ __forceinline__ void operator()(int f, int o, int n, int col, cplx<T> v) const {

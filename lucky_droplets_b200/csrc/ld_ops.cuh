@@ -57,10 +57,10 @@ template <typename T, int N> struct Ops {
                           cudaStream_t s, int variant = -2) {
     const int choice = variant != -2 ? variant : p->tune_y[INV ? 0 : 1];
     if constexpr (!PIPE) {
-      return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
+      return colpass<INV>(p, kid, LdRowsC<T, N, IN_MAP>{in}, st, ncols, nf, nouter, tw, s);
     } else {
       if (choice == 0 || cdiv(ncols, TB) * (long long)nf * nouter >= (1LL << 31))
-        return colpass<INV>(p, kid, LdRows<T, N>{in}, st, ncols, nf, nouter, tw, s);
+        return colpass<INV>(p, kid, LdRowsC<T, N, IN_MAP>{in}, st, ncols, nf, nouter, tw, s);
       ProfScope ps(p, kid, s);
       auto k = k_colfft_pipe<T, N, INV, St, IN_MAP>;
       if (int rc = set_smem(k, 2 * COL_SMEM)) return rc;
@@ -117,10 +117,10 @@ template <typename T, int N> struct Ops {
     if (int rc = z_r2c(p, u, fu, NN, Nf, Nf, Nf, NN * N, NN * Nf, ncomp, tw, s)) return rc;
     // y pass in place: columns kz (Nf), rows y, outer x
     auto yio = io(fu, NN * Nf, (long long)N * Nf, Nf, -1);
-    if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{yio}, StRows<T, N>{yio}, Nf, ncomp, N, tw, s)) return rc;
+    if (int rc = colpass<false>(p, KID_YFWD, LdRowsC<T, N, false>{yio}, StRowsC<T, N, false>{yio}, Nf, ncomp, N, tw, s)) return rc;
     // x pass in place: columns (ky, kz) flat, rows x
     auto xio = io(fu, NN * Nf, 0, N * Nf, -1);
-    return colpass<false>(p, KID_XPASS, LdRows<T, N>{xio}, StRows<T, N>{xio}, N * Nf, ncomp, 1, tw, s);
+    return colpass<false>(p, KID_XPASS, LdRowsC<T, N, false>{xio}, StRowsC<T, N, false>{xio}, N * Nf, ncomp, 1, tw, s);
   }
 
   static int irfft_full(ld_plan* p, const C* fu, T* u, int ncomp, cudaStream_t s) {
@@ -134,9 +134,9 @@ template <typename T, int N> struct Ops {
       const int nc = ncomp - c0 < chunk ? ncomp - c0 : chunk;
       auto xin = io(fu + c0 * per, per, 0, N * Nf, -1);
       auto xout = io(W, per, 0, N * Nf, -1);
-      if (int rc = colpass<true>(p, KID_XPASS, LdRows<T, N>{xin}, StRows<T, N>{xout}, N * Nf, nc, 1, tw, s)) return rc;
+      if (int rc = colpass<true>(p, KID_XPASS, LdRowsC<T, N, false>{xin}, StRowsC<T, N, false>{xout}, N * Nf, nc, 1, tw, s)) return rc;
       auto yio = io(W, per, (long long)N * Nf, Nf, -1);
-      if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yio}, StRows<T, N>{yio}, Nf, nc, N, tw, s)) return rc;
+      if (int rc = colpass<true>(p, KID_YINV, LdRowsC<T, N, false>{yio}, StRowsC<T, N, false>{yio}, Nf, nc, N, tw, s)) return rc;
       const T sc = T(1.0 / (double(N) * N * N));
       if (int rc = z_c2r(p, W, u + (long long)c0 * NN * N, NN, Nf, Nf, sc, NN * N, per, nc, tw, s)) return rc;
     }
@@ -156,10 +156,10 @@ template <typename T, int N> struct Ops {
       const int nc = ncomp - c0 < 6 ? ncomp - c0 : 6;
       auto xin = io(uk + c0 * cs, cs, 0, My * Mzp, kc);
       auto xout = io(W1, w1s, 0, My * Mzp, -1);
-      if (int rc = colpass<true>(p, KID_XPASS, LdRows<T, N>{xin}, StRows<T, N>{xout}, My * Mzp, nc, 1, tw, s)) return rc;
+      if (int rc = colpass<true>(p, KID_XPASS, LdRowsC<T, N, true>{xin}, StRowsC<T, N, false>{xout}, My * Mzp, nc, 1, tw, s)) return rc;
       auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
       auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
-      if (int rc = colpass<true>(p, KID_YINV, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, nc, N, tw, s)) return rc;
+      if (int rc = colpass<true>(p, KID_YINV, LdRowsC<T, N, true>{yin}, StRowsC<T, N, false>{yout}, Mzp, nc, N, tw, s)) return rc;
       const T sc = T(1.0 / (double(N) * N * N));
       if (int rc = z_c2r(p, W2, u + (long long)c0 * NN * N, NN, Mzp, kc + 1, sc, NN * N, w2s, nc, tw, s)) return rc;
     }
@@ -179,10 +179,10 @@ template <typename T, int N> struct Ops {
       if (int rc = z_r2c(p, u + (long long)c0 * NN * N, W2, NN, Mzp, Mzp, kc + 1, NN * N, w2s, nc, tw, s)) return rc;
       auto yin = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
       auto yout = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
-      if (int rc = colpass<false>(p, KID_YFWD, LdRows<T, N>{yin}, StRows<T, N>{yout}, Mzp, nc, N, tw, s)) return rc;
+      if (int rc = colpass<false>(p, KID_YFWD, LdRowsC<T, N, false>{yin}, StRowsC<T, N, true>{yout}, Mzp, nc, N, tw, s)) return rc;
       auto xin = io(W1, w1s, 0, My * Mzp, -1);
       auto xout = io(uk + c0 * cs, cs, 0, My * Mzp, kc);
-      if (int rc = colpass<false>(p, KID_XPASS, LdRows<T, N>{xin}, StCube<T, N>{xout, Mzp}, My * Mzp, nc, 1, tw, s)) return rc;
+      if (int rc = colpass<false>(p, KID_XPASS, LdRowsC<T, N, false>{xin}, StCube<T, N>{xout, Mzp}, My * Mzp, nc, 1, tw, s)) return rc;
     }
     return LD_OK;
   }
@@ -292,7 +292,7 @@ template <typename T, int N> struct Ops {
     // inverse x pass with the curl: 6 fields [u, w]
     LdCurl<T, N> lc{y, cs, kc, My, Mzp};
     auto xout = io(W1, w1s, 0, My * Mzp, -1);
-    if (int rc = colpass<true>(p, KID_XINV, lc, StRows<T, N>{xout}, My * Mzp, 6, 1, tw, s)) return rc;
+    if (int rc = colpass<true>(p, KID_XINV, lc, StRowsC<T, N, false>{xout}, My * Mzp, 6, 1, tw, s)) return rc;
     // inverse y pass
     auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
     auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
