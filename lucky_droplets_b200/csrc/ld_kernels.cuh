@@ -51,6 +51,10 @@ template <int N> struct Cfg {
   static constexpr int ZTHREADS = 256;
   static constexpr int ZROWS = ZTHREADS / NTZ;  // row units per CTA
   static constexpr int LOGEZ = ilog2(EZ);
+  // the dealiased cube of a plan of size N (ld_plan_create: kc = N / 3, rows padded to 8)
+  static constexpr int KC = N / 3;
+  static constexpr int MY = 2 * KC + 1;
+  static constexpr int MZP = (KC + 1 + 7) / 8 * 8;
   static constexpr int ZBUF = N + N / EZ;       // padded row buffer (bank-conflict free)
 };
 
@@ -97,7 +101,7 @@ template <typename T, int N> struct StRows {
 template <typename T, int N, bool MAP> struct LdRowsC {
   RowsIO<T> io;
   __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
-    const int r = MAP ? crow(n, N, io.kc) : n;
+    const int r = MAP ? crow(n, N, Cfg<N>::KC) : n;  // io.kc == Cfg<N>::KC for cube rows
     if (r < 0) return czero<cplx<T>>();
     cplx<T> v = io.p[io.at(f, o, r, col)];
     return cscale(v, io.scale);
@@ -110,7 +114,7 @@ template <typename T, int N, bool MAP> struct LdRowsC {
 template <typename T, int N, bool MAP> struct StRowsC {
   RowsIO<T> io;
   __device__ __forceinline__ void operator()(int f, int o, int n, int col, cplx<T> v) const {
-    const int r = MAP ? crow(n, N, io.kc) : n;
+    const int r = MAP ? crow(n, N, Cfg<N>::KC) : n;  // io.kc == Cfg<N>::KC for cube rows
     if (r < 0) return;
     io.p[io.at(f, o, r, col)] = v;
   }
@@ -138,7 +142,8 @@ template <typename T, int N> struct StCube {
 template <typename T, int N> struct LdCurl {
   const cplx<T>* u;
   long long cs;  // component stride (cube elements)
-  int kc, My, Mzp;
+  int kc_, My_, Mzp_;  // the plan's cube; equal to Cfg<N>::KC, MY, MZP, which the loader uses
+  static constexpr int kc = Cfg<N>::KC, My = Cfg<N>::MY, Mzp = Cfg<N>::MZP;
   __device__ __forceinline__ cplx<T> operator()(int f, int, int n, int col) const {
     const int r = crow(n, N, kc);
     if (r < 0) return czero<cplx<T>>();
@@ -333,7 +338,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
   const int col = blockIdx.x * TB + c;
   const bool ok = col < ncols;
   constexpr bool RK2 = MODE == UPD_RK2_1 || MODE == UPD_RK2_2;
-  const int Mx = 2 * A.kc + 1;
+  constexpr int Mx = Cfg<N>::MY;  // A.kc == Cfg<N>::KC, A.My == Cfg<N>::MY, A.Mzp == Cfg<N>::MZP
   cplx<T>* ybuf = sbuf + N * TB;  // (3, Mx, TB) staged rows of s1 (stage 1) or s2 (stage 2)
   const bool pre = RK2 && A.prefetch;
   if (pre) {
@@ -342,7 +347,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     const int col0 = blockIdx.x * TB;
     const int w = ncols - col0 < TB ? ncols - col0 : TB;  // a multiple of 8 (Mzp is)
     const int cpr = w / PER;
-    const long long rs = (long long)A.My * A.Mzp;
+    constexpr long long rs = (long long)Cfg<N>::MY * Cfg<N>::MZP;
     for (int q = threadIdx.x; q < 3 * Mx * (TB / PER); q += blockDim.x) {
       const int row = q / (TB / PER), k = q - row * (TB / PER);  // row = cc * Mx + r
       if (k >= cpr) continue;
@@ -367,11 +372,11 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     __syncthreads();
   }
   if (!ok) return;
-  const int iy = col / A.Mzp;
-  const int kzi = col - iy * A.Mzp;
-  const int kyi = cfreq(iy, A.kc);
+  const int iy = col / Cfg<N>::MZP;
+  const int kzi = col - iy * Cfg<N>::MZP;
+  const int kyi = cfreq(iy, Cfg<N>::KC);
   const T ky = T(kyi), kz = T(kzi);
-  const int kc = A.kc;
+  constexpr int kc = Cfg<N>::KC;
   unsigned flags = 0;
 #pragma unroll
   for (int m = 0; m < E; ++m) {
@@ -381,7 +386,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     const int kxi = n <= kc ? n : n - N;
     const T kx = T(kxi);
     const int k2 = kxi * kxi + kyi * kyi + kzi * kzi;
-    const long long idx = (long long)r * A.My * A.Mzp + col;
+    const long long idx = (long long)r * (Cfg<N>::MY * Cfg<N>::MZP) + col;
     const bool keep = (kzi <= kc) && (k2 <= kc * kc + kc);  // round(|k|) <= kc  (F:129)
     // forcing on shells kf_lo..kf_hi: factor[kint] * y  (F:253-264)
     T fac = T(0);

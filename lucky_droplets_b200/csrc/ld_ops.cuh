@@ -281,6 +281,8 @@ template <typename T, int N> struct Ops {
   static int rhs(ld_plan* p, C* s0, C* s1, C* s2, T* uout, const ld_flow_params* prm, double visc,
                  cudaStream_t s, C* s3 = nullptr) {
     const int kc = p->kc, My = p->My, Mzp = p->Mzp;
+    if (kc != Cfg<N>::KC || My != Cfg<N>::MY || Mzp != Cfg<N>::MZP)  // the kernels fix the cube by N
+      return ld_fail(LD_ERR_UNSUPPORTED, "plan cube (%d, %d, %d) differs from N = %d's", kc, My, Mzp, N);
     const C* tw = (const C*)p->tw;
     const long long NN = (long long)N * N;
     const long long cs = p->cube_elems();
