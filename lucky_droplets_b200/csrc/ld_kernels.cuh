@@ -699,11 +699,14 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
   const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
   cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
   const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR exactly
-  const long long fs = NR * Mzp;
+  (void)Mzp;
+  (void)kc;
+  constexpr int MZ = Cfg<N>::MZP, KIN = Cfg<N>::KC + 1;  // the plan's cube (checked at launch)
+  const long long fs = NR * MZ;
   const cplx<T>* in[6];
 #pragma unroll
-  for (int f = 0; f < 6; ++f) in[f] = W + f * fs + row * Mzp;
-  zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, Mzp, kc + 1, s, j, tw);
+  for (int f = 0; f < 6; ++f) in[f] = W + f * fs + row * MZ;
+  zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, j, tw);
 }
 
 // Pipelined fused z pass for one warp per row (N >= 256): persistent warps walk the rows with a
@@ -722,13 +725,16 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
   constexpr long long NR = (long long)N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const long long stage_elems = 12LL * Mzp;
+  (void)Mzp;
+  (void)kc;
+  constexpr int MZ = Cfg<N>::MZP, KIN = Cfg<N>::KC + 1;  // the plan's cube (checked at launch)
+  const long long stage_elems = 12LL * MZ;
   cplx<T>* base = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* stage = base + warp * stage_elems;
   cplx<T>* sb = base + nwarps * stage_elems + warp * Cfg<N>::ZBUF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(base + nwarps * (stage_elems + Cfg<N>::ZBUF)) + 2 * warp;
-  const long long fs = NR * Mzp;
-  const unsigned rowbytes = (unsigned)(Mzp * sizeof(cplx<T>));
+  const long long fs = NR * MZ;
+  const unsigned rowbytes = (unsigned)(MZ * sizeof(cplx<T>));
   const long long stride = (long long)gridDim.x * nwarps;
   long long row = (long long)blockIdx.x * nwarps + warp;
   if (lane == 0) {
@@ -742,7 +748,7 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
       fence_proxy_async();
       mbar_expect_tx(&bars[b], 6u * rowbytes);
 #pragma unroll
-      for (int f = 0; f < 6; ++f) bulk_g2s(stage + (6 * b + f) * (long long)Mzp, W + f * fs + r * Mzp, rowbytes, &bars[b]);
+      for (int f = 0; f < 6; ++f) bulk_g2s(stage + (6 * b + f) * (long long)MZ, W + f * fs + r * MZ, rowbytes, &bars[b]);
     }
   };
   unsigned ph[2] = {0u, 0u};
@@ -760,11 +766,11 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
     }
     ph[b] ^= 1u;
     pend[b] = false;
-    const cplx<T>* st = stage + 6 * b * (long long)Mzp;
+    const cplx<T>* st = stage + 6 * b * (long long)MZ;
     const cplx<T>* in[6];
 #pragma unroll
-    for (int f = 0; f < 6; ++f) in[f] = st + f * Mzp;
-    zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, Mzp, kc + 1, s, lane, tw);
+    for (int f = 0; f < 6; ++f) in[f] = st + f * MZ;
+    zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, lane, tw);
     __syncwarp();  // every lane is done with staging buffer b and the exchange buffer
   }
 }
