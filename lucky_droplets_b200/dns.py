@@ -187,11 +187,14 @@ class ForcedDNS:
         count gives, so a replay must start at the same step count modulo sort_every."""
         return StepGraph(self, nsteps)
 
-    def _step_one(self, stream, before_droplets=None, before_collide=None):
+    def _step_one(self, stream, before_droplets=None, before_collide=None, after_flow=None):
         """One time step on `stream`.  `before_droplets()` is called just before the first droplet
-        stage is enqueued, `before_collide()` after the state is final (update, epilogue and any
-        re-sorting enqueued) and before the collision search: the hooks of `step_host` that
-        overlap host copies with the flow transforms and the collision search."""
+        stage is enqueued, `after_flow()` once the flow state is final (last stage and epilogue
+        enqueued; the last droplet stage follows), `before_collide()` after the droplet state is
+        final (update and any re-sorting enqueued) and before the collision search: the hooks of
+        `step_host` that overlap host copies with the flow transforms, the last droplet stage and
+        the collision search.  The epilogue touches only the spectrum and the last droplet stage
+        only the droplets, so running the epilogue first changes no result."""
         L = _lib.lib()
         h = self.plan.handle
         st = stream_ptr(stream)
@@ -211,13 +214,19 @@ class ForcedDNS:
                 droplets_ready()
                 d.stage(1, self.u_phys, self.dt, stream)
             check(L.ld_rk2if_stage(h, 2, ptr(self.uk), ptr(self.aux), ptr(self.acc), up, prm, st))
+            if self.epilogue:
+                check(L.ld_step_epilogue_plane0(h, ptr(self.uk), st))
+            if after_flow is not None:
+                after_flow()
             if d is not None:
                 d.stage(2, self.u_phys, self.dt, stream)
         else:
             for s in (1, 2, 3, 4):
                 check(L.ld_rk4_stage(h, s, ptr(self.uk), ptr(self.aux), ptr(self.acc), None, prm, st))
-        if self.epilogue:
-            check(L.ld_step_epilogue_plane0(h, ptr(self.uk), st))
+            if self.epilogue:
+                check(L.ld_step_epilogue_plane0(h, ptr(self.uk), st))
+            if after_flow is not None:
+                after_flow()
         self.t += self.dt
         self.nstep += 1
         droplets_ready()
@@ -236,8 +245,10 @@ class ForcedDNS:
 
         The spectrum is needed by the first kernel, so its copy precedes the step; the droplet
         copies run on a side stream under the first stage's flow transforms (the droplets are
-        first read by the droplet stage), and the copies back run on a side stream under the
-        collision search of the last step, which reads the positions but writes no state."""
+        first read by the droplet stage).  The copies back run on a side stream: the spectrum's
+        as soon as the flow state is final, under the last droplet stage and the collision
+        search; the droplets' after their last update, under the collision search, which reads
+        the positions but writes no state."""
         torch = _torch()
         s = torch.cuda.current_stream() if stream is None else stream
         d = self.droplets if pos_host is not None else None
@@ -253,21 +264,27 @@ class ForcedDNS:
         def droplets_in():
             s.wait_stream(side[0])
 
-        def state_out():
+        def flow_out():
             side[1].wait_stream(s)
             with torch.cuda.stream(side[1]):
                 uk_host.copy_(self.uk, non_blocking=True)
-                if d is not None:
+
+        def droplets_out():
+            if d is not None:
+                side[1].wait_stream(s)
+                with torch.cuda.stream(side[1]):
                     pos_host.copy_(d.pos, non_blocking=True)
                     vel_host.copy_(d.vel, non_blocking=True)
 
         with torch.cuda.stream(s):
             for k in range(nsteps):
+                last = k == nsteps - 1
                 self._step_one(s, droplets_in if (k == 0 and d is not None) else None,
-                               state_out if k == nsteps - 1 else None)
+                               droplets_out if last else None, flow_out if last else None)
             if nsteps == 0:
                 droplets_in()
-                state_out()
+                flow_out()
+                droplets_out()
         s.wait_stream(side[1])
         s.synchronize()
         return uk_host, pos_host, vel_host
