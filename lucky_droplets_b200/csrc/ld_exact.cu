@@ -10,7 +10,8 @@
 // split across blocks so that even 1e4 points fill the GPU, and the per-chunk partial sums are
 // added in chunk order afterwards (deterministic).  Every thread of a warp walks the same
 // (kx, ky, kz) sequence, so the spectrum loads are warp-uniform (one broadcast transaction per
-// warp); the phases come from FP64 recurrences seeded by sincos once per row.
+// warp); the phases come from FP64 recurrences seeded by sincos once per row.  Along kz the
+// weight-2 terms accumulate unweighted in fused multiply-adds and are doubled once per row.
 #include "ld_internal.cuh"
 
 namespace {
@@ -43,21 +44,32 @@ k_exact_sum(const ld::cplx<T>* __restrict__ uk, long long cs, int N, int kc, int
       const int r2 = kx * kx + ky * ky;
       if (r2 <= lim) {
         const long long base = ((long long)ix * My + iy) * Mzp;
-        double ty[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-        double ezr = 1.0, ezi = 0.0;
-        for (int kz = 0; kz <= kc && r2 + kz * kz <= lim; ++kz) {
-          const double w = kz ? 2.0 : 1.0;
-          const double wr = w * ezr, wi = w * ezi;
+        // kz = 0 (weight 1) seeds the sum; the kz > 0 terms (weight 2) accumulate in fused
+        // multiply-adds and are doubled once at the end of the row
+        double t0[3][2], ty[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const ld::cplx<T> v = uk[c * cs + base];
+          t0[c][0] = (double)v.x;
+          t0[c][1] = (double)v.y;
+        }
+        double ezr = szr, ezi = szi;
+        for (int kz = 1; kz <= kc && r2 + kz * kz <= lim; ++kz) {
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             const ld::cplx<T> v = uk[c * cs + base + kz];
             const double vr = (double)v.x, vi = (double)v.y;
-            ty[c][0] += vr * wr - vi * wi;
-            ty[c][1] += vr * wi + vi * wr;
+            ty[c][0] = fma(vr, ezr, fma(-vi, ezi, ty[c][0]));
+            ty[c][1] = fma(vr, ezi, fma(vi, ezr, ty[c][1]));
           }
-          const double t = ezr * szr - ezi * szi;
-          ezi = ezr * szi + ezi * szr;
+          const double t = fma(ezr, szr, -ezi * szi);
+          ezi = fma(ezr, szi, ezi * szr);
           ezr = t;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          ty[c][0] = fma(2.0, ty[c][0], t0[c][0]);
+          ty[c][1] = fma(2.0, ty[c][1], t0[c][1]);
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -86,6 +98,14 @@ __global__ void k_exact_reduce(const double* __restrict__ part, int chunks, long
   }
 }
 
+// FP32 spectrum -> FP64 copy (exact), so that the sum converts nothing per mode.
+__global__ void k_spec_to_f64(const float2* __restrict__ in, double2* __restrict__ out, long long m) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m; e += (long long)gridDim.x * blockDim.x) {
+    const float2 v = in[e];
+    out[e] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
 }  // namespace
 
 extern "C" int ld_exact_sum(ld_plan* p, const void* uk, const double* pos, int64_t n, double* out, void* stream) {
@@ -96,8 +116,25 @@ extern "C" int ld_exact_sum(ld_plan* p, const void* uk, const double* pos, int64
   const int th = 128;
   // partial sums live in the plan's transform workspace (free between steps): points are taken
   // in batches that fit it
-  const long long cap = (long long)(p->work_bytes / sizeof(double));
+  long long cap = (long long)(p->work_bytes / sizeof(double));
   double* part = (double*)p->work;
+  // FP32 plans: an FP64 copy of the spectrum at the end of the workspace when it leaves room for
+  // the partial sums of one batch of points (the sum then converts nothing per mode)
+  const double2* uk64 = nullptr;
+  if (p->prec == LD_F32) {
+    const long long m = 3 * p->cube_elems();
+    const size_t copy_bytes = ((size_t)m * sizeof(double2) + 255) / 256 * 256;
+    const long long rest = (long long)((p->work_bytes - (copy_bytes < p->work_bytes ? copy_bytes : p->work_bytes)) /
+                                       sizeof(double));
+    if (copy_bytes < p->work_bytes && rest >= 3LL * p->My * (n < 4096 ? n : 4096)) {
+      double2* dst = (double2*)((char*)p->work + (p->work_bytes - copy_bytes) / 256 * 256);
+      long long gb = (m + 255) / 256;
+      if (gb > 148LL * 16) gb = 148LL * 16;
+      k_spec_to_f64<<<(unsigned)gb, 256, 0, s>>>((const float2*)uk, dst, m);
+      uk64 = dst;
+      cap = (long long)(((char*)dst - (char*)p->work) / sizeof(double));
+    }
+  }
   const double scale = 1.0 / ((double)p->N * p->N * p->N);
   for (long long b0 = 0; b0 < n; ) {
     long long nb = n - b0;
@@ -113,7 +150,10 @@ extern "C" int ld_exact_sum(ld_plan* p, const void* uk, const double* pos, int64
     const int per_chunk = (p->My + chunks - 1) / chunks;
     chunks = (p->My + per_chunk - 1) / per_chunk;
     const dim3 grid((unsigned)((nb + th - 1) / th), (unsigned)chunks);
-    if (p->prec == LD_F32)
+    if (uk64)
+      k_exact_sum<double><<<grid, th, 0, s>>>(uk64, p->cube_elems(), p->N, p->kc, p->My, p->Mzp, pos + 3 * b0, nb,
+                                              per_chunk, part);
+    else if (p->prec == LD_F32)
       k_exact_sum<float><<<grid, th, 0, s>>>((const float2*)uk, p->cube_elems(), p->N, p->kc, p->My, p->Mzp,
                                              pos + 3 * b0, nb, per_chunk, part);
     else
