@@ -398,17 +398,32 @@ __device__ __forceinline__ void col_visit(int i, int t, const double4* __restric
   const float4 mf = STAGED ? colbuf[t] : spf[i];
   const float mar = margin + 1e-6f * mf.w;
   unsigned c = 0;
+  // away from the z faces the three cells z-1, z, z+1 of a column are one contiguous sorted range
+  // with no periodic shift along z: 5 ranges (the own column from i + 1 through cell z + 1, then
+  // the four forward columns), visited in exactly the order of the 14 cells
+  const bool interior = cz >= 1 && cz <= nc - 2;
+  const int nseg = interior ? 5 : 14;
 #pragma unroll 1
-  for (int r = 0; r < 14; ++r) {
-    const int q = r < 2 ? 0 : 1 + (r - 2) / 3;
-    const int dz = r < 2 ? r : (r - 2) % 3 - 1;
-    const int zr = cz + dz;
-    const int zz = zr < 0 ? zr + nc : (zr >= nc ? zr - nc : zr);
-    const float sz = zr >= nc ? -Lf : (zr < 0 ? Lf : 0.f);
+  for (int r = 0; r < nseg; ++r) {
+    int q, g0, g1;
+    float sz;
+    if (interior) {
+      q = r;
+      sz = 0.f;
+      g0 = r == 0 ? i + 1 : cst[q * (nc + 1) + cz - 1];
+      g1 = cst[q * (nc + 1) + cz + 2];
+    } else {
+      q = r < 2 ? 0 : 1 + (r - 2) / 3;
+      const int dz = r < 2 ? r : (r - 2) % 3 - 1;
+      const int zr = cz + dz;
+      const int zz = zr < 0 ? zr + nc : (zr >= nc ? zr - nc : zr);
+      sz = zr >= nc ? -Lf : (zr < 0 ? Lf : 0.f);
+      g0 = r == 0 ? i + 1 : cst[q * (nc + 1) + zz];
+      g1 = cst[q * (nc + 1) + zz + 1];
+    }
     const float ax = mf.x + shx[q], ay = mf.y + shy[q], az = mf.z + sz;
-    const int g1 = cst[q * (nc + 1) + zz + 1];
     const int d = dl[q];
-    for (int g = r == 0 ? i + 1 : cst[q * (nc + 1) + zz]; g < g1; ++g) {
+    for (int g = g0; g < g1; ++g) {
       const float4 b = STAGED ? colbuf[g - d] : spf[g];
       const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
       const float rr = mf.w + b.w + mar;
