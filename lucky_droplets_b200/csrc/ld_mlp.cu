@@ -97,6 +97,8 @@ __device__ __forceinline__ float silu(float z) {
   const float h = 0.5f * z;
   return fmaf(h, tanh_fast(h), h);
 }
+// SiLU given h = z / 2 (the same arithmetic as silu(z) from there on).
+__device__ __forceinline__ float silu_half(float h) { return fmaf(h, tanh_fast(h), h); }
 __device__ __forceinline__ float dsilu(float z) {
   const float s = sigm(z);
   return s * (1.f + z * (1.f - s));
@@ -669,8 +671,11 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
     if (nrow < N3) v = *reinterpret_cast<const uint4*>(packed + P_W3T + nrow * KP2 + 8 * kc);
     *reinterpret_cast<uint4*>(sm + SM_W3 + blk_off(nrow, kc, N3P)) = v;
   }
+  // b1, b2 halved: the epilogues form h = z / 2 = fma(0.5, acc, b / 2), which is exactly
+  // 0.5 * (acc + b) (halving is exact), and SiLU(z) = h + h tanh(h); b3 as is
   for (int e = tid; e < 2 * H + N3P; e += FT_THREADS)
-    bias[e] = e < H ? params[OFF_B1 + e] : (e < 2 * H ? params[OFF_B2 + e - H] : (e - 2 * H < N3 ? params[OFF_B3 + e - 2 * H] : 0.f));
+    bias[e] = e < H ? 0.5f * params[OFF_B1 + e]
+                    : (e < 2 * H ? 0.5f * params[OFF_B2 + e - H] : (e - 2 * H < N3 ? params[OFF_B3 + e - 2 * H] : 0.f));
   if (tid == 0) {
     mbar_init(&bar_x[0], 1);
     mbar_init(&bar_x[1], 1);
@@ -745,8 +750,8 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const float4 b4 = b4p[j];
-            w[2 * j] = pack2(silu(v[4 * j] + b4.x), silu(v[4 * j + 1] + b4.y));
-            w[2 * j + 1] = pack2(silu(v[4 * j + 2] + b4.z), silu(v[4 * j + 3] + b4.w));
+            w[2 * j] = pack2(silu_half(fmaf(0.5f, v[4 * j], b4.x)), silu_half(fmaf(0.5f, v[4 * j + 1], b4.y)));
+            w[2 * j + 1] = pack2(silu_half(fmaf(0.5f, v[4 * j + 2], b4.z)), silu_half(fmaf(0.5f, v[4 * j + 3], b4.w)));
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)
