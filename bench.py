@@ -599,7 +599,7 @@ def run_ours(a):
                       "N": a.N, "n_droplets": a.nd, "interp": a.interp, "precision": a.precision,
                       "run": f"steps {pre}..{dns.nstep} of a {a.run_steps}-step run (timed: the last {a.steps})",
                       "parallelism": f"replicas x{world}", "l2": "working set > 1 GB per step (> L2); no flush",
-                      "launch": (f"timed steps replayed from a CUDA graph of {a.graph_steps} steps (both arms)"
+                      "launch": (f"timed steps replayed from a CUDA graph of {a.graph_steps} steps (also for the FP64 comparators)"
                                  if a.graph_steps > 0 and a.steps % a.graph_steps == 0 else "kernels launched one by one")},
            "droplet_steps_per_s": value * a.nd,
            "step_algo_gbs": step_bytes / (ms / a.steps * 1e-3) / 1e9,
