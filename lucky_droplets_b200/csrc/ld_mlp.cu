@@ -471,13 +471,11 @@ __device__ __forceinline__ void tile_forward(const bf16* X, bf16* h1, bf16* h2, 
   y[3] = a3[0][3] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
 }
 
-// ---- fused-feature inference, in two kernels --------------------------------------------------
-// k_mlp_features: warp per 8 droplets, no weights in shared memory: canonical-frame stencil
-// gather into shared memory (2 taps per lane per droplet), then lane 3r + c takes component c
-// of droplet r in registers (polynomial transform, partial sums, 64 features); the feature rows
-// (bf16, K1 per droplet) go to global memory in the tensor-core tile layout (tiles of TM rows,
-// 8x8 core matrices, see blk_off) and the per-droplet aux (tricubic xyz in the grid frame,
-// scale, frame code) as 8 floats.
+// ---- inference, in two kernels ------------------------------------------------------------------
+// k_mlp_features writes each droplet's feature row (bf16, K1 columns) to global memory in the
+// tensor-core tile layout (tiles of TM rows, 8x8 core matrices, see blk_off) and its aux
+// (tricubic xyz in the grid frame, scale, frame code) as 8 floats; k_mlp_forward_tc runs the
+// three layers on the tensor cores and writes the velocities.
 // Tensor-core tile layout of a K-major bf16 operand with `rows` rows: 8x8 core matrices (8 rows of
 // 16 bytes, 128 contiguous bytes), K-chunk major: byte offset of (row, 8-element K chunk kc).
 __host__ __device__ constexpr int blk_off(int row, int kc, int rows) {

@@ -106,6 +106,39 @@ def test_training_targets_are_exact(torch):
     assert np.abs(ue.reshape(3, -1)[:, idx].T - exact).max() / np.abs(exact).max() < 1e-12
 
 
+def test_inference_streams_many_tiles_per_cta(torch):
+    """At 94,797 droplets on a 128^3 plan (one batch: the workspace holds about 140k rows) every
+    CTA of the tensor-core forward takes 5-6 tiles of 128 droplets, the last one ragged, so the
+    feature chunks stream through the shared-memory ring with refills and both groups of warps
+    alternate on it.  A row's result does not depend on its tile or CTA: the whole batch must
+    equal, bit for bit, the same droplets inferred in batches of 2,000 (at most one tile per CTA,
+    no refill), and a subsample must match the oracle."""
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    N = 128
+    prm = C.ConfigParams(N=N, nu=0.01, dt=1e-3)
+    grid = C.ConfigGrid(N)
+    uk, u = C.init_flow(grid, prm, seed=8)
+    plan = Plan(N, "f32")
+    p = M.init_params(5)
+    fs = np.random.default_rng(3).uniform(0.5, 3.0, 64).astype(np.float32)
+    os = 0.01
+    li = G.LearnedInterp(plan, params=G.flat_from_mats(**p, fs=fs, os=os))
+    cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
+    u4 = li.interleaved(cube)
+    n = 148 * 128 * 5 + 77
+    pos = np.random.default_rng(4).uniform(-1, 7.5, (n, 3))
+    pos_d = torch.as_tensor(pos).cuda()
+    whole = li.infer(u4, pos_d).cpu().numpy()
+    parts = np.concatenate([li.infer(u4, pos_d[b:b + 2000]).cpu().numpy() for b in range(0, n, 2000)])
+    assert plan.status() == 0  # no bounded wait ran out
+    assert np.array_equal(whole, parts)
+    sub = slice(0, n, 7)
+    ref, tric = _oracle_infer(u, pos[sub], p, fs, os)
+    assert rel(whole[sub] - tric, ref - tric) < 5e-3
+    assert rel(whole[sub], ref) < 1e-4
+
+
 def test_training_beats_tricubic(torch):
     from lucky_droplets_b200.spectral import Plan
     from lucky_droplets_b200 import mlp as G
