@@ -40,7 +40,7 @@ template <typename T, int N> struct Ops {
   template <bool INV, class Ld, class St>
   static int colpass(ld_plan* p, int kid, Ld ld, St st, int ncols, int nf, int nouter, const C* tw, cudaStream_t s) {
     ProfScope ps(p, kid, s);
-    auto k = k_colfft<T, N, INV, Ld, St>;
+    auto k = colfft_kernel<T, N, INV, Ld, St>();
     if (int rc = set_smem(k, COL_SMEM)) return rc;
     dim3 grid((unsigned)(cdiv(ncols, TB) * nf), (unsigned)nouter);
     k<<<grid, Cfg<N>::COL_THREADS, COL_SMEM, s>>>(ld, st, ncols, nf, tw);
