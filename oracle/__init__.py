@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY.  Nothing in the product package imports this directory; only
 ``tests/``, ``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference`` legs of
-``bench.py`` use it, and only as the checker or as the timed CPU baseline.
+``bench.py`` use it, and only to check the GPU results or as the timed CPU baseline.
 
 Contents (FP64, NumPy/SciPy, numba for the droplet loops):
   * ``reference_np`` - a restatement of the reference's own single-rank algorithm
