@@ -15,6 +15,32 @@ def test_defaults():
     assert a.run_steps == 500 and a.judge_every == 500
 
 
+def test_reference_arm_line(capsys, monkeypatch):
+    """The reference arm (CPU restatement, no GPU) at 32^3 with 2000 droplets prints one JSON line
+    with the contract's keys: impl, metric, value, cpu_baseline (kind, cores, sample) and a
+    host-only e2e."""
+    import json
+    monkeypatch.delenv("RANK", raising=False)
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    bench.main(["--impl", "reference", "--N", "32", "--nd", "2000", "--steps", "2", "--warmup", "3"])
+    lines = [l for l in capsys.readouterr().out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "steps/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert d["config"]["N"] == 32 and d["config"]["n_droplets"] == 2000 and d["config"]["interp"] == "tricubic"
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_print_nothing(capsys, monkeypatch):
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    bench.main(["--impl", "reference", "--N", "32", "--nd", "100", "--steps", "1"])
+    assert capsys.readouterr().out == ""
+
+
 def _worker(rank, world, port, q):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
