@@ -78,7 +78,10 @@ LD_API const char* ld_last_error(void);
 
 /* ---- plans: grid and spectral operators of F:49-141 ---------------------------------- */
 /* Builds the twiddle tables (FP64, rounded once to the plan precision), operator tables and
- * transform workspace for an N^3 grid, N a power of two in [16, 512]. */
+ * transform workspace for an N^3 grid: N a power of two in [16, 512], or one of the mixed-radix
+ * sizes 96, 192, 360, 384 (radix-3 and radix-5 stages; the reference takes any N its slabs
+ * divide, F:27-29, F:52-57).  The learned interpolation (ld_mlp_infer, ld_mlp_samples) needs a
+ * power of two. */
 LD_API int ld_plan_create(ld_plan** plan, int n, int precision);
 LD_API int ld_plan_destroy(ld_plan* plan);
 /* dims[0..7] = N, kc, Mx, My, Mz, Mzp, Nf, precision; work_bytes = transform workspace. */
@@ -138,6 +141,12 @@ LD_API int ld_velocity_rhs(ld_plan* plan, const void* uk, void* ku, void* u_out,
  * interleaved (N, N, N, 4) as (u, v, w, 0) per grid point. */
 LD_API int ld_rk2if_stage(ld_plan* plan, int stage, void* uk, void* ustar, void* acc, void* u_out,
                    const ld_flow_params* prm, void* stream);
+/* Builds on `stream` the tables a time step with these parameters reads (the integrating factor
+ * exp(-nu k^2 dt) of ld_rk2if_stage; no counterpart in the reference, whose loop recomputes its
+ * operators each step, F:561-562).  ld_rk2if_stage builds it itself when nu dt changes, but a
+ * stage captured into a CUDA graph records the build into the graph and leaves the table
+ * unmarked; call this before capturing so that captured steps find it built. */
+LD_API int ld_plan_prepare(ld_plan* plan, const ld_flow_params* prm, void* stream);
 /* Classical RK4 with explicit viscosity, one stage per call (F:335-362):
  *   stage s evaluates ku_s = RHS(y_s) with y_1 = uk and
  *   s=1: acc = uk + h/6 ku1, y = uk + h/2 ku1;  s=2: acc += h/3 ku2, y = uk + h/2 ku2;
@@ -155,6 +164,14 @@ LD_API int ld_rk4_stage(ld_plan* plan, int stage, void* uk, void* y, void* acc, 
  * ld_plan_set_tuning applies a choice found on another plan of the same N and precision. */
 LD_API int ld_plan_autotune(ld_plan* plan, double* ms, int32_t* choice, void* stream);
 LD_API int ld_plan_set_tuning(ld_plan* plan, const int32_t* choice);
+/* Bounded device waits (no counterpart in the reference, whose failures end in comm.Abort,
+ * F:618-620): the waits of the plan's pipelined kernels (the fused z pass at N >= 256, the
+ * tensor-core MLP forward) give up after `limit` polls (0: the default, 2^24), raise
+ * LD_STATUS_WAIT_TIMEOUT, let the copies and MMAs they issued complete, free their tensor memory
+ * and return; the launch and the context stay usable.  stall != 0 tests that path: the first wait
+ * of every warp (z pass) or warp group (MLP forward) is on a barrier that nothing completes, so
+ * it runs out after `limit` polls while the first copy is in flight.  stall = 0 for production. */
+LD_API int ld_plan_set_wait_limit(ld_plan* plan, uint32_t limit, int stall);
 /* While vk is set (a cube-layout 3-vector), every RHS evaluation of the plan (ld_velocity_rhs,
  * ld_rk4_stage, ld_rk2if_stage) also writes the spectrum of the small-droplet (slow-manifold)
  * velocity of its stage input, v = u - tps Du/Dt - tps g z with Du/Dt = -grad p + nu lap u

@@ -82,6 +82,8 @@ SIGNATURES = {
     "ld_slow_manifold": (_c_i, [_c_p, _c_p, _c_d, _c_d]),
     "ld_plan_autotune": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_plan_set_tuning": (_c_i, [_c_p, _c_p]),
+    "ld_plan_set_wait_limit": (_c_i, [_c_p, ctypes.c_uint32, _c_i]),
+    "ld_plan_prepare": (_c_i, [_c_p, ctypes.POINTER(FlowParams), _c_p]),
     "ld_shell_cross": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_divergence_spec": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_droplet_predict": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),

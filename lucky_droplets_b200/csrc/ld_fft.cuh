@@ -14,6 +14,14 @@
 // Twiddles for stages >= 1 come from a table tw[p] = exp(-2 pi i p / N), p < N, computed on the
 // host in FP64 (and rounded once to the element type).  The radix-R butterflies use the exact
 // constants cos(2 pi m / 16), sin(2 pi m / 16).
+//
+// Lengths that are not powers of two (N = 2^a 3^b 5^c, E a power of two dividing N) take the
+// mixed-radix Stockham pipeline below (fft_run_mr): stage 0 is radix E in registers as above;
+// the remaining factor N / E is split into radix 8/4/2 stages, then radix 5, then radix 3 stages,
+// each stage's N / R butterflies dealt round-robin to the NT threads (a thread does up to
+// ceil(N / R / NT) of them; the rest idle), every stage reading and writing the exchange buffer;
+// the last stage writes natural order and each thread reads back its own positions, so the
+// register contract is the same.
 #pragma once
 #include "ld_common.cuh"
 
@@ -143,6 +151,119 @@ template <typename T, int E, bool PAD> __device__ __forceinline__ int sidx(int p
   else return p + (p >> ilog2(E));
 }
 
+// In-place length-3 and length-5 DFTs (forward sign exp(-2 pi i jk / R); INV conjugates).  The
+// constants are cos and sin of 2 pi / 3, 2 pi / 5 and 4 pi / 5.
+template <typename T, bool INV> __device__ __forceinline__ void dft3(cplx<T>* x) {
+  constexpr T s3 = T(0.86602540378443864676);  // sin(2 pi / 3)
+  const cplx<T> t1 = cadd(x[1], x[2]);
+  const cplx<T> d = csub(x[1], x[2]);
+  const cplx<T> m = cmk(x[0].x - T(0.5) * t1.x, x[0].y - T(0.5) * t1.y);
+  // -i s3 d (forward) / +i s3 d (inverse)
+  const cplx<T> r = INV ? cmk(-s3 * d.y, s3 * d.x) : cmk(s3 * d.y, -s3 * d.x);
+  x[0] = cadd(x[0], t1);
+  x[1] = cadd(m, r);
+  x[2] = csub(m, r);
+}
+
+template <typename T, bool INV> __device__ __forceinline__ void dft5(cplx<T>* x) {
+  constexpr T c1 = T(0.30901699437494742410);   // cos(2 pi / 5)
+  constexpr T c2 = T(-0.80901699437494742410);  // cos(4 pi / 5)
+  constexpr T s1 = T(0.95105651629515357212);   // sin(2 pi / 5)
+  constexpr T s2 = T(0.58778525229247312917);   // sin(4 pi / 5)
+  const cplx<T> a1 = cadd(x[1], x[4]), a2 = cadd(x[2], x[3]);
+  const cplx<T> b1 = csub(x[1], x[4]), b2 = csub(x[2], x[3]);
+  const cplx<T> t1 = cmk(x[0].x + c1 * a1.x + c2 * a2.x, x[0].y + c1 * a1.y + c2 * a2.y);
+  const cplx<T> t2 = cmk(x[0].x + c2 * a1.x + c1 * a2.x, x[0].y + c2 * a1.y + c1 * a2.y);
+  const cplx<T> u1 = cmk(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);
+  const cplx<T> u2 = cmk(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);
+  // forward: X1 = t1 - i u1, X4 = t1 + i u1, X2 = t2 - i u2, X3 = t2 + i u2
+  const cplx<T> iu1 = INV ? cmk(-u1.y, u1.x) : cmk(u1.y, -u1.x);
+  const cplx<T> iu2 = INV ? cmk(-u2.y, u2.x) : cmk(u2.y, -u2.x);
+  x[0] = cadd(x[0], cadd(a1, a2));
+  x[1] = cadd(t1, iu1);
+  x[4] = csub(t1, iu1);
+  x[2] = cadd(t2, iu2);
+  x[3] = csub(t2, iu2);
+}
+
+// Any radix of the mixed-radix pipeline: 2, 4, 8, 16 (bit-reversed passes), 3 or 5.
+template <typename T, int R, bool INV> __device__ __forceinline__ void dft_any(cplx<T>* x) {
+  if constexpr (R == 3) dft3<T, INV>(x);
+  else if constexpr (R == 5) dft5<T, INV>(x);
+  else dft<T, R, INV>(x);
+}
+
+__host__ __device__ constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+// radix of the next stage for a remaining factor m: 8, 4, 2 first, then 5, then 3
+__host__ __device__ constexpr int mr_pick(int m) {
+  return m % 8 == 0 ? 8 : (m % 4 == 0 ? 4 : (m % 2 == 0 ? 2 : (m % 5 == 0 ? 5 : (m % 3 == 0 ? 3 : m))));
+}
+// remaining factor before stage s (s >= 1) of a length-N pipeline whose stage 0 is radix E
+__host__ __device__ constexpr int mr_rest(int N, int E, int s) {
+  return s <= 1 ? N / E : mr_rest(N, E, s - 1) / mr_pick(mr_rest(N, E, s - 1));
+}
+__host__ __device__ constexpr int mr_nstages(int m) { return m <= 1 ? 0 : 1 + mr_nstages(m / mr_pick(m)); }
+// m is a product of 2s, 3s and 5s
+__host__ __device__ constexpr bool mr_ok(int m) {
+  return m == 1 || (m > 1 && ((m % 2 == 0 && mr_ok(m / 2)) || (m % 3 == 0 && mr_ok(m / 3)) || (m % 5 == 0 && mr_ok(m / 5))));
+}
+
+template <int N, int E> struct MrShape {
+  static_assert(is_pow2(E) && E >= 2 && E <= 16 && N % E == 0, "stage 0: a power-of-two radix dividing N");
+  static_assert(mr_ok(N / E), "N / E must factor into 2, 3 and 5");
+  static constexpr int NT = N / E;
+  static constexpr int S = 1 + mr_nstages(N / E);
+  static __host__ __device__ constexpr int radix(int s) { return s == 0 ? E : mr_pick(mr_rest(N, E, s)); }
+  static __host__ __device__ constexpr int ns(int s) { return N / mr_rest(N, E, s); }  // product of earlier radices
+};
+
+// Stage s >= 1 of the mixed-radix pipeline.
+template <typename T, int N, int E, bool INV, bool PAD, int s, class Sync>
+__device__ __forceinline__ void fft_stage_mr(cplx<T>* a, cplx<T>* sbuf, int sstride, int j,
+                                             const cplx<T>* __restrict__ tw, Sync sync) {
+  using Sh = MrShape<N, E>;
+  constexpr int NT = Sh::NT;
+  constexpr int R = Sh::radix(s);
+  constexpr int Ns = Sh::ns(s);
+  constexpr int NB = N / R;                  // butterflies of this stage
+  constexpr int Q = (NB + NT - 1) / NT;      // butterflies per thread
+  constexpr bool FULL = Q * NT == NB;
+  constexpr bool LAST = s == Sh::S - 1;
+  cplx<T> x[Q * R];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int b = j + NT * q;
+    if (FULL || b < NB) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, E, PAD>(b + r * NB) * sstride];
+    }
+  }
+  sync();
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int b = j + NT * q;
+    if (FULL || b < NB) {
+      const int k = b % Ns;
+#pragma unroll
+      for (int r = 1; r < R; ++r) x[q * R + r] = cmul(x[q * R + r], twid<T, INV>(tw, r * k * (N / (Ns * R))));
+      dft_any<T, R, INV>(x + q * R);
+      // Stockham output position (b / Ns) Ns R + k + r Ns; in the last stage b < Ns, which is
+      // natural order b + r NB
+      const int base = LAST ? b : (b / Ns) * Ns * R + k;
+      constexpr int step = LAST ? NB : Ns;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sbuf[sidx<T, E, PAD>(base + r * step) * sstride] = x[q * R + r];
+    }
+  }
+  sync();
+  if constexpr (!LAST) {
+    fft_stage_mr<T, N, E, INV, PAD, s + 1>(a, sbuf, sstride, j, tw, sync);
+  } else {
+#pragma unroll
+    for (int m = 0; m < E; ++m) a[m] = sbuf[sidx<T, E, PAD>(j + NT * m) * sstride];
+  }
+}
+
 // Stage s >= 1 of the Stockham pipeline (compile-time recursion over the stages).
 template <typename T, int N, int E, bool INV, bool PAD, int s, class Sync>
 __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride, int j,
@@ -188,13 +309,21 @@ __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride
 template <typename T, int N, int E, bool INV, bool PAD, class Sync>
 __device__ __forceinline__ void fft_run(cplx<T>* a, cplx<T>* sbuf, int sstride, int j,
                                         const cplx<T>* __restrict__ tw, Sync sync) {
-  using Sh = FftShape<N, E>;
   dft<T, E, INV>(a);  // stage 0: radix E, Ns = 1, no twiddles
-  if constexpr (Sh::S > 1) {
+  if constexpr (is_pow2(N)) {
+    using Sh = FftShape<N, E>;
+    if constexpr (Sh::S > 1) {
+#pragma unroll
+      for (int r = 0; r < E; ++r) sbuf[sidx<T, E, PAD>(j * E + r) * sstride] = a[r];
+      sync();
+      fft_stage<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
+    }
+  } else {
+    static_assert(MrShape<N, E>::S > 1, "mixed-radix lengths have later stages");
 #pragma unroll
     for (int r = 0; r < E; ++r) sbuf[sidx<T, E, PAD>(j * E + r) * sstride] = a[r];
     sync();
-    fft_stage<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
+    fft_stage_mr<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
   }
 }
 

@@ -1,0 +1,3 @@
+// Kernel instance: precision float, N = 360.
+#include "ld_ops.cuh"
+LD_DEFINE_TABLE(f32, float, 360)

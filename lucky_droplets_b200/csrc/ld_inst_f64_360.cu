@@ -1,0 +1,3 @@
+// Kernel instance: precision double, N = 360.
+#include "ld_ops.cuh"
+LD_DEFINE_TABLE(f64, double, 360)

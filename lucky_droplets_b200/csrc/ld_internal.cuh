@@ -60,6 +60,8 @@ struct ld_plan {
   int tune_y[2] = {-1, -1};  // [inverse, forward]
   void* sm_vk = nullptr;          // slow-manifold velocity output of every RHS (none when null)
   double sm_tps = 0.0, sm_g = 0.0;
+  unsigned wait_limit = 1u << 24; // polls before a bounded device wait gives up (ld_plan_set_wait_limit)
+  int wait_stall = 0;             // test of the time-out path: first waits on a barrier nothing completes
   bool prof = false;              // record per-launch events
   std::vector<ProfRec> recs;      // recorded launches
   std::vector<cudaEvent_t> pool;  // reusable events
@@ -98,11 +100,18 @@ struct OpsTable {
   // times every launch variant of the y passes (ms[2][4]: one-shot, pipelined with 1..3 CTAs/SM)
   // and keeps the fastest in the plan
   int (*autotune)(ld_plan*, cudaStream_t, double* ms);
+  // builds the tables a time step of these flow parameters reads (integrating factor)
+  int (*prepare)(ld_plan*, const ld_flow_params*, cudaStream_t);
 };
 
+// Grid sizes with kernel instances: powers of two 16..512, and the mixed-radix sizes
+// 96 = 2^5 3, 192 = 2^6 3, 360 = 2^3 3^2 5 and 384 = 2^7 3 (the grids between 256 and 512 on
+// which the FP64 tricubic step is compared at equal interpolation error).
 #define LD_FOR_EACH_INSTANCE(X) \
   X(f32, 16) X(f32, 32) X(f32, 64) X(f32, 128) X(f32, 256) X(f32, 512) \
-  X(f64, 16) X(f64, 32) X(f64, 64) X(f64, 128) X(f64, 256) X(f64, 512)
+  X(f64, 16) X(f64, 32) X(f64, 64) X(f64, 128) X(f64, 256) X(f64, 512) \
+  X(f32, 96) X(f32, 192) X(f32, 360) X(f32, 384) \
+  X(f64, 96) X(f64, 192) X(f64, 360) X(f64, 384)
 #define LD_DECL_TABLE(P, N) const OpsTable* ops_table_##P##_##N();
 LD_FOR_EACH_INSTANCE(LD_DECL_TABLE)
 #undef LD_DECL_TABLE

@@ -39,17 +39,24 @@ template <typename T> __device__ __forceinline__ vec4<T> mk4(T a, T b, T c, T d)
   vec4<T> v; v.x = a; v.y = b; v.z = c; v.w = d; return v;
 }
 
+// Launch shapes by N.  Powers of two: as tuned.  Mixed-radix N = 2^a 3^b 5^c (a >= 3): eight
+// elements per thread in both kinds of pass (stage 0 radix 8), a CTA of 8 columns (64-byte FP32 /
+// 128-byte FP64 row segments; N/8 x 8 threads leave the FP64 update pass, which holds three
+// transformed columns, enough registers), and as many z row units per CTA as fit 256 threads (a
+// power of two, so that N^2 rows split evenly); their rows may span warps, so they exchange with
+// block-wide barriers.
 template <int N> struct Cfg {
+  static constexpr bool P2 = is_pow2(N);
   // column passes: E elements per thread, TB columns per CTA
-  static constexpr int EC = (N == 32 || N == 64) ? 8 : 16;
+  static constexpr int EC = P2 ? ((N == 32 || N == 64) ? 8 : 16) : 8;
   static constexpr int NTC = N / EC;
-  static constexpr int TB = N == 16 ? 64 : (N == 32 ? 32 : 16);
+  static constexpr int TB = P2 ? (N == 16 ? 64 : (N == 32 ? 32 : 16)) : 8;
   static constexpr int COL_THREADS = TB * NTC;
-  // z passes: E elements per thread, NTZ threads per row (a row never spans two warps)
-  static constexpr int EZ = N >= 512 ? 16 : 8;
+  // z passes: E elements per thread, NTZ threads per row
+  static constexpr int EZ = P2 ? (N >= 512 ? 16 : 8) : 8;
   static constexpr int NTZ = N / EZ;
-  static constexpr int ZTHREADS = 256;
-  static constexpr int ZROWS = ZTHREADS / NTZ;  // row units per CTA
+  static constexpr int ZROWS = P2 ? 256 / NTZ : (256 / NTZ >= 16 ? 16 : (256 / NTZ >= 8 ? 8 : (256 / NTZ >= 4 ? 4 : (256 / NTZ >= 2 ? 2 : 1))));
+  static constexpr int ZTHREADS = ZROWS * NTZ;  // row units per CTA x threads per row
   static constexpr int LOGEZ = ilog2(EZ);
   // the dealiased cube of a plan of size N (ld_plan_create: kc = N / 3, rows padded to 8)
   static constexpr int KC = N / 3;
@@ -532,7 +539,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
 // Exchange barrier of the z passes: warp-level when a row unit owns a whole warp (N >= 256),
 // block-wide when several row units share a warp (the warp-level form gave wrong results for
 // N <= 32 in the fused pass; the block-wide form is verified at every size).
-template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ >= 32), SyncWarp, SyncBlock>::type;
+template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ == 32), SyncWarp, SyncBlock>::type;
 // Row-buffer slot of element i: the same map as the FFT exchange of the row (sidx with PAD).
 template <typename T, int N> struct ZIdx {
   static __device__ __forceinline__ int p(int i) { return sidx<T, Cfg<N>::EZ, true>(i); }
@@ -597,7 +604,7 @@ __device__ __forceinline__ void zstore_pair(const cplx<T>* a, cplx<T>* sb, cplx<
       cplx<T> ra = czero<cplx<T>>(), rb = czero<cplx<T>>();
       if (k < Kval) {
         const cplx<T> y = a[m];
-        const cplx<T> z = sb[ZIdx<T, N>::p((N - k) & (N - 1))];
+        const cplx<T> z = sb[ZIdx<T, N>::p(k == 0 ? 0 : N - k)];
         ra = cmk(T(0.5) * (y.x + z.x), T(0.5) * (y.y - z.y));
         rb = cmk(T(0.5) * (y.y + z.y), T(-0.5) * (y.x - z.x));
       }
@@ -745,15 +752,19 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
 // Pipelined fused z pass for one warp per row (N >= 256): persistent warps walk the rows with a
 // stride; lane 0 of each warp prefetches the next row's six field rows into a double-buffered
 // shared staging area with bulk asynchronous copies (the TMA engine), completed on per-buffer
-// mbarriers, while the warp transforms the current row.  Waits are bounded: on time-out the
-// warp raises LD_STATUS_WAIT_TIMEOUT, drains its copies in flight (again bounded) and returns.
-// Shared memory per warp: 2 x 6 x Mzp staging + ZBUF exchange elements, then 2 mbarriers.
+// mbarriers, while the warp transforms the current row.  Waits are bounded: a wait for a row
+// gives up after wait_limit polls (the plan's setting); the warp then raises
+// LD_STATUS_WAIT_TIMEOUT, drains its copies in flight (bounded by kWaitLimit) and returns.  With
+// `stall` set (a test of that path) each warp first waits on a third mbarrier that nothing
+// completes, so the wait runs out while the warp's first copy is in flight.
+// Shared memory per warp: 2 x 6 x Mzp staging + ZBUF exchange elements, then 3 mbarriers.
 constexpr unsigned kWaitLimit = 1u << 24;
 
 template <typename T, int N>
 __global__ void __launch_bounds__(256)
 k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
-               int kc, T s, const cplx<T>* __restrict__ tw, unsigned* status) {
+               int kc, T s, const cplx<T>* __restrict__ tw, unsigned* status, unsigned wait_limit,
+               int stall) {
   static_assert(Cfg<N>::NTZ == 32, "one warp per row");
   constexpr long long NR = (long long)N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -765,7 +776,7 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
   cplx<T>* base = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* stage = base + warp * stage_elems;
   cplx<T>* sb = base + nwarps * stage_elems + warp * Cfg<N>::ZBUF;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(base + nwarps * (stage_elems + Cfg<N>::ZBUF)) + 2 * warp;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + nwarps * (stage_elems + Cfg<N>::ZBUF)) + 3 * warp;
   const long long fs = NR * MZ;
   const unsigned rowbytes = (unsigned)(MZ * sizeof(cplx<T>));
   const long long stride = (long long)gridDim.x * nwarps;
@@ -773,6 +784,7 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
   if (lane == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
     mbar_init_fence();
   }
   __syncwarp();
@@ -787,11 +799,16 @@ k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __rest
   unsigned ph[2] = {0u, 0u};
   bool pend[2] = {false, false};
   if (row < NR) { issue(row, 0); pend[0] = true; }
+  if (stall && row < NR && !mbar_wait_bounded(&bars[2], 0u, wait_limit)) {
+    if (lane == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
+    mbar_wait_bounded(&bars[0], ph[0], kWaitLimit);  // the first row's copy is in flight
+    return;
+  }
   int b = 0;
   for (; row < NR; row += stride, b ^= 1) {
     const long long next = row + stride;
     if (next < NR) { issue(next, b ^ 1); pend[b ^ 1] = true; }
-    if (!mbar_wait_bounded(&bars[b], ph[b], kWaitLimit)) {
+    if (!mbar_wait_bounded(&bars[b], ph[b], wait_limit)) {
       if (lane == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
       for (int q = 0; q < 2; ++q)
         if (pend[q]) mbar_wait_bounded(&bars[q], ph[q], kWaitLimit);
@@ -1072,6 +1089,12 @@ template <typename T> struct AxisW<T, LD_INTERP_COSINE> {
   }
 };
 
+// i in [-N, 2N) -> i mod N (stencil offsets around a cell index in [0, N); any N)
+__device__ __forceinline__ int wrap_index(int i, int N) {
+  i = i < 0 ? i + N : i;
+  return i >= N ? i - N : i;
+}
+
 template <typename T, int METHOD>
 __device__ __forceinline__ void gather_point(const T* __restrict__ f, int ncomp, long long fstride, int N,
                                              double L, double px, double py, double pz, T* out) {
@@ -1084,14 +1107,14 @@ __device__ __forceinline__ void gather_point(const T* __restrict__ f, int ncomp,
   A::get(pz, N, L, iz, wz);
   int jz[W];
 #pragma unroll
-  for (int c = 0; c < W; ++c) jz[c] = (iz + LO + c + N) & (N - 1);
+  for (int c = 0; c < W; ++c) jz[c] = wrap_index(iz + LO + c, N);
   for (int c = 0; c < ncomp; ++c) out[c] = T(0);
 #pragma unroll
   for (int a = 0; a < W; ++a) {
-    const int jx = (ix + LO + a + N) & (N - 1);
+    const int jx = wrap_index(ix + LO + a, N);
 #pragma unroll
     for (int b = 0; b < W; ++b) {
-      const int jy = (iy + LO + b + N) & (N - 1);
+      const int jy = wrap_index(iy + LO + b, N);
       const long long base = ((long long)jx * N + jy) * N;
       const T wab = wx[a] * wy[b];
       for (int c = 0; c < ncomp; ++c) {
@@ -1128,14 +1151,14 @@ __device__ __forceinline__ void gather_point4(const vec4<T>* __restrict__ f, int
   A::get(pz, N, L, iz, wz);
   int jz[W];
 #pragma unroll
-  for (int c = 0; c < W; ++c) jz[c] = (iz + LO + c + N) & (N - 1);
+  for (int c = 0; c < W; ++c) jz[c] = wrap_index(iz + LO + c, N);
   T o0 = 0, o1 = 0, o2 = 0;
 #pragma unroll
   for (int a = 0; a < W; ++a) {
-    const int jx = (ix + LO + a + N) & (N - 1);
+    const int jx = wrap_index(ix + LO + a, N);
 #pragma unroll
     for (int b = 0; b < W; ++b) {
-      const int jy = (iy + LO + b + N) & (N - 1);
+      const int jy = wrap_index(iy + LO + b, N);
       const vec4<T>* row = f + ((long long)jx * N + jy) * N;
       T s0 = 0, s1 = 0, s2 = 0;
 #pragma unroll

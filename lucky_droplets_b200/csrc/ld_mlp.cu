@@ -601,8 +601,12 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
 //   layer 3: 8 MMAs (N 16: W3 padded); 4 warps write out = tricubic + scale * os * MLP in the grid
 //   frame.
 // The group's leader issues its MMAs and commits them to the group's mbarrier; group barriers are
-// named barriers.  Every wait is bounded: a wait that runs out raises LD_STATUS_WAIT_TIMEOUT and
-// the group stops; the CTA frees its tensor memory.
+// named barriers.  Every wait is bounded (wait_limit polls, the plan's setting): a wait that runs
+// out raises LD_STATUS_WAIT_TIMEOUT and the group stops; before the CTA frees its tensor memory
+// and exits, one thread waits (bounded by kWaitLimitMlp) for the feature copy and the MMAs that
+// are still in flight, so that nothing writes shared or tensor memory after the CTA has left.
+// With `stall` set (a test of that path) each group first waits on a barrier that nothing
+// completes, while the CTA's first feature copy is in flight.
 constexpr int FT_THREADS = 512;
 constexpr int FT_GROUP = 256;                         // threads of a group
 constexpr int N3P = 16;                               // layer-3 N padded for M = 128
@@ -613,9 +617,10 @@ constexpr int SM_X = SM_W3 + N3P * H * 2;             // + 4096
 constexpr int SM_H0 = SM_X + TILE_X_BYTES;
 constexpr int SM_H1 = SM_H0 + TM * H * 2;
 constexpr int SM_BIAS = SM_H1 + TM * H * 2;           // b1[128], b2[128], b3[16]
-constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma[2]
-constexpr int SM_TMEM = SM_BAR + 4 * 8;
-constexpr size_t SMEM_FWD = SM_TMEM + 16;
+constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma[2], bar_stall
+constexpr int SM_TMEM = SM_BAR + 5 * 8;
+constexpr int SM_CNT = SM_TMEM + 16;
+constexpr size_t SMEM_FWD = SM_CNT + 8 * 4;
 constexpr unsigned TMEM_COLS = 512;                   // group g: columns 256 g .. 256 g + 143
 constexpr unsigned kWaitLimitMlp = 1u << 24;
 
@@ -641,7 +646,7 @@ template <typename T>
 __global__ void __launch_bounds__(FT_THREADS, 1)
 k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__ auxg, long long n,
                  const bf16* __restrict__ packed, const float* __restrict__ params, T* __restrict__ out,
-                 unsigned* __restrict__ status) {
+                 unsigned* __restrict__ status, unsigned wait_limit, int stall) {
   extern __shared__ __align__(1024) unsigned char sm[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int g = warp >> 3, gw = warp & 7;             // group, warp within the group
@@ -651,7 +656,12 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   // barrier's k-th wait has parity k % 2 (a fresh barrier counts parity 1 as complete)
   uint64_t* bar_x = reinterpret_cast<uint64_t*>(sm + SM_BAR);
   uint64_t* bar_mma = bar_x + 2;
+  uint64_t* bar_stall = bar_x + 4;  // completed by nothing: the first wait of a stall test
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + SM_TMEM);
+  // drain bookkeeping: X copies issued to / waited on each bar_x, MMA commits to / waits on each
+  // bar_mma; each counter has one writer (a group leader; cnt[0] leaves out the first copy, which
+  // thread 0 issues before the loop) and thread 0 reads them after the final barrier
+  unsigned* cnt = reinterpret_cast<unsigned*>(sm + SM_CNT);  // [x_issued 2][x_waited 2][mma_commit 2][mma_wait 2]
   // weights into the tile layout (from the packed, row-padded copies)
   for (int e = tid; e < H * (K1 / 8); e += FT_THREADS) {
     const int nrow = e / (K1 / 8), kc = e % (K1 / 8);
@@ -679,8 +689,10 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
     mbar_init(&bar_x[1], 1);
     mbar_init(&bar_mma[0], 1);
     mbar_init(&bar_mma[1], 1);
+    mbar_init(bar_stall, 1);
     mbar_init_fence();
   }
+  if (tid < 8) cnt[tid] = 0u;
   if (warp == 0) {
     tmem_alloc(tmem_slot, TMEM_COLS);
     tmem_relinquish();
@@ -695,7 +707,7 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   const long long ntiles = (n + TM - 1) / TM;
   const long long mine = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // CTA's tiles
   constexpr unsigned ID1 = umma_idesc_bf16(128, 128), ID3 = umma_idesc_bf16(128, N3P);
-  if (tid == 0 && mine > 0) {
+  if (tid == 0 && mine > 0) {  // the first copy is counted at the end (x_issued[0] + 1)
     mbar_expect_tx(&bar_x[0], TILE_X_BYTES);
     bulk_g2s(sm + SM_X, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
   }
@@ -713,22 +725,30 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
     }
     // X of this tile (the i-th copy into the X buffer, on bar_x[g], the group's (i/2)-th wait);
     // failures are made group-uniform
-    failed = group_or(g, !mbar_wait_bounded(&bar_x[g], (unsigned)((i >> 1) & 1), kWaitLimitMlp));
+    if (stall && i == g) {  // a wait on a barrier that nothing completes runs out
+      failed = group_or(g, !mbar_wait_bounded(bar_stall, 0u, wait_limit));
+      if (failed) break;
+    }
+    failed = group_or(g, !mbar_wait_bounded(&bar_x[g], (unsigned)((i >> 1) & 1), wait_limit));
     if (failed) break;
     if (leader) {
+      cnt[2 + g] += 1u;
       tc_fence_after();
 #pragma unroll 1
       for (int k = 0; k < K1 / 16; ++k)
         umma_bf16(tmem, umma_desc(sm + SM_X + 2 * k * (TM / 8) * 128, (TM / 8) * 128, 128),
                   umma_desc(sm + SM_W1 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), ID1, k > 0);
       umma_commit(&bar_mma[g]);
+      cnt[4 + g] += 1u;
     }
     for (int layer = 0; layer < 3; ++layer) {
-      failed = group_or(g, !mbar_wait_bounded(&bar_mma[g], ph, kWaitLimitMlp));
+      failed = group_or(g, !mbar_wait_bounded(&bar_mma[g], ph, wait_limit));
+      if (!failed && leader) cnt[6 + g] += 1u;
       ph ^= 1u;
       tc_fence_after();
       if (layer == 0 && leader && !failed && i + 1 < mine) {
         // layer 1 has consumed X: bring in the CTA's next tile (the other group's, on its barrier)
+        cnt[g ^ 1] += 1u;
         mbar_expect_tx(&bar_x[g ^ 1], TILE_X_BYTES);
         bulk_g2s(sm + SM_X, Xg + (tile + gridDim.x) * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[g ^ 1]);
       }
@@ -773,6 +793,7 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
                         umma_desc(sm + SM_W3 + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), ID3, k > 0);
           }
           umma_commit(&bar_mma[g]);
+          cnt[4 + g] += 1u;
         }
       } else if (gw < 4) {
         float v[16];
@@ -794,8 +815,23 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   }
   if (failed && (tid & (FT_GROUP - 1)) == 0) atomicOr(status, LD_STATUS_WAIT_TIMEOUT);
   tc_fence_before();
-  __syncthreads();
+  const bool any_failed = __syncthreads_or(failed) != 0;
   tc_fence_after();
+  if (any_failed) {
+    // a group stopped early: copies and MMAs it (or the other group) issued may still be in
+    // flight; wait for each barrier's outstanding completion (the k-th completion of a barrier
+    // has parity k % 2) before the tensor memory is freed and the shared memory released
+    if (tid == 0) {
+      for (int b = 0; b < 2; ++b) {
+        const unsigned x_issued = cnt[b] + (b == 0 && mine > 0 ? 1u : 0u);
+        if (x_issued > cnt[2 + b]) mbar_wait_bounded(&bar_x[b], cnt[2 + b] & 1u, kWaitLimitMlp);
+        if (cnt[4 + b] > cnt[6 + b]) mbar_wait_bounded(&bar_mma[b], cnt[6 + b] & 1u, kWaitLimitMlp);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
   if (warp == 0) tmem_dealloc(*tmem_slot, TMEM_COLS);
 }
 
@@ -1097,6 +1133,7 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
   if (!p || !u4 || !packed || !params || n < 0 || (n > 0 && (!pos || !out)))
     return ld_fail(LD_ERR_ARG, "ld_mlp_infer: bad arguments");
   if (p->N > 1024) return ld_fail(LD_ERR_ARG, "ld_mlp_infer: N > 1024 (stencil offsets are 32-bit)");
+  if (p->N & (p->N - 1)) return ld_fail(LD_ERR_UNSUPPORTED, "ld_mlp_infer: N = %d (the stencil wrap needs a power of two)", p->N);
   if (n == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;
@@ -1126,7 +1163,8 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
       }
       ProfScope ps(p, KID_MLP_INFER, s);
       k_mlp_forward_tc<float><<<(unsigned)gm, FT_THREADS, SMEM_FWD, s>>>(X, aux, nb, (const bf16*)packed, params,
-                                                                        (float*)out + 3 * b0, p->status);
+                                                                        (float*)out + 3 * b0, p->status,
+                                                                        p->wait_limit, p->wait_stall);
     } else {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_forward_tc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)SMEM_FWD));
@@ -1137,7 +1175,8 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
       }
       ProfScope ps(p, KID_MLP_INFER, s);
       k_mlp_forward_tc<double><<<(unsigned)gm, FT_THREADS, SMEM_FWD, s>>>(X, aux, nb, (const bf16*)packed,
-                                                                         params, (double*)out + 3 * b0, p->status);
+                                                                         params, (double*)out + 3 * b0, p->status,
+                                                                         p->wait_limit, p->wait_stall);
     }
     LD_LAUNCH_CHECK();
   }
@@ -1164,6 +1203,7 @@ int ld_mlp_samples(ld_plan* p, const void* u4, const void* ue, const int64_t* id
   if (!p || !u4 || !ue || ns < 0 || (ns > 0 && (!idx || !params || !X || !T || !aux)))
     return ld_fail(LD_ERR_ARG, "ld_mlp_samples: bad arguments");
   if (p->N > 1024) return ld_fail(LD_ERR_ARG, "ld_mlp_samples: N > 1024 (stencil offsets are 32-bit)");
+  if (p->N & (p->N - 1)) return ld_fail(LD_ERR_UNSUPPORTED, "ld_mlp_samples: N = %d (the stencil wrap needs a power of two)", p->N);
   if (ns == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;

@@ -198,12 +198,18 @@ template <typename T, int N> struct Ops {
     return LD_OK;
   }
 
+  // The integrating-factor table exp(-nu h k^2) for the current nu h, built on the stream when
+  // nu h changes.  While the stream is being captured into a CUDA graph the table kernel is
+  // recorded into the graph and the table is not marked built: the graph may never be replayed
+  // (a discarded capture), so only a launch that runs marks it.
   static int ensure_ifac(ld_plan* p, double nuh, cudaStream_t s) {
     if (p->ifac_key == nuh) return LD_OK;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    LD_CUDA_CHECK(cudaStreamIsCapturing(s, &cap));
     ProfScope ps(p, KID_IFAC, s);
     k_ifac<T><<<grid1d(p->nifac, 256), 256, 0, s>>>((T*)p->ifac, p->nifac, nuh);
     LD_LAUNCH_CHECK();
-    p->ifac_key = nuh;
+    if (cap == cudaStreamCaptureStatusNone) p->ifac_key = nuh;
     return LD_OK;
   }
 
@@ -211,7 +217,7 @@ template <typename T, int N> struct Ops {
   static int zcross_pipe(ld_plan* p, const C* W2, C* W1, T* uout, int ulayout, T sc, cudaStream_t s) {
     constexpr int WARPS = sizeof(T) == 4 ? 8 : 4;
     const long long NN = (long long)N * N;
-    const size_t smem = (size_t)WARPS * ((size_t)12 * p->Mzp + Cfg<N>::ZBUF) * sizeof(C) + 16 * WARPS;
+    const size_t smem = (size_t)WARPS * ((size_t)12 * p->Mzp + Cfg<N>::ZBUF) * sizeof(C) + 24 * WARPS;
     auto k = k_z_cross_pipe<T, N>;
     if (int rc = set_smem(k, smem)) return rc;
     static int blocks_per_sm = -1;
@@ -227,7 +233,8 @@ template <typename T, int N> struct Ops {
     long long grid = (long long)sms * blocks_per_sm;
     const long long need = (NN + WARPS - 1) / WARPS;
     if (grid > need) grid = need;
-    k<<<(unsigned)grid, WARPS * 32, smem, s>>>(W2, W1, uout, ulayout, p->Mzp, p->kc, sc, (const C*)p->tw, p->status);
+    k<<<(unsigned)grid, WARPS * 32, smem, s>>>(W2, W1, uout, ulayout, p->Mzp, p->kc, sc, (const C*)p->tw, p->status,
+                                               p->wait_limit, p->wait_stall);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
@@ -415,6 +422,9 @@ template <typename T, int N> struct Table {
     return LD_OK;
   }
   static int autotune(ld_plan* p, cudaStream_t s, double* ms) { return O::autotune(p, s, ms); }
+  static int prepare(ld_plan* p, const ld_flow_params* prm, cudaStream_t s) {
+    return O::ensure_ifac(p, prm->nu * prm->dt, s);
+  }
   static int rhs(ld_plan* p, int mode, void* s0, void* s1, void* s2, void* s3, void* uout,
                  const ld_flow_params* prm, double visc, cudaStream_t s) {
     C *a = (C*)s0, *b = (C*)s1, *c = (C*)s2, *d = (C*)s3;
@@ -458,7 +468,7 @@ template <typename T, int N> struct Table {
   }
   static const OpsTable* get() {
     static const OpsTable t = {rfft_full, irfft_full, irfft_cube, rfft_cube, to_cube, from_cube,
-                               shell_spectrum, rhs, epilogue, epilogue0, gather, dstage, autotune};
+                               shell_spectrum, rhs, epilogue, epilogue0, gather, dstage, autotune, prepare};
     return &t;
   }
 };

@@ -80,8 +80,14 @@ const char* ld_last_error(void) { return g_last_error; }
 int ld_plan_create(ld_plan** out, int n, int precision) {
   if (!out) return ld_fail(LD_ERR_ARG, "null output pointer");
   *out = nullptr;
-  if (n < 16 || n > 512 || (n & (n - 1))) return ld_fail(LD_ERR_UNSUPPORTED, "N=%d: need a power of two in [16,512]", n);
   if (precision != LD_F32 && precision != LD_F64) return ld_fail(LD_ERR_ARG, "precision %d", precision);
+  {
+    ld_plan probe;
+    probe.N = n;
+    probe.prec = precision;
+    if (!table_of(&probe))
+      return ld_fail(LD_ERR_UNSUPPORTED, "N=%d: grids are powers of two in [16, 512] or 96, 192, 360, 384", n);
+  }
   ld_plan* p = new (std::nothrow) ld_plan();
   if (!p) return ld_fail(LD_ERR_NOMEM, "host allocation failed");
   p->N = n;
@@ -271,6 +277,19 @@ int ld_plan_set_tuning(ld_plan* p, const int32_t* choice) {
     return ld_fail(LD_ERR_ARG, "ld_plan_set_tuning: bad arguments");
   p->tune_y[0] = choice[0];
   p->tune_y[1] = choice[1];
+  return LD_OK;
+}
+
+int ld_plan_prepare(ld_plan* p, const ld_flow_params* prm, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!prm) return ld_fail(LD_ERR_ARG, "ld_plan_prepare: bad arguments");
+  return table_of(p)->prepare(p, prm, S(stream));
+}
+
+int ld_plan_set_wait_limit(ld_plan* p, uint32_t limit, int stall) {
+  if (int rc = check_plan(p)) return rc;
+  p->wait_limit = limit == 0 ? (1u << 24) : limit;
+  p->wait_stall = stall ? 1 : 0;
   return LD_OK;
 }
 

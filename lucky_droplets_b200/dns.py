@@ -42,6 +42,8 @@ class ForcedDNS:
         self.epilogue = epilogue
         self.prm = flow_params(dt, nu, f0, shell_no)
         p = self.plan
+        if integrator == "rk2if":  # the integrating-factor table, built before any capture
+            check(_lib.lib().ld_plan_prepare(p.handle, ctypes.byref(self.prm), stream_ptr()))
         self.uk = p.empty_cube(3)
         self.aux = p.empty_cube(3)   # ustar (rk2if) or the stage input y (rk4)
         self.acc = p.empty_cube(3)
@@ -142,9 +144,15 @@ class ForcedDNS:
         return paths, self.diagnostics()
 
     def load(self, dirpath):
-        """Restart from Fields_k_0.npz (the spectral velocity in the reference's layout)."""
-        from .outputs import read_fields
-        return self.set_uk_full(read_fields(dirpath))
+        """Restart from the Fields_k_{slab}.npz files of a checkpoint written by any number of
+        ranks (the spectral velocity in the reference's layout, re-slabbed as load_npz does,
+        F:374-407).  Raises outputs.CheckpointError for a missing, truncated or mis-shaped
+        checkpoint, or one of another grid size."""
+        from .outputs import CheckpointError, read_fields
+        uk = read_fields(dirpath)
+        if uk.shape[1] != self.N:
+            raise CheckpointError(f"checkpoint grid N = {uk.shape[1]}, this run N = {self.N}")
+        return self.set_uk_full(uk)
 
     def attach(self, droplets, collider=None, sort_every=0, pair_capacity=None):
         """Advance ``droplets`` with the flow.
@@ -178,6 +186,64 @@ class ForcedDNS:
     def step(self, nsteps=1, stream=None):
         for k in range(nsteps):
             self._step_one(stream)
+
+    def interp_state(self):
+        """The droplet interpolation the next step will enqueue (what a captured graph freezes)."""
+        d = self.droplets
+        return None if d is None else d.interp_state()
+
+    def judge(self, frac=0.01, seed=0, stream=None):
+        """The judge of the learned interpolation on the current state: the exact spectral sum at a
+        random fraction of the droplets against the learned and the tricubic velocities; the
+        LearnedInterp's rule then switches the network off (tricubic fallback) or on.  Returns
+        {"step", "learned", "tricubic", "n_sample", "enabled"} or None without a network."""
+        torch = _torch()
+        d = self.droplets
+        li = getattr(d, "learned", None) if d is not None else None
+        if li is None:
+            return None
+        n = max(1, int(round(frac * d.n)))
+        g = torch.Generator(device="cpu").manual_seed(int(seed) * 1000003 + self.nstep)
+        sel = torch.randperm(d.n, generator=g)[:n].to(d.pos.device)
+        pos = d.pos[sel].contiguous()
+        e_l, e_t = li.judge(self.uk, li.interleaved(self.uk), pos)
+        return {"step": self.nstep, "learned": e_l, "tricubic": e_t, "n_sample": n, "enabled": li.enabled}
+
+    def evolve(self, nsteps, st=0, on_output=None, judge_frac=0.01, judge_seed=0, graph_steps=0):
+        """The time loop of evolve_and_save (F:556-627): `nsteps` steps; at every output interval -
+        a step count divisible by `st` (F:575 `i % st == 0`), and once more after the last step
+        (F:624) - the judge of the learned interpolation runs (when the droplets have one) and then
+        `on_output(self)` (e.g. ``self.save(...)``).  The blow-up test of F:618-620 is read from the
+        device status word at every output (and raises BlowUpError); the kernels raise the flag at
+        the step it happens.  With graph_steps > 0 the steps between outputs run as replays of
+        CUDA graphs of that many steps (one graph per re-sorting phase, re-captured when the
+        judge switches the interpolation).  Returns the list of judgements."""
+        verdicts = []
+
+        def output():
+            self.check()
+            v = self.judge(judge_frac, judge_seed)
+            if v is not None:
+                verdicts.append(v)
+            if on_output is not None:
+                on_output(self)
+
+        graphs = {}
+        end = self.nstep + int(nsteps)
+        while self.nstep < end:
+            if st and self.nstep % st == 0:
+                output()
+            nxt = end if not st else min(end, (self.nstep // st + 1) * st)
+            while graph_steps > 0 and nxt - self.nstep >= graph_steps:
+                period = self.sort_every if (self.droplets is not None and self.sort_every > 0) else 0
+                key = self.nstep % period if period else 0
+                g = graphs.get(key)
+                if g is None:
+                    g = graphs[key] = self.capture(graph_steps)
+                g.replay()
+            self.step(nxt - self.nstep)
+        output()
+        return verdicts
 
     def capture(self, nsteps):
         """Capture `nsteps` steps from the current step count into a CUDA graph (nothing runs
@@ -237,11 +303,14 @@ class ForcedDNS:
         if d is not None and self.collider is not None:
             d.collide(self.collider, self.pairs, stream)
 
-    def step_host(self, uk_host, pos_host=None, vel_host=None, nsteps=1, stream=None):
+    def step_host(self, uk_host, pos_host=None, vel_host=None, nsteps=1, stream=None, layout="cube"):
         """Drop-in for one call of the reference's time-loop body with host state (F:582-610):
-        copies the cube-layout spectrum (and droplet positions/velocities) from host memory,
-        advances ``nsteps`` steps and copies the new state back into the same host arrays.
-        Host tensors should be pinned for asynchronous copies.  Returns the host tensors.
+        copies the spectrum (and droplet positions/velocities) from host memory, advances
+        ``nsteps`` steps and copies the new state back into the same host arrays.  ``layout``:
+        "cube" - the dealiased cube (3, Mx, My, Mzp) the step keeps on the device; "full" - the
+        reference's own layout (3, N, N, N/2+1) (F:158), converted on the device (the dealias of
+        F:567-569 on the way in, zeros outside the mask on the way out).  Host tensors should be
+        pinned for asynchronous copies.  Returns the host tensors.
 
         The spectrum is needed by the first kernel, so its copy precedes the step; the droplet
         copies run on a side stream under the first stage's flow transforms (the droplets are
@@ -250,11 +319,23 @@ class ForcedDNS:
         search; the droplets' after their last update, under the collision search, which reads
         the positions but writes no state."""
         torch = _torch()
+        if layout not in ("cube", "full"):
+            raise ValueError("layout must be 'cube' or 'full'")
         s = torch.cuda.current_stream() if stream is None else stream
         d = self.droplets if pos_host is not None else None
         side = self._copy_streams()
+        full = None
+        if layout == "full":
+            p = self.plan
+            full = getattr(self, "_full", None)
+            if full is None:
+                full = self._full = p.empty_full(3)
         with torch.cuda.stream(s):
-            self.uk.copy_(uk_host, non_blocking=True)
+            if full is None:
+                self.uk.copy_(uk_host, non_blocking=True)
+            else:
+                full.copy_(uk_host, non_blocking=True)
+                self.plan.to_cube(full, self.uk, stream=s)
         if d is not None:
             side[0].wait_stream(s)  # earlier users of pos/vel are done before they are overwritten
             with torch.cuda.stream(side[0]):
@@ -265,9 +346,13 @@ class ForcedDNS:
             s.wait_stream(side[0])
 
         def flow_out():
+            src = self.uk
+            if full is not None:
+                self.plan.from_cube(self.uk, full, stream=s)
+                src = full
             side[1].wait_stream(s)
             with torch.cuda.stream(side[1]):
-                uk_host.copy_(self.uk, non_blocking=True)
+                uk_host.copy_(src, non_blocking=True)
 
         def droplets_out():
             if d is not None:
@@ -308,11 +393,17 @@ class StepGraph:
     buffers the steps use must stay where they are (they do: every operation works in place)."""
 
     def __init__(self, dns, nsteps):
-        torch = _torch()
         self.dns = dns
         self.nsteps = int(nsteps)
         self.period = dns.sort_every if (dns.droplets is not None and dns.sort_every > 0) else 0
         self.phase = dns.nstep % self.period if self.period else 0
+        self.recaptures = 0
+        self._capture()
+
+    def _capture(self):
+        torch = _torch()
+        dns = self.dns
+        self.interp = dns.interp_state()
         saved = (dns.t, dns.nstep)
         self.graph = torch.cuda.CUDAGraph()
         cap = torch.cuda.Stream(device=dns.plan.device)
@@ -324,12 +415,18 @@ class StepGraph:
             dns.t, dns.nstep = saved
 
     def replay(self, n=1):
-        """Advance the state by n * nsteps steps (graph launches on the current stream)."""
+        """Advance the state by n * nsteps steps (graph launches on the current stream).  A graph
+        whose droplet interpolation is no longer the droplets' current one (the judge switched the
+        learned interpolation off or on since the capture) is captured again first."""
         dns = self.dns
         for _ in range(n):
             if self.period and dns.nstep % self.period != self.phase:
                 raise RuntimeError(f"step graph captured at step phase {self.phase} (mod {self.period}), "
                                    f"replayed at step {dns.nstep}")
+            if dns.interp_state() != self.interp:
+                self.graph = None
+                self._capture()
+                self.recaptures += 1
             self.graph.replay()
             for _ in range(self.nsteps):  # the same sum as stepping one by one
                 dns.t += dns.dt
@@ -410,6 +507,11 @@ class Droplets:
         """Rows of a per-droplet tensor in droplet-id order (host numpy)."""
         order = _torch().argsort(self.ids)
         return t[order].cpu().numpy()
+
+    def interp_state(self):
+        """"learned" while an attached network is enabled, else the droplets' own method."""
+        li = getattr(self, "learned", None)
+        return "learned" if (li is not None and li.enabled) else self.method
 
     def use_learned(self, learned):
         """Interpolate with a trained LearnedInterp (tricubic + learned correction); the judge of

@@ -13,8 +13,10 @@ drives the kernels of csrc/ld_mlp.cu:
 * ``train``: Adam on mini-batches with the project's forward/backward kernels.
 * ``infer``: fused stencil gather + tricubic + MLP correction at droplet positions.
 * ``judge``: relative L2 error against the exact direct Fourier sum (``Plan.exact_sum``) on a
-  sample of droplets, with tricubic as the comparison; ``enabled`` turns off when the learned
-  error exceeds the tolerance or loses to tricubic.
+  sample of droplets, with tricubic as the comparison; with the default rule ("tolerance")
+  ``enabled`` turns off when the learned error exceeds the tolerance, and back on when a later
+  judgement meets it.  The rule "tolerance_or_better" keeps the network while it still beats
+  tricubic (off only when it misses the tolerance and loses to tricubic).
 """
 import ctypes
 
@@ -91,7 +93,9 @@ def init_flat(seed=0, scale_mode=1):
 class LearnedInterp:
     """MLP parameters, optimiser state and packed weights on one device."""
 
-    def __init__(self, plan, seed=0, params=None, tol=1e-4, scale_mode=1):
+    RULES = ("tolerance", "tolerance_or_better")
+
+    def __init__(self, plan, seed=0, params=None, tol=1e-4, scale_mode=1, rule="tolerance"):
         torch = _torch()
         n_params, n_packed, k_in, tile = sizes()
         assert n_params == N_PARAMS and k_in == K1
@@ -105,7 +109,10 @@ class LearnedInterp:
         self.grad = torch.zeros_like(self.params)
         self.loss = torch.zeros(1, dtype=torch.float32, device=dev)
         self.step_count = 0
+        if rule not in self.RULES:
+            raise ValueError(f"rule must be one of {self.RULES}")
         self.tol = tol
+        self.rule = rule
         self.enabled = True
         self.history = []
         check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
@@ -272,7 +279,8 @@ class LearnedInterp:
     # ---- judge ------------------------------------------------------------------------------------
     def judge(self, uk, u4, pos, n_sample=None, seed=0):
         """Relative L2 errors (learned, tricubic) against the exact Fourier sum on a sample of
-        positions; disables the network when it misses the tolerance and loses to tricubic."""
+        positions; sets ``enabled`` by the judge's rule (default: off when the learned error
+        exceeds the tolerance)."""
         torch = _torch()
         p = self.plan
         n = int(pos.shape[0])
@@ -288,7 +296,10 @@ class LearnedInterp:
         den = torch.linalg.norm(exact)
         e_l = float(torch.linalg.norm(learned - exact) / den)
         e_t = float(torch.linalg.norm(tric.to(torch.float64) - exact) / den)
-        self.enabled = (e_l <= self.tol) or (e_l < e_t)
+        if self.rule == "tolerance":
+            self.enabled = e_l <= self.tol
+        else:
+            self.enabled = (e_l <= self.tol) or (e_l < e_t)
         self.history.append((e_l, e_t, self.enabled))
         return e_l, e_t
 

@@ -122,6 +122,19 @@ class ReferenceRun:
         self.c_stage = torch.empty((nd, 7), **f64)
         self.work = torch.empty((int(_lib.lib().ld_ref_workspace_doubles()),), **f64)
 
+    def load(self, dirpath, n_dir=None):
+        """Restart the flow and the number density from a checkpoint of the reference written by
+        any number of ranks (load_npz, F:374-407): Fields_k_{slab}.npz in dirpath, n_{slab}.npz
+        in n_dir (the reference keeps them in its droplet directory, F:449-450; default dirpath)."""
+        from .outputs import CheckpointError, read_n
+        self.dns.load(dirpath)
+        n = read_n(dirpath if n_dir is None else n_dir)
+        N = self.dns.N
+        if n.shape != (N, N, N):
+            raise CheckpointError(f"n of shape {n.shape} in a run of N = {N}")
+        self.n.copy_(_torch().as_tensor(np.asarray(n, np.float64)))
+        return self
+
     # ---- pieces -----------------------------------------------------------------------------------
     def n_rhs(self, n_field, fc, out, stream=None):
         """kn = irfft((-i k . (n v)^ - fc^) dealias) (F:325-330), with v = self.v."""

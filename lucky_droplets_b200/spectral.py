@@ -163,6 +163,11 @@ class Plan:
         return {"ms": {"inverse_y": [round(x, 5) for x in ms[:4]], "forward_y": [round(x, 5) for x in ms[4:]]},
                 "choice": [int(ch[0]), int(ch[1])]}
 
+    def set_wait_limit(self, limit=0, stall=False):
+        """Polls before a bounded device wait of this plan's kernels gives up (0: the default);
+        stall=True makes the first waits run out on purpose (a test of the time-out path)."""
+        check(_lib.lib().ld_plan_set_wait_limit(self._h, int(limit), int(bool(stall))))
+
     def set_tuning(self, choice):
         ch = (ctypes.c_int32 * 2)(*[int(c) for c in choice])
         check(_lib.lib().ld_plan_set_tuning(self._h, ch))

@@ -18,7 +18,9 @@ Two runs are made per case with the same seed:
 Only the recorded arrays are written (``*.npz``); no reference source enters the repository.
 This script needs the reference checkout and is run by hand in the build container:
 
-    NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py [reference_dir]
+    NUMBA_NUM_THREADS=1 python tests/golden/make_golden.py <reference_dir>
+
+The reference checkout is the first argument, or the environment variable LD_REFERENCE_DIR.
 """
 import contextlib
 import io
@@ -164,5 +166,14 @@ def main(ref_dir):
         print(f"wrote {path} ({path.stat().st_size/1e6:.2f} MB)")
 
 
+def reference_dir(argv=None):
+    """The reference checkout: the first argument, else $LD_REFERENCE_DIR; no default."""
+    argv = sys.argv[1:] if argv is None else argv
+    d = argv[0] if argv else os.environ.get("LD_REFERENCE_DIR")
+    if not d:
+        raise SystemExit("usage: make_golden.py <reference_dir>  (or set LD_REFERENCE_DIR)")
+    return d
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir())

@@ -43,6 +43,6 @@ def test_version_and_argument_errors_without_gpu():
     # argument validation happens before any CUDA call
     h = ctypes.c_void_p()
     assert L.ld_plan_create(ctypes.byref(h), 100, 0) == -3   # LD_ERR_UNSUPPORTED
-    assert b"power of two" in L.ld_last_error()
+    assert b"powers of two" in L.ld_last_error() and b"360" in L.ld_last_error()
     assert L.ld_plan_create(ctypes.byref(h), 64, 7) == -1     # LD_ERR_ARG
     assert L.ld_rfft_mpi(None, None, None, 1, None) == -1

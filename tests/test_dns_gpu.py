@@ -39,7 +39,7 @@ def test_velocity_rhs_matches_reference(torch, golden, name, prec):
     assert rel(full, ref) < TOL[prec]
 
 
-@pytest.mark.parametrize("N", [64, 128, 256])
+@pytest.mark.parametrize("N", [64, 128, 256, 96, 360])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_velocity_rhs_matches_oracle(torch, N, prec):
     """The same RHS at larger N against the FP64 restatement, on a seeded initial field."""
@@ -84,7 +84,7 @@ def test_rk4_time_loop_matches_reference(torch, golden, name, prec):
     assert rel(dns.uk_full(), g["run_uk"] * grid.dealias) < TOL[prec]
 
 
-@pytest.mark.parametrize("N", [32, 64])
+@pytest.mark.parametrize("N", [32, 64, 96])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_rk2if_matches_oracle(torch, N, prec):
     """RK2 + integrating factor against the FP64 NumPy restatement, 5 steps."""
@@ -264,3 +264,58 @@ def test_step_graph_replay_matches_eager_steps(torch):
     b.step(1)
     with pytest.raises(RuntimeError):
         g.replay()
+
+
+def test_step_host_reference_layout(torch):
+    """step_host with the state in the reference's layout (3, N, N, N/2+1) (F:158): the same steps
+    as device-resident stepping, the spectrum handed back dealiased in the reference layout."""
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    from lucky_droplets_b200.collide import Collider
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3, g=0.1)
+    uk0, u0 = C.init_flow(C.ConfigGrid(N), prm, seed=18)
+    pos, tau, rad = C.init_droplets(prm, 18, "uniform_tau", nd=3000)
+    rad = rad * 5.0
+    vel = C.gather(u0, pos, "tricubic")
+    runs = []
+    for _ in range(2):
+        dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision="f32")
+        dns.set_uk_full(uk0)
+        d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g, radius=rad)
+        dns.attach(d, collider=Collider(d.n, 2 * rad.max()), sort_every=2)
+        runs.append((dns, d))
+    (a, da), (b, db) = runs
+    a.step(4)
+    ukf = torch.as_tensor(uk0).to(torch.complex64).pin_memory()
+    pos_h = db.pos.cpu().pin_memory()
+    vel_h = db.vel.cpu().pin_memory()
+    for _ in range(4):
+        b.step_host(ukf, pos_h, vel_h, layout="full")
+    torch.cuda.synchronize()
+    assert torch.equal(b.uk, a.uk)
+    assert torch.equal(ukf, a.plan.from_cube(a.uk).cpu())
+    assert torch.equal(pos_h, da.pos.cpu()) and torch.equal(vel_h, da.vel.cpu())
+
+
+@pytest.mark.parametrize("N", [96, 360])
+def test_tricubic_droplet_step_on_mixed_radix_grid(torch, N):
+    """The plain FP64 tricubic step on a mixed-radix grid (the equal-error comparator's grids):
+    one coupled step against the FP64 oracle, droplets near the periodic faces included."""
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    prm = C.ConfigParams(N=N, nu=2.5e-3, dt=1e-3, g=0.1)
+    grid = C.ConfigGrid(N)
+    uk0, u0 = C.init_flow(grid, prm, seed=N)
+    rng = np.random.default_rng(N)
+    pos = rng.uniform(-0.01, 2 * np.pi + 0.01, (3000, 3))
+    tau = np.exp(rng.uniform(np.log(0.05), np.log(2.0), 3000))
+    vel = C.gather(u0, pos, "tricubic")
+    dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision="f64")
+    dns.set_uk_full(uk0)
+    d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g)
+    dns.attach(d)
+    uk, p_, v_ = C.step(grid, prm, uk0, pos, vel, tau, "tricubic")
+    uk = grid.project(np.stack([grid.rfft(grid.irfft(uk[c])) for c in range(3)]))
+    dns.step(1)
+    assert rel(dns.uk_full(), uk * grid.dealias) < 1e-12
+    assert np.abs(d.pos.cpu().numpy() - p_).max() < 1e-13
+    assert rel(d.vel.cpu().numpy(), v_) < 1e-12

@@ -38,7 +38,9 @@ def test_rfft_irfft_golden_N16(torch, golden, prec):
     assert rel(x, g["ifft_out"]) < TOL[prec]
 
 
-@pytest.mark.parametrize("N", [16, 32, 64, 128, 256])
+# powers of two, and the mixed-radix sizes (radix-3 and radix-5 stages; the reference takes any N,
+# scipy.fft being mixed-radix)
+@pytest.mark.parametrize("N", [16, 32, 64, 128, 256, 96, 192, 360, 384])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_rfft_matches_scipy(torch, N, prec):
     rng = np.random.default_rng(N)
@@ -53,7 +55,7 @@ def test_rfft_matches_scipy(torch, N, prec):
     assert rel(x, sfft.irfftn(X, s=(N, N, N), axes=(1, 2, 3))) < TOL[prec] * (2 if N >= 128 else 1)
 
 
-@pytest.mark.parametrize("N", [16, 64, 256])
+@pytest.mark.parametrize("N", [16, 64, 256, 96, 360])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_cube_transforms(torch, N, prec):
     """Dealiased (cube-layout) transforms equal the full ones applied to dealiased spectra."""
@@ -94,3 +96,21 @@ def test_autotuned_variants_give_identical_rhs(N):
         outs.append(p.velocity_rhs(uk, prm.nu, prm.f0, prm.shell_no).clone())
     for o in outs[1:]:
         assert torch.equal(o, outs[0])
+
+
+def test_unsupported_sizes_are_refused():
+    """Sizes without kernel instances, and the learned interpolation on a mixed-radix grid, fail
+    with LD_ERR_UNSUPPORTED and a message."""
+    from lucky_droplets_b200._lib import LDError
+    from lucky_droplets_b200.spectral import Plan
+    import torch
+    from lucky_droplets_b200.mlp import LearnedInterp
+    for N in (100, 48, 1024):
+        with pytest.raises(LDError, match="grids are"):
+            Plan(N, "f32")
+    p = Plan(96, "f32")
+    li = LearnedInterp(p)
+    u4 = torch.zeros((96, 96, 96, 4), dtype=torch.float32, device="cuda")
+    pos = torch.zeros((10, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(LDError, match="power of two"):
+        li.infer(u4, pos)

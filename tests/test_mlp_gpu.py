@@ -147,7 +147,7 @@ def test_training_beats_tricubic(torch):
     grid = C.ConfigGrid(N)
     uk, _ = C.init_flow(grid, prm, seed=10)
     plan = Plan(N, "f32")
-    li = G.LearnedInterp(plan, seed=1, tol=1e-12)
+    li = G.LearnedInterp(plan, seed=1, tol=1e-12, rule="tolerance_or_better")
     cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
     li.calibrate(cube)
     X, T, W, _ = li.make_samples(cube, n_shifts=400, per_shift=1024, seed=1)
@@ -157,4 +157,7 @@ def test_training_beats_tricubic(torch):
     pos = torch.as_tensor(rng.uniform(0, 2 * np.pi, (4000, 3))).cuda()
     e_learned, e_tric = li.judge(cube, li.interleaved(cube), pos)
     assert e_learned < e_tric, (e_learned, e_tric)
-    assert li.enabled
+    assert li.enabled  # misses the (impossible) tolerance but beats tricubic
+    li.rule = "tolerance"
+    li.judge(cube, li.interleaved(cube), pos)
+    assert not li.enabled  # the default rule: off above the tolerance

@@ -40,3 +40,87 @@ def test_flux_is_reversed_cumulative_transfer():
     assert np.allclose(pik, np.cumsum(T[::-1])[::-1])
     scale = np.abs(T).max()
     assert abs(pik[0]) < 1e-10 * scale * N
+
+
+def _slab_checkpoint(tmp_path, P, N=16, seed=3):
+    """The files a P-rank run of the reference leaves (F:446-450): rank r writes the ky slab r of
+    the spectra and the x slab r of n."""
+    rng = np.random.default_rng(seed)
+    Nf = N // 2 + 1
+    uk = rng.standard_normal((3, N, N, Nf)) + 1j * rng.standard_normal((3, N, N, Nf))
+    n = rng.random((N, N, N))
+    Np = N // P
+    for r in range(P):
+        np.savez_compressed(tmp_path / f"Fields_k_{r}.npz", uk=uk[0][:, r * Np:(r + 1) * Np],
+                            vk=uk[1][:, r * Np:(r + 1) * Np], wk=uk[2][:, r * Np:(r + 1) * Np])
+        np.savez_compressed(tmp_path / f"n_{r}.npz", n=n[r * Np:(r + 1) * Np])
+    return uk, n
+
+
+def _load_npz_restated(path, N):
+    """load_npz of F:374-407 on one rank (Np = N): ky plane j from slab j // (N/P), index j % (N/P)."""
+    P = len([x for x in path.iterdir() if "Fields" in x.name and x.name.endswith(".npz")])
+    per = N // P
+    uk = np.zeros((3, N, N, N // 2 + 1), complex)
+    n = np.zeros((N, N, N))
+    for j in range(N):
+        F = np.load(path / f"Fields_k_{j // per}.npz")
+        nF = np.load(path / f"n_{j // per}.npz")
+        uk[0, :, j] = F["uk"][:, j % per]
+        uk[1, :, j] = F["vk"][:, j % per]
+        uk[2, :, j] = F["wk"][:, j % per]
+        n[j] = nF["n"][j % per]
+    return uk, n
+
+
+def test_multi_slab_checkpoint_reads_back_exactly(tmp_path):
+    """A 4-rank checkpoint is re-slabbed onto one GPU exactly as load_npz (F:374-407) does."""
+    from lucky_droplets_b200.outputs import read_n
+    uk, n = _slab_checkpoint(tmp_path, 4)
+    got = read_fields(tmp_path)
+    assert np.array_equal(got, uk)
+    assert np.array_equal(read_n(tmp_path), n)
+    ref_uk, ref_n = _load_npz_restated(tmp_path, 16)
+    assert np.array_equal(got, ref_uk) and np.array_equal(read_n(tmp_path), ref_n)
+
+
+def test_written_slabs_round_trip(tmp_path):
+    """write_outputs(slabs=P) writes what a P-rank run writes; reading it back is exact."""
+    from lucky_droplets_b200.outputs import read_n
+    rng = np.random.default_rng(5)
+    uk = rng.standard_normal((3, 16, 16, 9)) + 1j * rng.standard_normal((3, 16, 16, 9))
+    n = rng.random((16, 16, 16))
+    paths = write_outputs(tmp_path, uk, np.zeros(9), np.zeros(9), n=n, slabs=8)
+    assert sorted(p.name for p in paths if p.name.startswith("Fields")) == [f"Fields_k_{r}.npz" for r in range(8)]
+    assert np.load(tmp_path / "Fields_k_3.npz")["uk"].shape == (16, 2, 9)
+    assert np.load(tmp_path / "n_3.npz")["n"].shape == (2, 16, 16)
+    assert np.array_equal(read_fields(tmp_path), uk)
+    assert np.array_equal(read_n(tmp_path), n)
+
+
+def test_bad_checkpoints_raise_cleanly(tmp_path):
+    """Missing slabs, truncated archives, missing keys and a wrong shape raise CheckpointError."""
+    import pytest
+    from lucky_droplets_b200.outputs import CheckpointError
+    with pytest.raises(CheckpointError):
+        read_fields(tmp_path / "absent")
+    with pytest.raises(CheckpointError):
+        read_fields(tmp_path)  # no Fields files
+    _slab_checkpoint(tmp_path, 4)
+    (tmp_path / "Fields_k_2.npz").unlink()
+    with pytest.raises(CheckpointError, match="slabs"):
+        read_fields(tmp_path)
+    _slab_checkpoint(tmp_path, 4)
+    raw = (tmp_path / "Fields_k_1.npz").read_bytes()
+    (tmp_path / "Fields_k_1.npz").write_bytes(raw[: len(raw) // 2])  # truncated archive
+    with pytest.raises(CheckpointError, match="Fields_k_1"):
+        read_fields(tmp_path)
+    _slab_checkpoint(tmp_path, 4)
+    np.savez_compressed(tmp_path / "Fields_k_0.npz", uk=np.zeros((16, 4, 9)), vk=np.zeros((16, 4, 9)))
+    with pytest.raises(CheckpointError, match="wk"):
+        read_fields(tmp_path)
+    _slab_checkpoint(tmp_path, 4)
+    np.savez_compressed(tmp_path / "Fields_k_0.npz", uk=np.zeros((16, 3, 9)), vk=np.zeros((16, 3, 9)),
+                        wk=np.zeros((16, 3, 9)))
+    with pytest.raises(CheckpointError):
+        read_fields(tmp_path)

@@ -61,3 +61,31 @@ def test_diagnostics_and_round_trip(torch, tmp_path):
     u = dns.velocity().cpu().numpy()
     ref = C.gather(u, s["pos"], "trilinear")
     assert np.abs(s["umat"] - ref).max() < 1e-12
+
+
+def test_restart_from_multi_rank_checkpoint(torch, tmp_path):
+    """ForcedDNS.load and ReferenceRun.load take a 4-slab checkpoint (as a 4-rank reference run
+    writes it, F:446-450) and restore uk and n exactly; a truncated slab raises CheckpointError."""
+    from lucky_droplets_b200.dns import ForcedDNS
+    from lucky_droplets_b200.outputs import CheckpointError, write_outputs
+    from lucky_droplets_b200.refmode import ReferenceRun
+    dns, _ = _dns("f64", N=16)
+    dns.step(2)
+    rng = np.random.default_rng(11)
+    n = rng.random((16, 16, 16))
+    write_outputs(tmp_path, dns.uk_full(), dns.energy_spectrum(), dns.flux_spectrum(), n=n, slabs=4)
+    other = ForcedDNS.reference(16, precision="f64")
+    run = ReferenceRun(other, np.ones((16, 16, 16)), None, tps=0.0, g=0.0)
+    run.load(tmp_path)
+    assert torch.equal(other.uk, dns.uk)
+    assert np.array_equal(run.n.cpu().numpy(), n)
+    raw = (tmp_path / "Fields_k_3.npz").read_bytes()
+    (tmp_path / "Fields_k_3.npz").write_bytes(raw[:100])
+    with pytest.raises(CheckpointError):
+        other.load(tmp_path)
+    big = ForcedDNS.config(32, 0.01, 2e-3, precision="f64")
+    write_outputs(tmp_path, dns.uk_full(), dns.energy_spectrum(), dns.flux_spectrum(), slabs=2)
+    for r in (2, 3):
+        (tmp_path / f"Fields_k_{r}.npz").unlink()
+    with pytest.raises(CheckpointError, match="N = 16"):
+        big.load(tmp_path)
