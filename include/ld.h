@@ -111,6 +111,14 @@ LD_API int ld_rfft_cube(ld_plan* plan, const void* u, void* uk, int ncomp, void*
 /* full -> cube: dealias * full (F:567-569 applies dealias after rfft_mpi); cube -> full. */
 LD_API int ld_spec_to_cube(ld_plan* plan, const void* full, void* cube, int ncomp, void* stream);
 LD_API int ld_spec_from_cube(ld_plan* plan, const void* cube, void* full, int ncomp, void* stream);
+/* The dealiased part of a reference-layout spectrum moved by strided copies, for host state that
+ * stays in the reference's layout (F:158) - host (pinned) or device memory on the full side:
+ *   direction 0: full (ncomp, N, N, N/2+1) -> cube: the rows kz = 0..kc of every (kx, ky) of the
+ *                cube are copied, then the modes outside the mask are zeroed (= ld_spec_to_cube);
+ *   direction 1: cube -> full: the same rows are written; no other element of `full` is touched
+ *                (they stay whatever they were - zeros for a dealiased state).
+ * Four cudaMemcpy3DAsync per component and direction; no counterpart in the reference. */
+LD_API int ld_spec_copy_region(ld_plan* plan, const void* src, void* dst, int ncomp, int direction, void* stream);
 
 /* ---- spectrum and forcing, F:232-275 ------------------------------------------------- */
 /* Shell energy spectrum e3d_to_e1d(0.5 |uk|^2 normalize) (F:232-233, F:243-245) of a cube-layout

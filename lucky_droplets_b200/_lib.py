@@ -44,6 +44,7 @@ SIGNATURES = {
     "ld_rfft_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
     "ld_spec_to_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
     "ld_spec_from_cube": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
+    "ld_spec_copy_region": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_i, _c_p]),
     "ld_shell_spectrum": (_c_i, [_c_p, _c_p, _c_p, _c_p]),
     "ld_velocity_rhs": (_c_i, [_c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_d, _c_p]),
     "ld_rk2if_stage": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, ctypes.POINTER(FlowParams), _c_p]),

@@ -40,11 +40,13 @@ template <typename T> __device__ __forceinline__ vec4<T> mk4(T a, T b, T c, T d)
 }
 
 // Launch shapes by N.  Powers of two: as tuned.  Mixed-radix N = 2^a 3^b 5^c (a >= 3): eight
-// elements per thread in both kinds of pass (stage 0 radix 8), a CTA of 8 columns (64-byte FP32 /
-// 128-byte FP64 row segments; N/8 x 8 threads leave the FP64 update pass, which holds three
-// transformed columns, enough registers), and as many z row units per CTA as fit 256 threads (a
-// power of two, so that N^2 rows split evenly); their rows may span warps, so they exchange with
-// block-wide barriers.
+// elements per thread (stage 0 radix 8) in both kinds of pass; column passes with a CTA of 8
+// columns (64-byte FP32 / 128-byte FP64 row segments; N/8 x 8 threads leave the FP64 update pass,
+// which holds three transformed columns, enough registers); z passes with as many row units per
+// CTA as fit 256 threads (a power of two, so that N^2 rows split evenly); their rows span warps,
+// so they exchange with block-wide barriers.  (Measured at 360^3 in FP64 against four elements
+// per thread, two or three CTAs per SM and a block-pipelined variant with bulk-copy prefetch:
+// this shape was the fastest of them.)
 template <int N> struct Cfg {
   static constexpr bool P2 = is_pow2(N);
   // column passes: E elements per thread, TB columns per CTA
@@ -677,25 +679,31 @@ k_z_r2c(const T* __restrict__ x, cplx<T>* __restrict__ X, long long nrows, int s
 // One row of the fused z pass: C2R of the six y-transformed fields [u, w] (kz < Kin of each row
 // pointer in[f]), optional store of physical u, u x w (F:299-301), R2C of the three products
 // (kz < Mzp stored, zero beyond Kin) into P + f*fs + row*Mzp.
-template <typename T, int N>
+// HOIST: the three pairs are loaded before the first transform (rows read from global memory:
+// one load phase per row instead of three); the pipelined pass reads staged rows and loads each
+// pair just before its transform.
+template <typename T, int N, bool HOIST = false>
 __device__ __forceinline__ void zcross_row(const cplx<T>* const* in, cplx<T>* sb, cplx<T>* P, long long fs,
                                            long long row, T* uphys, int ulayout, int Mzp, int Kin, T s, int j,
                                            const cplx<T>* __restrict__ tw) {
   constexpr int E = Cfg<N>::EZ, NT = Cfg<N>::NTZ;
-  constexpr long long NR = (long long)N * N;
   using Sy = ZSync<N>;
   cplx<T> p0[E], p1[E], p2[E];
   zload_pair<T, N>(p0, in[0], in[1], Kin, j, s);  // pair (u_x, u_y)
+  if constexpr (HOIST) {
+    zload_pair<T, N>(p1, in[2], in[3], Kin, j, s);  // pair (u_z, w_x)
+    zload_pair<T, N>(p2, in[4], in[5], Kin, j, s);  // pair (w_y, w_z)
+  }
   fft_run<T, N, E, true, true>(p0, sb, 1, j, tw, Sy());
   Sy()();
-  zload_pair<T, N>(p1, in[2], in[3], Kin, j, s);  // pair (u_z, w_x)
+  if constexpr (!HOIST) zload_pair<T, N>(p1, in[2], in[3], Kin, j, s);
   fft_run<T, N, E, true, true>(p1, sb, 1, j, tw, Sy());
   Sy()();
-  zload_pair<T, N>(p2, in[4], in[5], Kin, j, s);  // pair (w_y, w_z)
+  if constexpr (!HOIST) zload_pair<T, N>(p2, in[4], in[5], Kin, j, s);
   fft_run<T, N, E, true, true>(p2, sb, 1, j, tw, Sy());
   Sy()();
   if (uphys && ulayout == 0) {  // planar (3, N, N, N)
-    const long long NN3 = NR * N;
+    const long long NN3 = (long long)N * N * N;
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const int n = j + NT * m;
@@ -746,7 +754,7 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
   const cplx<T>* in[6];
 #pragma unroll
   for (int f = 0; f < 6; ++f) in[f] = W + f * fs + row * MZ;
-  zcross_row<T, N>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, j, tw);
+  zcross_row<T, N, !Cfg<N>::P2>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, j, tw);
 }
 
 // Pipelined fused z pass for one warp per row (N >= 256): persistent warps walk the rows with a

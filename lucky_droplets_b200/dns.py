@@ -308,9 +308,11 @@ class ForcedDNS:
         copies the spectrum (and droplet positions/velocities) from host memory, advances
         ``nsteps`` steps and copies the new state back into the same host arrays.  ``layout``:
         "cube" - the dealiased cube (3, Mx, My, Mzp) the step keeps on the device; "full" - the
-        reference's own layout (3, N, N, N/2+1) (F:158), converted on the device (the dealias of
-        F:567-569 on the way in, zeros outside the mask on the way out).  Host tensors should be
-        pinned for asynchronous copies.  Returns the host tensors.
+        reference's own layout (3, N, N, N/2+1) (F:158): only the rows of the dealiased cube move
+        (strided copies), the modes outside the mask are dropped on the way in (the dealias of
+        F:567-569); on the way out the first call for a host array writes all of it (zeros outside
+        the mask), later calls only the cube rows (the rest stays zero unless the caller writes
+        there).  Host tensors should be pinned for asynchronous copies.  Returns the host tensors.
 
         The spectrum is needed by the first kernel, so its copy precedes the step; the droplet
         copies run on a side stream under the first stage's flow transforms (the droplets are
@@ -324,18 +326,20 @@ class ForcedDNS:
         s = torch.cuda.current_stream() if stream is None else stream
         d = self.droplets if pos_host is not None else None
         side = self._copy_streams()
-        full = None
-        if layout == "full":
-            p = self.plan
-            full = getattr(self, "_full", None)
-            if full is None:
-                full = self._full = p.empty_full(3)
+        full = layout == "full"
+        first_out = False
+        if full:
+            clean = getattr(self, "_clean_hosts", None)
+            if clean is None:
+                clean = self._clean_hosts = set()
+            key = (uk_host.data_ptr(), tuple(uk_host.shape))
+            first_out = key not in clean
+            clean.add(key)
         with torch.cuda.stream(s):
-            if full is None:
+            if not full:
                 self.uk.copy_(uk_host, non_blocking=True)
             else:
-                full.copy_(uk_host, non_blocking=True)
-                self.plan.to_cube(full, self.uk, stream=s)
+                self.plan.copy_region_in(uk_host, self.uk, stream=s)
         if d is not None:
             side[0].wait_stream(s)  # earlier users of pos/vel are done before they are overwritten
             with torch.cuda.stream(side[0]):
@@ -346,13 +350,19 @@ class ForcedDNS:
             s.wait_stream(side[0])
 
         def flow_out():
-            src = self.uk
-            if full is not None:
-                self.plan.from_cube(self.uk, full, stream=s)
-                src = full
+            if full and first_out:
+                dev = self.plan.from_cube(self.uk, stream=s)
+                side[1].wait_stream(s)
+                with torch.cuda.stream(side[1]):
+                    uk_host.copy_(dev, non_blocking=True)
+                dev.record_stream(side[1])
+                return
             side[1].wait_stream(s)
             with torch.cuda.stream(side[1]):
-                uk_host.copy_(src, non_blocking=True)
+                if full:
+                    self.plan.copy_region_out(self.uk, uk_host, stream=side[1])
+                else:
+                    uk_host.copy_(self.uk, non_blocking=True)
 
         def droplets_out():
             if d is not None:

@@ -145,6 +145,24 @@ class Plan:
         check(_lib.lib().ld_spec_from_cube(self._h, ptr(cube), ptr(full), nc, stream_ptr(stream)))
         return full
 
+    def copy_region_in(self, full, cube, stream=None):
+        """Cube-layout spectra from reference-layout ones (host pinned or device): only the rows of
+        the dealiased cube are copied, then masked - the result of to_cube."""
+        nc = self._chk(cube, self.cdtype, (self.Mx, self.My, self.Mzp))
+        if full.dtype != self.cdtype or not full.is_contiguous() or tuple(full.shape[-3:]) != (self.N, self.N, self.Nf):
+            raise ValueError(f"expected a contiguous {self.cdtype} (..., N, N, N/2+1) tensor")
+        check(_lib.lib().ld_spec_copy_region(self._h, ptr(full), ptr(cube), nc, 0, stream_ptr(stream)))
+        return cube
+
+    def copy_region_out(self, cube, full, stream=None):
+        """Write the dealiased cube rows of reference-layout spectra (host pinned or device) from
+        cube-layout ones; no other element of `full` is written."""
+        nc = self._chk(cube, self.cdtype, (self.Mx, self.My, self.Mzp))
+        if full.dtype != self.cdtype or not full.is_contiguous() or tuple(full.shape[-3:]) != (self.N, self.N, self.Nf):
+            raise ValueError(f"expected a contiguous {self.cdtype} (..., N, N, N/2+1) tensor")
+        check(_lib.lib().ld_spec_copy_region(self._h, ptr(cube), ptr(full), nc, 1, stream_ptr(stream)))
+        return full
+
     # ---- spectra and RHS ---------------------------------------------------------------------------
     def e3d_to_e1d(self, uk, out=None, stream=None):
         """Shell energy spectrum of a cube-layout 3-vector (FP64, length N/2+1)."""

@@ -114,3 +114,37 @@ def test_unsupported_sizes_are_refused():
     pos = torch.zeros((10, 3), dtype=torch.float64, device="cuda")
     with pytest.raises(LDError, match="power of two"):
         li.infer(u4, pos)
+
+
+@pytest.mark.parametrize("N", [32, 96])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_region_copies_match_layout_conversions(torch, N, prec):
+    """ld_spec_copy_region moves only the dealiased cube rows between a reference-layout spectrum
+    (pinned host or device) and the cube: in, it equals ld_spec_to_cube; out, it writes exactly
+    the cube rows of from_cube and leaves every other element as it was."""
+    p = plan(N, prec)
+    rng = np.random.default_rng(N)
+    shape = (3, N, N, N // 2 + 1)
+    X = torch.as_tensor(rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).to(p.cdtype)
+    ref = p.to_cube(X.cuda())
+    for src in (X.pin_memory(), X.cuda()):
+        got = p.empty_cube(3)
+        got.fill_(1.0)
+        p.copy_region_in(src, got)
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref)
+    full = p.from_cube(ref).cpu()
+    inside = torch.zeros(shape, dtype=torch.bool)
+    kc = p.kc
+    rows = list(range(0, kc + 1)) + list(range(N - kc, N))
+    inside[:, rows[0]:kc + 1, :, :kc + 1] = True
+    inside[:, N - kc:, :, :kc + 1] = True
+    cols = torch.zeros(N, dtype=torch.bool)
+    cols[rows] = True
+    inside &= cols[None, None, :, None]
+    for dst in (torch.full(shape, 7 + 7j, dtype=p.cdtype).pin_memory(), torch.full(shape, 7 + 7j, dtype=p.cdtype).cuda()):
+        p.copy_region_out(ref, dst)
+        torch.cuda.synchronize()
+        d = dst.cpu()
+        assert torch.equal(d[inside], full[inside])
+        assert bool((d[~inside] == 7 + 7j).all())
