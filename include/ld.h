@@ -83,6 +83,13 @@ LD_API const char* ld_last_error(void);
  * divide, F:27-29, F:52-57).  The learned interpolation (ld_mlp_infer, ld_mlp_samples) needs a
  * power of two. */
 LD_API int ld_plan_create(ld_plan** plan, int n, int precision);
+/* A plan for nbox independent boxes of the same grid (no counterpart in the reference, which runs
+ * one box per job): every stage call (ld_rk2if_stage, ld_rk4_stage, ld_velocity_rhs,
+ * ld_step_epilogue_plane0) then advances all boxes, each pass one launch over all of them, on
+ * states laid out (nbox, 3, Mx, My, Mzp) with physical velocities (nbox, N, N, N, 4); the forcing
+ * factors are per box.  The transform workspace grows with nbox.  nbox = 1 is ld_plan_create. */
+LD_API int ld_plan_create_boxes(ld_plan** plan, int n, int precision, int nbox);
+LD_API int ld_plan_boxes(const ld_plan* plan, int32_t* nbox);
 LD_API int ld_plan_destroy(ld_plan* plan);
 /* dims[0..7] = N, kc, Mx, My, Mz, Mzp, Nf, precision; work_bytes = transform workspace. */
 LD_API int ld_plan_dims(const ld_plan* plan, int32_t* dims, size_t* work_bytes);
@@ -208,6 +215,12 @@ LD_API int ld_gather(ld_plan* plan, const void* field, int ncomp, const double* 
 LD_API int ld_droplet_stage(ld_plan* plan, int stage, const void* u, double* pos, void* vel,
                      const void* tau, void* a1, int64_t n, int method, double h, double g,
                      void* stream);
+/* The same for the droplets of all boxes of a multi-box plan in one launch: droplet i belongs to
+ * box[i] (int32) and samples that box's velocity u + box[i] N^3 (interleaved (nbox, N, N, N, 4)).
+ * No counterpart in the reference. */
+LD_API int ld_droplet_stage_boxes(ld_plan* plan, int stage, const void* u, const int32_t* box, double* pos,
+                                  void* vel, const void* tau, void* a1, int64_t n, int method, double h, double g,
+                                  void* stream);
 
 /* ---- exact spectral velocity (no counterpart in the reference) ------------------------- */
 /* u_c(x) = (1/N^3) sum_k w_kz Re(uk_c(k) exp(i k.x)) over the modes of the spherical mask of a
@@ -296,6 +309,10 @@ LD_API int ld_deposit_pull(const uint32_t* sval, const int32_t* cs, const double
 /* A collider owns the workspace of the cell-list search for up to nmax droplets on an
  * nc x nc x nc cell grid (nc = floor(L / cell_size), cell_size >= 2 * max radius, nc >= 1). */
 LD_API int ld_collider_create(ld_collider** collider, int64_t nmax, int32_t nc);
+/* A collider for the droplets of nbox independent boxes (each an nc^3 cell grid of the same side
+ * L; no counterpart in the reference): cells are keyed box-major, so one sort and one search
+ * cover every box and pairs never cross boxes.  Use ld_collide_boxes / ld_cell_order_boxes. */
+LD_API int ld_collider_create_boxes(ld_collider** collider, int64_t nmax, int32_t nc, int32_t nbox);
 LD_API int ld_collider_destroy(ld_collider* collider);
 /* Colliding pairs of n droplets, pos (n,3) double, radius (n) double, in a periodic box of side L:
  * wrapped positions, cell = min(int(p / (L/nc)), nc-1) per axis, minimum-image FP64 distance
@@ -306,6 +323,12 @@ LD_API int ld_collider_destroy(ld_collider* collider);
  * in the collider's status word (ld_collider_status). */
 LD_API int ld_collide(ld_collider* collider, const double* pos, const double* radius, int64_t n, double L,
                       int32_t* pairs, int64_t cap, int64_t* count, void* stream);
+/* ld_collide over the droplets of all boxes: droplet i lies in box[i] (int32, < nbox); pairs as
+ * ld_collide (array indices; both droplets of a pair in one box), in box order; box_counts
+ * (nullable, int64 [nbox], device) receives the pairs of every box. */
+LD_API int ld_collide_boxes(ld_collider* collider, const double* pos, const double* radius, const int32_t* box,
+                            int64_t n, double L, int32_t* pairs, int64_t cap, int64_t* count, int64_t* box_counts,
+                            void* stream);
 LD_API int ld_collider_status(ld_collider* collider, uint32_t* flags, int clear, void* stream);
 /* Record this collider's launches in the event trace of `plan` (ld_profile); NULL stops. */
 LD_API int ld_collider_trace(ld_collider* collider, ld_plan* plan);
@@ -316,6 +339,9 @@ LD_API int ld_collider_sorted(ld_collider* collider, const uint32_t** keys, cons
  * collider's grid, ties by index): the permutation that keeps droplet gathers local in memory. */
 LD_API int ld_cell_order(ld_collider* collider, const double* pos, int64_t n, double L, uint32_t* order,
                          void* stream);
+/* The same order over the droplets of all boxes (box major, then cell, then index). */
+LD_API int ld_cell_order_boxes(ld_collider* collider, const double* pos, const int32_t* box, int64_t n, double L,
+                               uint32_t* order, void* stream);
 /* dst row i = src row order[i] for n rows of row_bytes bytes (a multiple of 4); src != dst.  Applies
  * a droplet permutation to every per-droplet array (the reference's send(), P:233-275, reorders the
  * droplets the same way and tracks them by prtclid). */

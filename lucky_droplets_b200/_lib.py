@@ -35,6 +35,9 @@ SIGNATURES = {
     "ld_version": (_c_i, []),
     "ld_last_error": (ctypes.c_char_p, []),
     "ld_plan_create": (_c_i, [ctypes.POINTER(_c_p), _c_i, _c_i]),
+    "ld_plan_create_boxes": (_c_i, [ctypes.POINTER(_c_p), _c_i, _c_i, _c_i]),
+    "ld_plan_boxes": (_c_i, [_c_p, ctypes.POINTER(_c_i32)]),
+    "ld_droplet_stage_boxes": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_i, _c_d, _c_d, _c_p]),
     "ld_plan_destroy": (_c_i, [_c_p]),
     "ld_plan_dims": (_c_i, [_c_p, ctypes.POINTER(_c_i32), ctypes.POINTER(ctypes.c_size_t)]),
     "ld_rfft_mpi": (_c_i, [_c_p, _c_p, _c_p, _c_i, _c_p]),
@@ -92,6 +95,9 @@ SIGNATURES = {
     "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_mlp_adam": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_float, _c_p, _c_p]),
     "ld_collider_create": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32]),
+    "ld_collider_create_boxes": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32, _c_i32]),
+    "ld_collide_boxes": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_i64, _c_p, _c_p, _c_p]),
+    "ld_cell_order_boxes": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_p]),
     "ld_collider_destroy": (_c_i, [_c_p]),
     "ld_collide": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_i64, _c_p, _c_p]),
     "ld_collider_status": (_c_i, [_c_p, ctypes.POINTER(ctypes.c_uint32), _c_i, _c_p]),

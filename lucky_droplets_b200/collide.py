@@ -17,17 +17,21 @@ def _torch():
 class Collider:
     """Workspace for the collision search of up to ``nmax`` droplets with cells >= cell_size."""
 
-    def __init__(self, nmax, cell_size, L=TWO_PI, device=None):
+    def __init__(self, nmax, cell_size, L=TWO_PI, device=None, nbox=1):
+        """nbox > 1: one collider for the droplets of nbox independent boxes of side L (cells keyed
+        box-major; collide_boxes / cell_order_boxes take each droplet's box)."""
         torch = _torch()
         self.L = float(L)
         self.nc = max(1, int(math.floor(self.L / float(cell_size))))
         self.nmax = int(nmax)
+        self.nbox = int(nbox)
         self.device = torch.device(device if device is not None else "cuda")
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
-            check(_lib.lib().ld_collider_create(ctypes.byref(h), self.nmax, self.nc))
+            check(_lib.lib().ld_collider_create_boxes(ctypes.byref(h), self.nmax, self.nc, self.nbox))
         self._h = h
         self.count = torch.zeros(1, dtype=torch.int64, device=self.device)
+        self.box_counts = torch.zeros(self.nbox, dtype=torch.int64, device=self.device)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -63,6 +67,20 @@ class Collider:
         if order is None:
             order = torch.empty(n, dtype=torch.int32, device=self.device)
         check(_lib.lib().ld_cell_order(self._h, ptr(pos), n, self.L, ptr(order), stream_ptr(stream)))
+        return order
+
+    def collide_boxes(self, pos, radius, box, pairs, stream=None):
+        """Pairs of the droplets of every box (array indices, i < j, box order) into ``pairs``;
+        the total in ``self.count``, the pairs per box in ``self.box_counts`` (on the device)."""
+        n = int(pos.shape[0])
+        check(_lib.lib().ld_collide_boxes(self._h, ptr(pos), ptr(radius), ptr(box), n, self.L, ptr(pairs),
+                                          int(pairs.shape[0]), ptr(self.count), ptr(self.box_counts),
+                                          stream_ptr(stream)))
+
+    def cell_order_boxes(self, pos, box, order, stream=None):
+        """Permutation (int32) into (box, cell) order."""
+        check(_lib.lib().ld_cell_order_boxes(self._h, ptr(pos), ptr(box), int(pos.shape[0]), self.L, ptr(order),
+                                             stream_ptr(stream)))
         return order
 
     def status(self, clear=True, stream=None):

@@ -37,25 +37,32 @@ __device__ __forceinline__ int cell_of(double p, double cw, int nc) {
   return c < nc - 1 ? c : nc - 1;
 }
 
+// Cell keys of a multi-box collider: box b's cells come after those of boxes 0..b-1 (box = null:
+// one box).
+__device__ __forceinline__ unsigned box_base(const int* __restrict__ box, long long i, int nc) {
+  return box ? (unsigned)box[i] * (unsigned)nc * (unsigned)nc * (unsigned)nc : 0u;
+}
+
 __global__ void k_cell_keys(const double* __restrict__ pos, long long n, double L, double cw, int nc,
-                            unsigned* __restrict__ key, unsigned* __restrict__ val) {
+                            unsigned* __restrict__ key, unsigned* __restrict__ val, const int* __restrict__ box) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int cx = cell_of(wrapL(pos[3 * i], L), cw, nc);
     const int cy = cell_of(wrapL(pos[3 * i + 1], L), cw, nc);
     const int cz = cell_of(wrapL(pos[3 * i + 2], L), cw, nc);
-    key[i] = (unsigned)((cx * nc + cy) * nc + cz);
+    key[i] = box_base(box, i, nc) + (unsigned)((cx * nc + cy) * nc + cz);
     val[i] = (unsigned)i;
   }
 }
 
 // ---- counting sort by cell (the sort of ld_collide) -------------------------------------------
 __global__ void k_cell_count(const double* __restrict__ pos, long long n, double L, double cw, int nc,
-                             unsigned* __restrict__ key, unsigned* __restrict__ rank, unsigned* __restrict__ occ) {
+                             unsigned* __restrict__ key, unsigned* __restrict__ rank, unsigned* __restrict__ occ,
+                             const int* __restrict__ box) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int cx = cell_of(wrapL(pos[3 * i], L), cw, nc);
     const int cy = cell_of(wrapL(pos[3 * i + 1], L), cw, nc);
     const int cz = cell_of(wrapL(pos[3 * i + 2], L), cw, nc);
-    const unsigned k = (unsigned)((cx * nc + cy) * nc + cz);
+    const unsigned k = box_base(box, i, nc) + (unsigned)((cx * nc + cy) * nc + cz);
     key[i] = k;
     rank[i] = atomicAdd(&occ[k], 1u);  // arrival order: unordered
   }
@@ -302,8 +309,10 @@ __global__ void k_pairs(const double4* __restrict__ sp, const unsigned* __restri
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const double4 me = sp[s];
     const unsigned id = sval[s];
+    const int nc3 = nc * nc * nc;
     const int key = (int)skey[s];
-    const int cz = key % nc, cy = (key / nc) % nc, cx = key / (nc * nc);
+    const int kb = (key / nc3) * nc3;  // the box's first cell
+    const int cz = key % nc, cy = (key / nc) % nc, cx = (key / (nc * nc)) % nc;
     unsigned c = 0;
     long long o = 0, o_end = 0;
     if (MODE == 1) { o = off[id]; o_end = o + (off[id + 1] - off[id]); }
@@ -314,7 +323,7 @@ __global__ void k_pairs(const double4* __restrict__ sp, const unsigned* __restri
       for (int b = -1; b <= 1; ++b)
         for (int d = -1; d <= 1; ++d) {
           const int nx = (cx + a + nc) % nc, ny = (cy + b + nc) % nc, nz = (cz + d + nc) % nc;
-          const int nk = (nx * nc + ny) * nc + nz;
+          const int nk = kb + (nx * nc + ny) * nc + nz;
           if (DEDUP) {
             bool dup = false;
             for (int q = 0; q < ns; ++q) dup |= seen[q] == nk;
@@ -436,7 +445,8 @@ __device__ __forceinline__ void col_visit(int i, int t, const double4* __restric
   cnt[i] = c;
 }
 
-__global__ void __launch_bounds__(COL_THREADS)
+template <int CT>  // threads per block: fewer for sparse columns (a multi-box collider's small boxes)
+__global__ void __launch_bounds__(CT)
 k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
             const int* __restrict__ cs, int nc, int parts, double L, int cap_smem, unsigned* __restrict__ cnt,
             int* __restrict__ scr) {
@@ -446,19 +456,22 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
   __shared__ long long kq[5];
   __shared__ int lo[5], so[6], dl[5];
   __shared__ float shx[5], shy[5];
-  const long long col = blockIdx.x / parts;
+  const long long colg = blockIdx.x / parts;  // (box, cx, cy) of a multi-box collider
   const int part = (int)(blockIdx.x % parts);
+  const long long ncol = (long long)nc * nc;
+  const long long bbase = (colg / ncol) * ncol * nc;  // the box's first cell
+  const long long col = colg % ncol;
   const int cx = (int)(col / nc), cy = (int)(col % nc);
   const float Lf = (float)L, margin = (float)(1e-6 * L);
   if (threadIdx.x < 5) {
     int ox, oy;
     col_offset(threadIdx.x, ox, oy);
-    kq[threadIdx.x] = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
+    kq[threadIdx.x] = bbase + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
     shx[threadIdx.x] = (cx + ox >= nc) ? -Lf : 0.f;
     shy[threadIdx.x] = (cy + oy >= nc) ? -Lf : ((cy + oy < 0) ? Lf : 0.f);
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < 5 * (nc + 1); e += COL_THREADS) {
+  for (int e = threadIdx.x; e < 5 * (nc + 1); e += CT) {
     const int q = e / (nc + 1), z = e - q * (nc + 1);
     cst[e] = cs[kq[q] + z];
   }
@@ -478,12 +491,12 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
   if (staged) {
     for (int q = 0; q < 5; ++q) {
       const int n_q = so[q + 1] - so[q];
-      for (int t = threadIdx.x; t < n_q; t += COL_THREADS) colbuf[so[q] + t] = spf[lo[q] + t];
+      for (int t = threadIdx.x; t < n_q; t += CT) colbuf[so[q] + t] = spf[lo[q] + t];
     }
   }
   __syncthreads();
   const int len0 = so[1] - so[0];
-  for (int t = part * COL_THREADS + threadIdx.x; t < len0; t += parts * COL_THREADS) {
+  for (int t = part * CT + threadIdx.x; t < len0; t += parts * CT) {
     const int i = lo[0] + t;
     const int cz = (int)(skey[i] - (unsigned)kq[0]);
     if (staged) col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, Lf, margin, cnt, scr);
@@ -508,7 +521,9 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
       continue;
     }
     const unsigned key = skey[i];
-    const int cz = (int)(key % (unsigned)nc), cy = (int)((key / nc) % nc), cx = (int)(key / ((unsigned)nc * nc));
+    const unsigned nc3 = (unsigned)nc * nc * nc;
+    const long long kb = (long long)(key / nc3) * nc3;  // the box's first cell
+    const int cz = (int)(key % (unsigned)nc), cy = (int)((key / nc) % nc), cx = (int)((key / ((unsigned)nc * nc)) % nc);
     const float4 mf = spf[i];
     const float mar = margin + 1e-6f * mf.w;
     const double4 me = sp[i];
@@ -520,7 +535,7 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
       const int z = (cz + dz + nc) % nc;
       const int ox = q < 2 ? 0 : 1;
       const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
-      const long long k = ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc + z;
+      const long long k = kb + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc + z;
       const int g1 = cs[k + 1];
       for (int g = r == 0 ? i + 1 : cs[k]; g < g1; ++g) {
         if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
@@ -540,6 +555,23 @@ __global__ void k_map_pairs(const unsigned* __restrict__ total, long long cap, c
     const int a = (int)sval[pairs[2 * e]], b = (int)sval[pairs[2 * e + 1]];
     pairs[2 * e] = a < b ? a : b;
     pairs[2 * e + 1] = a < b ? b : a;
+  }
+}
+
+// Pairs per box, sorted order (nc >= 3: the pairs of sorted droplet s are counted at off[s], and
+// box b's droplets are the sorted slots start[b nc^3] .. start[(b + 1) nc^3] - 1).
+__global__ void k_box_counts_sorted(const unsigned* __restrict__ off, const int* __restrict__ start, long long nc3,
+                                    int nbox, int64_t* __restrict__ bc) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nbox; b += gridDim.x * blockDim.x)
+    bc[b] = (int64_t)off[start[(b + 1) * nc3]] - (int64_t)off[start[b * nc3]];
+}
+
+// Pairs per box, droplet order (nc < 3: counts are indexed by droplet); bc zeroed before.
+__global__ void k_box_counts_ids(const unsigned* __restrict__ off, const int* __restrict__ box, long long n,
+                                 int64_t* __restrict__ bc) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned c = off[i + 1] - off[i];
+    if (c) atomicAdd(reinterpret_cast<unsigned long long*>(bc + (box ? box[i] : 0)), (unsigned long long)c);
   }
 }
 
@@ -572,6 +604,7 @@ inline int gridn(long long n, int th) {
 struct ld_collider {
   long long nmax = 0;
   int nc = 0;
+  int nbox = 1;  // boxes of a multi-box collider: cells (box, cx, cy, cz), box major
   unsigned *key = nullptr, *val = nullptr, *key2 = nullptr, *val2 = nullptr, *hist = nullptr, *cnt = nullptr;
   int* start = nullptr;  // cell starts, ncell + 1 entries
   double4* sp = nullptr;
@@ -602,16 +635,20 @@ int scan_u32(ld_collider* c, unsigned* a, long long m, cudaStream_t s) {
 
 extern "C" {
 
-int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) {
-  if (!out || nmax < 1 || nmax > (1LL << 31) - 2 || nc < 1 || (long long)nc * nc * nc > (1LL << 31))
+int ld_collider_create(ld_collider** out, int64_t nmax, int32_t nc) { return ld_collider_create_boxes(out, nmax, nc, 1); }
+
+int ld_collider_create_boxes(ld_collider** out, int64_t nmax, int32_t nc, int32_t nbox) {
+  if (!out || nmax < 1 || nmax > (1LL << 31) - 2 || nc < 1 || nbox < 1 ||
+      (long long)nc * nc * nc * nbox > (1LL << 31) - 2)
     return ld_fail(LD_ERR_ARG, "ld_collider_create: bad arguments");
   *out = nullptr;
   ld_collider* c = new (std::nothrow) ld_collider();
   if (!c) return ld_fail(LD_ERR_NOMEM, "host allocation failed");
   c->nmax = nmax;
   c->nc = nc;
+  c->nbox = nbox;
   c->nblocks = (int)((nmax + RS_TILE - 1) / RS_TILE);
-  const long long ncell = (long long)nc * nc * nc;
+  const long long ncell = (long long)nc * nc * nc * nbox;
   cudaError_t e = cudaSuccess;
   auto A = [&](void** p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
   A((void**)&c->key, 4 * nmax);
@@ -677,13 +714,21 @@ int ld_radix_sort_u32(ld_collider* c, unsigned* key, unsigned* val, int64_t n, i
 
 int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t n, double L, int32_t* pairs,
                int64_t cap, int64_t* count, void* stream) {
+  if (c && c->nbox != 1) return ld_fail(LD_ERR_ARG, "ld_collide: a multi-box collider needs ld_collide_boxes");
+  return ld_collide_boxes(c, pos, radius, nullptr, n, L, pairs, cap, count, nullptr, stream);
+}
+
+int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, const int32_t* box, int64_t n, double L,
+                     int32_t* pairs, int64_t cap, int64_t* count, int64_t* box_counts, void* stream) {
   if (!c || !count || n < 0 || n > c->nmax || cap < 0 || !(L > 0) || (n > 0 && (!pos || !radius)) ||
-      (n > 0 && cap > 0 && !pairs))
+      (n > 0 && cap > 0 && !pairs) || (c->nbox > 1 && n > 0 && !box))
     return ld_fail(LD_ERR_ARG, "ld_collide: bad arguments");
   cudaStream_t s = (cudaStream_t)stream;
   const int nc = c->nc;
   const double cw = L / nc;
-  const long long ncell = (long long)nc * nc * nc;
+  const long long nc3 = (long long)nc * nc * nc;
+  const long long ncell = nc3 * c->nbox;
+  if (box_counts) LD_CUDA_CHECK(cudaMemsetAsync(box_counts, 0, sizeof(int64_t) * c->nbox, s));
   if (n == 0) {
     LD_CUDA_CHECK(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
     return LD_OK;
@@ -692,7 +737,7 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
     ProfScope ps(c->trace, KID_COLL_SORT, s);
     if (ncell + 1 > (long long)SCAN_TILE * SCAN_TILE) {
       // more cells than one scan handles: stable radix sort of the keys, starts by binary search
-      k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val);
+      k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val, box);
       int bits = 1;
       while ((1LL << bits) < ncell) ++bits;
       if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
@@ -706,7 +751,7 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
       unsigned* occ = reinterpret_cast<unsigned*>(c->start);
       LD_CUDA_CHECK(cudaMemsetAsync(occ, 0, sizeof(unsigned) * (size_t)(ncell + 1), s));
       LD_CUDA_CHECK(cudaMemsetAsync(c->nbig, 0, sizeof(unsigned), s));
-      k_cell_count<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key2, c->val2, occ);
+      k_cell_count<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key2, c->val2, occ, box);
       if (int rc = scan_u32(c, occ, ncell + 1, s)) return rc;
       k_cell_scatter<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->val2, c->start, n, c->cnt);
       k_cell_place<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->start, c->cnt, n, pos, radius, L, c->val, c->key, c->sp,
@@ -720,7 +765,7 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
   if (nc >= 3) {
     // block per cell column (and part); pairs come out as sorted-array indices and are mapped
     // back to droplet indices by k_map_pairs
-    const long long ncol = (long long)nc * nc;
+    const long long ncol = (long long)nc * nc * c->nbox;  // cell columns of every box
     const long long per_col = (n + ncol - 1) / ncol;
     const long long parts = per_col > 512 ? (per_col + 511) / 512 : 1;
     const size_t starts_bytes = sizeof(int) * 5 * (size_t)(nc + 1);
@@ -732,13 +777,28 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
     if (want > room) want = room;
     const int cap_smem = (int)want;
     const size_t smem = sizeof(float4) * (size_t)cap_smem + starts_bytes;
-    LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_col_pairs<<<(unsigned)(ncol * parts), COL_THREADS, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts,
-                                                                    L, cap_smem, c->cnt, c->scr);
+    // blocks of 64 or 128 threads where columns hold few droplets (as the boxes of an ensemble
+    // do), 256 otherwise
+    if (per_col <= 64) {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_col_pairs<64><<<(unsigned)(ncol * parts), 64, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
+                                                                 cap_smem, c->cnt, c->scr);
+    } else if (per_col <= 128) {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_col_pairs<128><<<(unsigned)(ncol * parts), 128, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
+                                                                   cap_smem, c->cnt, c->scr);
+    } else {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<COL_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem));
+      k_col_pairs<COL_THREADS><<<(unsigned)(ncol * parts), COL_THREADS, smem, s>>>(
+          c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem, c->cnt, c->scr);
+    }
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
     k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, n, c->cnt, c->scr, pairs,
                                                cap);
     k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + n, cap, c->val, pairs);
+    if (box_counts)
+      k_box_counts_sorted<<<(c->nbox + 255) / 256, 256, 0, s>>>(c->cnt, c->start, nc3, c->nbox, box_counts);
   } else {
     const int* end = c->start + 1;  // end of cell k = start of cell k + 1
     k_pairs<0, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, end, n, nc, L, c->cnt,
@@ -746,6 +806,7 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
     k_pairs<1, true><<<gridn(n, 128), 128, 0, s>>>(c->sp, c->val, c->key, c->start, end, n, nc, L, nullptr,
                                                    c->cnt, pairs, cap);
+    if (box_counts) k_box_counts_ids<<<gridn(n, 256), 256, 0, s>>>(c->cnt, box, n, box_counts);
   }
   k_finish<<<1, 1, 0, s>>>(c->cnt, n, cap, count, c->status);
   LD_LAUNCH_CHECK();
@@ -753,14 +814,20 @@ int ld_collide(ld_collider* c, const double* pos, const double* radius, int64_t 
 }
 
 int ld_cell_order(ld_collider* c, const double* pos, int64_t n, double L, uint32_t* order, void* stream) {
-  if (!c || n < 0 || n > c->nmax || !(L > 0) || (n > 0 && (!pos || !order)))
+  if (c && c->nbox != 1) return ld_fail(LD_ERR_ARG, "ld_cell_order: a multi-box collider needs ld_cell_order_boxes");
+  return ld_cell_order_boxes(c, pos, nullptr, n, L, order, stream);
+}
+
+int ld_cell_order_boxes(ld_collider* c, const double* pos, const int32_t* box, int64_t n, double L, uint32_t* order,
+                        void* stream) {
+  if (!c || n < 0 || n > c->nmax || !(L > 0) || (n > 0 && (!pos || !order)) || (c->nbox > 1 && n > 0 && !box))
     return ld_fail(LD_ERR_ARG, "ld_cell_order: bad arguments");
   if (n == 0) return LD_OK;
   cudaStream_t s = (cudaStream_t)stream;
   ProfScope ps(c->trace, KID_CELL_ORDER, s);
   const int nc = c->nc;
-  const long long ncell = (long long)nc * nc * nc;
-  k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, L / nc, nc, c->key, c->val);
+  const long long ncell = (long long)nc * nc * nc * c->nbox;
+  k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, L / nc, nc, c->key, c->val, box);
   int bits = 1;
   while ((1LL << bits) < ncell) ++bits;
   if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;

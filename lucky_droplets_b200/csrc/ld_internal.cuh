@@ -42,6 +42,7 @@ struct ProfRec {
 
 struct ld_plan {
   int N, kc, Mx, My, Mz, Mzp, Nf, prec;
+  int nbox = 1;          // boxes of a multi-box plan (ld_plan_create_boxes): states (nbox, 3, cube)
   size_t esz;            // bytes per real element
   void* tw = nullptr;    // N complex twiddles exp(-2 pi i p / N)
   void* ifac = nullptr;  // exp(-nu h k^2) by k^2 (plan precision)
@@ -96,7 +97,7 @@ struct OpsTable {
   int (*gather)(ld_plan*, const void* f, int ncomp, const double* pos, long long n, int method, void* out,
                 cudaStream_t);
   int (*dstage)(ld_plan*, int stage, int method, const void* u, double* pos, void* vel, const void* tau,
-                void* a1, long long n, double h, double g, cudaStream_t);
+                void* a1, long long n, double h, double g, const int* box, cudaStream_t);
   // times every launch variant of the y passes (ms[2][4]: one-shot, pipelined with 1..3 CTAs/SM)
   // and keeps the fastest in the plan
   int (*autotune)(ld_plan*, cudaStream_t, double* ms);

@@ -152,11 +152,12 @@ template <typename T, int N> struct LdCurl {
   const cplx<T>* u;
   long long cs;  // component stride (cube elements)
   int kc_, My_, Mzp_;  // the plan's cube; equal to Cfg<N>::KC, MY, MZP, which the loader uses
+  long long bs;  // box stride (elements): the outer index is the box of a multi-box plan
   static constexpr int kc = Cfg<N>::KC, My = Cfg<N>::MY, Mzp = Cfg<N>::MZP;
-  __device__ __forceinline__ cplx<T> operator()(int f, int, int n, int col) const {
+  __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
     const int r = crow(n, N, kc);
     if (r < 0) return czero<cplx<T>>();
-    const long long b = (long long)r * My * Mzp + col;
+    const long long b = (long long)o * bs + (long long)r * My * Mzp + col;
     if (f < 3) return u[f * cs + b];
     const T kx = T(n <= kc ? n : n - N);
     const int iy = col / Mzp;
@@ -347,6 +348,10 @@ template <typename T> struct UpdArgs {
   // and the non-finite / blow-up checks, as k_epilogue does them) is done here, so that the
   // epilogue that follows needs only the kz = 0 plane (k_epilogue_plane0)
   T blowup;
+  // multi-box plans: blockIdx.y is the box; strides of nl, of the cube states and of the forcing
+  // factors from one box to the next
+  long long nl_bs, cube_bs;
+  int fac_bs;
 };
 
 // The step epilogue of one kz > 0 mode (k_epilogue's arithmetic): projection with its own k
@@ -375,6 +380,15 @@ __global__ void __launch_bounds__(Cfg<N>::COL_THREADS, (N == 256 && sizeof(T) ==
 k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
   constexpr int E = Cfg<N>::EC, TB = Cfg<N>::TB, NT = Cfg<N>::NTC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (blockIdx.y) {  // box of a multi-box plan
+    const long long bo = blockIdx.y;
+    A.nl += bo * A.nl_bs;
+    if (A.s0) A.s0 += bo * A.cube_bs;
+    if (A.s1) A.s1 += bo * A.cube_bs;
+    if (A.s2) A.s2 += bo * A.cube_bs;
+    if (A.s3) A.s3 += bo * A.cube_bs;
+    A.factor += bo * A.fac_bs;
+  }
   cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
   const int c = threadIdx.x % TB, j = threadIdx.x / TB;
   const int col = blockIdx.x * TB + c;
@@ -739,14 +753,13 @@ __device__ __forceinline__ void zcross_row(const cplx<T>* const* in, cplx<T>* sb
 template <typename T, int N>
 __global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
 k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
-          int kc, T s, const cplx<T>* __restrict__ tw) {
+          int kc, T s, const cplx<T>* __restrict__ tw, long long NR) {
   constexpr int NT = Cfg<N>::NTZ;
-  constexpr long long NR = (long long)N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* sbuf = reinterpret_cast<cplx<T>*>(smem_raw);
   const int unit = threadIdx.x / NT, j = threadIdx.x % NT;
   cplx<T>* sb = sbuf + unit * Cfg<N>::ZBUF;
-  const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR exactly
+  const long long row = (long long)blockIdx.x * Cfg<N>::ZROWS + unit;  // grid covers NR (rows per field) exactly
   (void)Mzp;
   (void)kc;
   constexpr int MZ = Cfg<N>::MZP, KIN = Cfg<N>::KC + 1;  // the plan's cube (checked at launch)
@@ -754,7 +767,7 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
   const cplx<T>* in[6];
 #pragma unroll
   for (int f = 0; f < 6; ++f) in[f] = W + f * fs + row * MZ;
-  zcross_row<T, N, !Cfg<N>::P2>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, j, tw);
+  zcross_row<T, N, true>(in, sb, P, fs, row, uphys, ulayout, MZ, KIN, s, j, tw);
 }
 
 // Pipelined fused z pass for one warp per row (N >= 256): persistent warps walk the rows with a
@@ -772,9 +785,8 @@ template <typename T, int N>
 __global__ void __launch_bounds__(256)
 k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
                int kc, T s, const cplx<T>* __restrict__ tw, unsigned* status, unsigned wait_limit,
-               int stall) {
+               int stall, long long NR) {
   static_assert(Cfg<N>::NTZ == 32, "one warp per row");
-  constexpr long long NR = (long long)N * N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   (void)Mzp;
@@ -885,8 +897,11 @@ __global__ void k_from_cube(const cplx<T>* __restrict__ cube, cplx<T>* __restric
 template <typename T>
 __global__ void k_shell_sum(const cplx<T>* __restrict__ u, long long cs, const int* __restrict__ off,
                             const int* __restrict__ idx, int Mzp, int shell0,
-                            double norm0, double* __restrict__ out, double f0, int as_factor) {
+                            double norm0, double* __restrict__ out, double f0, int as_factor, long long ubs = 0,
+                            int obs = 0) {
   __shared__ double red[256];
+  u += blockIdx.y * ubs;  // box of a multi-box plan
+  out += blockIdx.y * obs;
   const int s = shell0 + blockIdx.x;
   double acc = 0.0;
   for (int t = off[s] + threadIdx.x; t < off[s + 1]; t += blockDim.x) {
@@ -923,6 +938,7 @@ __global__ void k_shell_sum(const cplx<T>* __restrict__ u, long long cs, const i
 template <typename T>
 __global__ void k_epilogue(cplx<T>* __restrict__ u, long long cs, int kc, int My, int Mzp,
                            T blowup, unsigned* status) {
+  u += blockIdx.y * 3 * cs;  // box of a multi-box plan
   const long long total = (long long)My * My * Mzp;
   unsigned flags = 0;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
@@ -994,6 +1010,7 @@ __global__ void k_epilogue(cplx<T>* __restrict__ u, long long cs, int kc, int My
 template <typename T>
 __global__ void k_epilogue_plane0(cplx<T>* __restrict__ u, long long cs, int kc, int My, int Mzp, T blowup,
                                   unsigned* status) {
+  u += blockIdx.y * 3 * cs;  // box of a multi-box plan
   const long long total = (long long)My * My;
   unsigned flags = 0;
   for (long long e2 = blockIdx.x * (long long)blockDim.x + threadIdx.x; e2 < total; e2 += (long long)gridDim.x * blockDim.x) {
@@ -1200,10 +1217,12 @@ __global__ void k_gather4(const vec4<T>* __restrict__ f, int N, double L, const 
 }
 
 template <typename T, int METHOD, int STAGE>
-__global__ void k_droplet_stage(const vec4<T>* __restrict__ u, int N, double L, double* __restrict__ pos,
+__global__ void k_droplet_stage(const vec4<T>* __restrict__ u0, int N, double L, double* __restrict__ pos,
                                 T* __restrict__ vel, const T* __restrict__ tau, T* __restrict__ a1,
-                                long long n, double h, T g) {
+                                long long n, double h, T g, const int* __restrict__ box = nullptr) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    // the droplet's box of a multi-box plan: its field is box (N, N, N, 4) further on
+    const vec4<T>* u = box ? u0 + (long long)box[i] * N * N * N : u0;
     const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
     const T vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
     const T it = T(1) / tau[i];

@@ -192,8 +192,9 @@ template <typename T, int N> struct Ops {
     if (prm->kf_hi < prm->kf_lo || prm->f0 == 0.0) return LD_OK;
     ProfScope ps(p, KID_FORCING, s);
     const double norm0 = std::pow(2.0 * M_PI, 3) / std::pow((double)N, 6);
-    k_shell_sum<T><<<prm->kf_hi - prm->kf_lo + 1, 256, 0, s>>>(y, p->cube_elems(), p->shell_off, p->shell_idx,
-                                                               p->Mzp, prm->kf_lo, norm0, p->factor, prm->f0, 1);
+    dim3 grid((unsigned)(prm->kf_hi - prm->kf_lo + 1), (unsigned)p->nbox);
+    k_shell_sum<T><<<grid, 256, 0, s>>>(y, p->cube_elems(), p->shell_off, p->shell_idx, p->Mzp, prm->kf_lo, norm0,
+                                        p->factor, prm->f0, 1, 3 * p->cube_elems(), p->Nf);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
@@ -216,7 +217,7 @@ template <typename T, int N> struct Ops {
   // ---- pipelined fused z pass (one warp per row) -------------------------------------------------
   static int zcross_pipe(ld_plan* p, const C* W2, C* W1, T* uout, int ulayout, T sc, cudaStream_t s) {
     constexpr int WARPS = sizeof(T) == 4 ? 8 : 4;
-    const long long NN = (long long)N * N;
+    const long long NN = (long long)N * N * p->nbox;  // rows per field, all boxes
     const size_t smem = (size_t)WARPS * ((size_t)12 * p->Mzp + Cfg<N>::ZBUF) * sizeof(C) + 24 * WARPS;
     auto k = k_z_cross_pipe<T, N>;
     if (int rc = set_smem(k, smem)) return rc;
@@ -234,7 +235,7 @@ template <typename T, int N> struct Ops {
     const long long need = (NN + WARPS - 1) / WARPS;
     if (grid > need) grid = need;
     k<<<(unsigned)grid, WARPS * 32, smem, s>>>(W2, W1, uout, ulayout, p->Mzp, p->kc, sc, (const C*)p->tw, p->status,
-                                               p->wait_limit, p->wait_stall);
+                                               p->wait_limit, p->wait_stall, NN);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
@@ -257,13 +258,14 @@ template <typename T, int N> struct Ops {
         ms[4 * pass + v] = -1.0;
         if (v >= nv) continue;
         auto run = [&]() -> int {
+          const int nb = p->nbox;
           if (pass == 0)
-            return colpass_rows<true, true>(p, KID_YINV, io(W1, w1s, (long long)My * Mzp, Mzp, kc),
-                                            StRowsC<T, N, false>{io(W2, w2s, (long long)N * Mzp, Mzp, -1)}, Mzp, 6, N,
-                                            tw, s, v);
-          return colpass_rows<false, false>(p, KID_YFWD, io(W1, w2s, (long long)N * Mzp, Mzp, -1),
-                                            StRowsC<T, N, true>{io(W2, w1s, (long long)My * Mzp, Mzp, kc)}, Mzp, 3, N,
-                                            tw, s, v);
+            return colpass_rows<true, true>(p, KID_YINV, io(W1, nb * w1s, (long long)My * Mzp, Mzp, kc),
+                                            StRowsC<T, N, false>{io(W2, nb * w2s, (long long)N * Mzp, Mzp, -1)}, Mzp,
+                                            6, nb * N, tw, s, v);
+          return colpass_rows<false, false>(p, KID_YFWD, io(W1, nb * w2s, (long long)N * Mzp, Mzp, -1),
+                                            StRowsC<T, N, true>{io(W2, nb * w1s, (long long)My * Mzp, Mzp, kc)}, Mzp,
+                                            3, nb * N, tw, s, v);
         };
         if (int rc = run()) return rc;  // warm-up
         LD_CUDA_CHECK(cudaEventRecord(a, s));
@@ -297,15 +299,20 @@ template <typename T, int N> struct Ops {
     C* W2 = (C*)p->W2;
     const long long w1s = (long long)N * My * Mzp, w2s = NN * Mzp;
     const C* y = s1;  // stage input in every mode
+    // boxes of a multi-box plan: each pass is one launch over all of them; the workspace holds
+    // the box index next to x (fields (f, box, x, ...)), so that (box, x) is one outer index
+    const int nb = p->nbox;
+    if (nb > 1 && p->sm_vk) return ld_fail(LD_ERR_UNSUPPORTED, "slow-manifold output of a multi-box plan");
     if (int rc = forcing_factor(p, y, prm, s)) return rc;
     // inverse x pass with the curl: 6 fields [u, w]
-    LdCurl<T, N> lc{y, cs, kc, My, Mzp};
-    auto xout = io(W1, w1s, 0, My * Mzp, -1);
-    if (int rc = colpass<true>(p, KID_XINV, lc, StRowsC<T, N, false>{xout}, My * Mzp, 6, 1, tw, s)) return rc;
+    LdCurl<T, N> lc{y, cs, kc, My, Mzp, 3 * cs};
+    auto xout = io(W1, nb * w1s, w1s, My * Mzp, -1);
+    if (int rc = colpass<true>(p, KID_XINV, lc, StRowsC<T, N, false>{xout}, My * Mzp, 6, nb, tw, s)) return rc;
     // inverse y pass
-    auto yin = io(W1, w1s, (long long)My * Mzp, Mzp, kc);
-    auto yout = io(W2, w2s, (long long)N * Mzp, Mzp, -1);
-    if (int rc = colpass_rows<true, true>(p, KID_YINV, yin, StRowsC<T, N, false>{yout}, Mzp, 6, N, tw, s)) return rc;
+    auto yin = io(W1, nb * w1s, (long long)My * Mzp, Mzp, kc);
+    auto yout = io(W2, nb * w2s, (long long)N * Mzp, Mzp, -1);
+    if (int rc = colpass_rows<true, true>(p, KID_YINV, yin, StRowsC<T, N, false>{yout}, Mzp, 6, nb * N, tw, s))
+      return rc;
     // fused z pass: u, w -> u x w  (W2 -> W1 as (3, N*N, Mzp))
     {
       ProfScope ps(p, KID_ZCROSS, s);
@@ -316,17 +323,21 @@ template <typename T, int N> struct Ops {
       } else {
         auto k = k_z_cross<T, N>;
         if (int rc = set_smem(k, Z_SMEM)) return rc;
-        k<<<(unsigned)(NN / Cfg<N>::ZROWS), Cfg<N>::ZTHREADS, Z_SMEM, s>>>(W2, W1, uout, ulayout, Mzp, kc, sc, tw);
+        const long long rows = NN * nb;
+        k<<<(unsigned)(rows / Cfg<N>::ZROWS), Cfg<N>::ZTHREADS, Z_SMEM, s>>>(W2, W1, uout, ulayout, Mzp, kc, sc, tw,
+                                                                            rows);
         LD_LAUNCH_CHECK();
       }
     }
     // forward y pass (W1 -> W2 as (3, N, My, Mzp))
-    auto fyin = io(W1, w2s, (long long)N * Mzp, Mzp, -1);
-    auto fyout = io(W2, w1s, (long long)My * Mzp, Mzp, kc);
-    if (int rc = colpass_rows<false, false>(p, KID_YFWD, fyin, StRowsC<T, N, true>{fyout}, Mzp, 3, N, tw, s)) return rc;
+    auto fyin = io(W1, nb * w2s, (long long)N * Mzp, Mzp, -1);
+    auto fyout = io(W2, nb * w1s, (long long)My * Mzp, Mzp, kc);
+    if (int rc = colpass_rows<false, false>(p, KID_YFWD, fyin, StRowsC<T, N, true>{fyout}, Mzp, 3, nb * N, tw, s))
+      return rc;
     // forward x pass + k-space update
     UpdArgs<T> A;
-    A.nl = W2; A.nls = w1s;
+    A.nl = W2; A.nls = nb * w1s;
+    A.nl_bs = w1s; A.cube_bs = 3 * cs; A.fac_bs = p->Nf;
     A.s0 = s0; A.s1 = s1; A.s2 = s2; A.s3 = s3; A.cs = cs;
     A.factor = p->factor; A.kf_lo = prm->kf_lo; A.kf_hi = (prm->f0 == 0.0) ? -1 : prm->kf_hi;
     A.ifac = (const T*)p->ifac;
@@ -342,7 +353,8 @@ template <typename T, int N> struct Ops {
     ProfScope ps(p, KID_XFWD_UPD, s);
     auto k = k_xfwd_update<T, N, MODE>;
     if (int rc = set_smem(k, smem)) return rc;
-    k<<<(unsigned)cdiv((long long)My * Mzp, TB), Cfg<N>::COL_THREADS, smem, s>>>(A, My * Mzp, tw);
+    dim3 ugrid((unsigned)cdiv((long long)My * Mzp, TB), (unsigned)nb);
+    k<<<ugrid, Cfg<N>::COL_THREADS, smem, s>>>(A, My * Mzp, tw);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
@@ -362,23 +374,25 @@ template <typename T, int N> struct Ops {
 
   template <int M>
   static int dstage_m(ld_plan* p, int stage, const T* u, double* pos, T* vel, const T* tau, T* a1, long long n, double h,
-                      double g, cudaStream_t s) {
+                      double g, const int* box, cudaStream_t s) {
     ProfScope ps(p, stage == 1 ? KID_DROPLET1 : KID_DROPLET2, s);
     const int th = 256;
     const int gr = grid1d(n, th);
     const double L = 2.0 * M_PI;
     const vec4<T>* u4 = reinterpret_cast<const vec4<T>*>(u);
-    if (stage == 1) k_droplet_stage<T, M, 1><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g));
-    else k_droplet_stage<T, M, 2><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g));
+    if (stage == 1) k_droplet_stage<T, M, 1><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g), box);
+    else k_droplet_stage<T, M, 2><<<gr, th, 0, s>>>(u4, N, L, pos, vel, tau, a1, n, h, T(g), box);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
 
   static int dstage(ld_plan* p, int stage, int method, const T* u, double* pos, T* vel, const T* tau, T* a1, long long n,
-                    double h, double g, cudaStream_t s) {
-    if (method == LD_INTERP_TRILINEAR) return dstage_m<LD_INTERP_TRILINEAR>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
-    if (method == LD_INTERP_TRICUBIC) return dstage_m<LD_INTERP_TRICUBIC>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
-    return dstage_m<LD_INTERP_COSINE>(p, stage, u, pos, vel, tau, a1, n, h, g, s);
+                    double h, double g, const int* box, cudaStream_t s) {
+    if (method == LD_INTERP_TRILINEAR)
+      return dstage_m<LD_INTERP_TRILINEAR>(p, stage, u, pos, vel, tau, a1, n, h, g, box, s);
+    if (method == LD_INTERP_TRICUBIC)
+      return dstage_m<LD_INTERP_TRICUBIC>(p, stage, u, pos, vel, tau, a1, n, h, g, box, s);
+    return dstage_m<LD_INTERP_COSINE>(p, stage, u, pos, vel, tau, a1, n, h, g, box, s);
   }
 };
 
@@ -445,15 +459,16 @@ template <typename T, int N> struct Table {
     ProfScope ps(p, KID_EPILOGUE, s);
     const long long total = p->cube_elems();
     const double blow = 100.0 * (double)N * N * N;
-    ld::k_epilogue<T><<<grid1d(total, 256), 256, 0, s>>>((C*)uk, total, p->kc, p->My, p->Mzp, T(blow), p->status);
+    dim3 grid((unsigned)grid1d(total, 256), (unsigned)p->nbox);
+    ld::k_epilogue<T><<<grid, 256, 0, s>>>((C*)uk, total, p->kc, p->My, p->Mzp, T(blow), p->status);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }  static int epilogue0(ld_plan* p, void* uk, cudaStream_t s) {
     ProfScope ps(p, KID_EPILOGUE, s);
     const double blow = 100.0 * (double)N * N * N;
     const long long plane = (long long)p->My * p->My;
-    ld::k_epilogue_plane0<T><<<grid1d(plane, 256), 256, 0, s>>>((C*)uk, p->cube_elems(), p->kc, p->My, p->Mzp,
-                                                                 T(blow), p->status);
+    dim3 grid((unsigned)grid1d(plane, 256), (unsigned)p->nbox);
+    ld::k_epilogue_plane0<T><<<grid, 256, 0, s>>>((C*)uk, p->cube_elems(), p->kc, p->My, p->Mzp, T(blow), p->status);
     LD_LAUNCH_CHECK();
     return LD_OK;
   }
@@ -463,8 +478,8 @@ template <typename T, int N> struct Table {
     return O::gather(p, (const T*)f, nc, pos, n, method, (T*)out, s);
   }
   static int dstage(ld_plan* p, int stage, int method, const void* u, double* pos, void* vel, const void* tau,
-                    void* a1, long long n, double h, double g, cudaStream_t s) {
-    return O::dstage(p, stage, method, (const T*)u, pos, (T*)vel, (const T*)tau, (T*)a1, n, h, g, s);
+                    void* a1, long long n, double h, double g, const int* box, cudaStream_t s) {
+    return O::dstage(p, stage, method, (const T*)u, pos, (T*)vel, (const T*)tau, (T*)a1, n, h, g, box, s);
   }
   static const OpsTable* get() {
     static const OpsTable t = {rfft_full, irfft_full, irfft_cube, rfft_cube, to_cube, from_cube,

@@ -77,9 +77,12 @@ int ld_version(void) { return 1; }
 
 const char* ld_last_error(void) { return g_last_error; }
 
-int ld_plan_create(ld_plan** out, int n, int precision) {
+int ld_plan_create(ld_plan** out, int n, int precision) { return ld_plan_create_boxes(out, n, precision, 1); }
+
+int ld_plan_create_boxes(ld_plan** out, int n, int precision, int nbox) {
   if (!out) return ld_fail(LD_ERR_ARG, "null output pointer");
   *out = nullptr;
+  if (nbox < 1 || nbox > 4096) return ld_fail(LD_ERR_ARG, "ld_plan_create_boxes: nbox = %d", nbox);
   if (precision != LD_F32 && precision != LD_F64) return ld_fail(LD_ERR_ARG, "precision %d", precision);
   {
     ld_plan probe;
@@ -92,6 +95,7 @@ int ld_plan_create(ld_plan** out, int n, int precision) {
   if (!p) return ld_fail(LD_ERR_NOMEM, "host allocation failed");
   p->N = n;
   p->prec = precision;
+  p->nbox = nbox;
   p->esz = precision == LD_F32 ? sizeof(float) : sizeof(double);
   p->kc = n / 3;
   p->Mx = p->My = 2 * p->kc + 1;
@@ -145,8 +149,8 @@ int ld_plan_create(ld_plan** out, int n, int precision) {
     if (e == cudaSuccess) e = cudaMalloc(&p->shell_idx, sizeof(int) * (idx.size() ? idx.size() : 1));
     if (e == cudaSuccess) e = cudaMemcpy(p->shell_off, cnt.data(), sizeof(int) * (Nf + 1), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && idx.size()) e = cudaMemcpy(p->shell_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&p->factor, sizeof(double) * Nf);
-    if (e == cudaSuccess) e = cudaMemset(p->factor, 0, sizeof(double) * Nf);
+    if (e == cudaSuccess) e = cudaMalloc(&p->factor, sizeof(double) * Nf * nbox);
+    if (e == cudaSuccess) e = cudaMemset(p->factor, 0, sizeof(double) * Nf * nbox);
     if (e == cudaSuccess) e = cudaMalloc(&p->status, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(p->status, 0, sizeof(unsigned));
     p->nifac = 3 * p->kc * p->kc + 1;
@@ -155,8 +159,8 @@ int ld_plan_create(ld_plan** out, int n, int precision) {
   }
   // transform workspace
   {
-    const size_t w1 = (size_t)6 * n * p->My * p->Mzp * csz;
-    const size_t w2 = (size_t)6 * n * n * p->Mzp * csz;
+    const size_t w1 = (size_t)6 * n * p->My * p->Mzp * csz * nbox;
+    const size_t w2 = (size_t)6 * n * n * p->Mzp * csz * nbox;
     p->work_bytes = w1 + w2;
     cudaError_t e = cudaMalloc(&p->work, p->work_bytes);
     if (e != cudaSuccess) { ld_set_last_error(e); return cleanup(LD_ERR_CUDA); }
@@ -179,6 +183,13 @@ int ld_plan_destroy(ld_plan* p) {
   cudaFree(p->status);
   cudaFree(p->work);
   delete p;
+  return LD_OK;
+}
+
+int ld_plan_boxes(const ld_plan* p, int32_t* nbox) {
+  if (int rc = check_plan(p)) return rc;
+  if (!nbox) return ld_fail(LD_ERR_ARG, "ld_plan_boxes: bad arguments");
+  *nbox = p->nbox;
   return LD_OK;
 }
 
@@ -328,7 +339,16 @@ int ld_droplet_stage(ld_plan* p, int stage, const void* u, double* pos, void* ve
   if (!u || !pos || !vel || !tau || !a1 || n < 0 || method < 0 || method > 2 || (stage != 1 && stage != 2))
     return ld_fail(LD_ERR_ARG, "ld_droplet_stage: bad arguments");
   if (n == 0) return LD_OK;
-  return table_of(p)->dstage(p, stage, method, u, pos, vel, tau, a1, n, h, g, S(stream));
+  return table_of(p)->dstage(p, stage, method, u, pos, vel, tau, a1, n, h, g, nullptr, S(stream));
+}
+
+int ld_droplet_stage_boxes(ld_plan* p, int stage, const void* u, const int32_t* box, double* pos, void* vel,
+                           const void* tau, void* a1, int64_t n, int method, double h, double g, void* stream) {
+  if (int rc = check_plan(p)) return rc;
+  if (!u || !box || !pos || !vel || !tau || !a1 || n < 0 || method < 0 || method > 2 || (stage != 1 && stage != 2))
+    return ld_fail(LD_ERR_ARG, "ld_droplet_stage_boxes: bad arguments");
+  if (n == 0) return LD_OK;
+  return table_of(p)->dstage(p, stage, method, u, pos, vel, tau, a1, n, h, g, box, S(stream));
 }
 
 int ld_profile(ld_plan* p, int enable) {

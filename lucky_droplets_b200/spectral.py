@@ -27,7 +27,9 @@ def _torch():
 class Plan:
     """One N^3 grid in FP32 ("f32") or FP64 ("f64") on a CUDA device."""
 
-    def __init__(self, N, precision="f32", device=None):
+    def __init__(self, N, precision="f32", device=None, nbox=1):
+        """nbox > 1: a plan for nbox independent boxes; its stage calls advance states laid out
+        (nbox, 3, Mx, My, Mzp) in one launch per pass (ld_plan_create_boxes)."""
         torch = _torch()
         if not torch.cuda.is_available():
             raise RuntimeError("lucky_droplets_b200 needs a CUDA device (no CPU fallback)")
@@ -41,8 +43,9 @@ class Plan:
         self.cdtype = torch.complex64 if precision == "f32" else torch.complex128
         L = _lib.lib()
         h = ctypes.c_void_p()
+        self.nbox = int(nbox)
         with torch.cuda.device(self.device):
-            check(L.ld_plan_create(ctypes.byref(h), int(N), prec))
+            check(L.ld_plan_create_boxes(ctypes.byref(h), int(N), prec, self.nbox))
         self._h = h
         dims = (ctypes.c_int32 * 8)()
         wb = ctypes.c_size_t()

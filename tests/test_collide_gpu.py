@@ -211,3 +211,41 @@ def test_partners_beyond_the_record_are_searched_again(torch):
     ref = K.collide(pos, rad, 0.1)
     assert len(ref) > 100000
     assert got.shape == ref.shape and np.array_equal(got, ref)
+
+
+def test_multi_box_collider_matches_each_box_alone():
+    """One multi-box collider over the droplets of several boxes (cells keyed box-major) finds, box
+    by box, exactly the pairs the FP64 rule gives for that box alone, counts them per box, and
+    never pairs droplets of different boxes; the cell order keeps the boxes contiguous."""
+    import torch
+    from lucky_droplets_b200.collide import Collider
+    from oracle import collide_np as K
+    rng = np.random.default_rng(17)
+    sizes = [3000, 0, 1200, 4500]
+    pos = [rng.uniform(-0.5, 2 * np.pi + 0.5, (n, 3)) for n in sizes]
+    rad = [0.02 + 0.03 * rng.random(n) for n in sizes]
+    box = np.concatenate([np.full(n, j, np.int32) for j, n in enumerate(sizes)])
+    P = torch.as_tensor(np.concatenate(pos)).cuda()
+    R = torch.as_tensor(np.concatenate(rad)).cuda()
+    Bx = torch.as_tensor(box).cuda()
+    n = int(P.shape[0])
+    for cell in (0.11, 3.0):  # nc >= 3, and nc < 3
+        col = Collider(n, cell, nbox=len(sizes))
+        pairs = torch.empty((4 * n, 2), dtype=torch.int32, device="cuda")
+        col.collide_boxes(P, R, Bx, pairs)
+        m = int(col.count.item())
+        got = pairs[:m].cpu().numpy().astype(np.int64)
+        assert (box[got[:, 0]] == box[got[:, 1]]).all()
+        off = np.concatenate([[0], np.cumsum(sizes)])
+        bc = col.box_counts.cpu().numpy()
+        for j, nj in enumerate(sizes):
+            sel = got[box[got[:, 0]] == j] - off[j]
+            sel = np.sort(sel, axis=1)
+            sel = sel[np.lexsort((sel[:, 1], sel[:, 0]))]
+            ref = K.collide(pos[j], rad[j], cell) if nj else np.zeros((0, 2), np.int64)
+            assert np.array_equal(sel, ref), (cell, j)
+            assert bc[j] == len(ref)
+        order = torch.empty(n, dtype=torch.int32, device="cuda")
+        col.cell_order_boxes(P, Bx, order)
+        ob = box[order.cpu().numpy()]
+        assert (np.diff(ob) >= 0).all()

@@ -1,5 +1,6 @@
-"""Ensemble of boxes advanced by CUDA-graph replays over several streams: bit-identical to the
-same boxes stepped eagerly one after another, re-sorting and collisions included."""
+"""The ensemble as one multi-box batch (one launch per pass over all boxes, droplets of every box
+in one set of arrays, one multi-box collider): graph replays equal eager steps, and every box
+equals the same seed run alone as one ForcedDNS, bit for bit."""
 import numpy as np
 import pytest
 
@@ -13,39 +14,48 @@ def torch():
     return torch
 
 
-def _ens(seed):
+def _ens(seed, **kw):
     from lucky_droplets_b200.ensemble import Ensemble
-    return Ensemble(n_boxes=4, N=32, nd=(300, 2000), seed=seed, sort_every=2)
+    return Ensemble(n_boxes=4, N=32, nd=(300, 2000), seed=seed, sort_every=2, **kw)
 
 
 def test_graph_replay_equals_eager(torch):
     a, b = _ens(3), _ens(3)
     a.step_eager(1)
-    a.capture(3, 2)
-    a.replay(2)
+    a.capture(2)
+    a.replay(3)
     b.step_eager(7)
     torch.cuda.synchronize()
-    for ba, bb in zip(a.boxes, b.boxes):
-        assert ba.nstep == bb.nstep == 7
-        assert torch.equal(ba.uk, bb.uk)
-        da, db = ba.droplets, bb.droplets
-        assert np.array_equal(da.by_id(da.pos), db.by_id(db.pos))
-        assert np.array_equal(da.by_id(da.vel), db.by_id(db.vel))
-        assert int(ba.collider.count.item()) == int(bb.collider.count.item())
+    assert a.nstep == b.nstep == 7
+    assert torch.equal(a.uk, b.uk)
+    for j in range(a.nb):
+        _, pa, va = a.box_state(j)
+        _, pb, vb = b.box_state(j)
+        assert np.array_equal(pa, pb) and np.array_equal(va, vb)
     assert a.collision_counts() == b.collision_counts()
+    assert int(a.collider.count.item()) == sum(a.collision_counts())
+    # a replay from another phase of the re-sorting period gets a graph of its own
+    a.step_eager(1)
+    a.replay(2)
+    b.step_eager(5)
+    torch.cuda.synchronize()
+    assert a.nstep == b.nstep == 12 and len(a.graphs) == 2
+    assert torch.equal(a.uk, b.uk)
+    for j in range(a.nb):
+        assert np.array_equal(a.box_state(j)[1], b.box_state(j)[1])
 
 
 def test_boxes_differ_and_counts_follow_the_seed(torch):
     from lucky_droplets_b200.ensemble import box_counts
     e = _ens(5)
-    assert [d.droplets.n for d in e.boxes] == [int(c) for c in box_counts(4, 5, 300, 2000)]
-    assert not torch.equal(e.boxes[0].uk, e.boxes[1].uk)
+    per_box = np.bincount(e.box.cpu().numpy(), minlength=4)
+    assert list(per_box) == [int(c) for c in box_counts(4, 5, 300, 2000)]
+    assert not torch.equal(e.uk[0], e.uk[1])
 
 
 def test_box_equals_the_same_seed_run_alone(torch):
-    """Box b of an ensemble (boxes stepped together from CUDA graphs on several streams) ends in
-    exactly the state of the same seed run alone as one ForcedDNS stepped eagerly: spectrum,
-    droplets by id and the collision count, bit for bit."""
+    """Box b of the batch ends in exactly the state of the same seed run alone (flow, droplets by
+    index, collision count), after steps that include re-sorting and graph replays."""
     from lucky_droplets_b200.collide import Collider
     from lucky_droplets_b200.dns import ForcedDNS, Droplets
     from lucky_droplets_b200.ensemble import box_counts
@@ -53,9 +63,10 @@ def test_box_equals_the_same_seed_run_alone(torch):
     seed, nb = 7, 4
     e = _ens(seed)
     e.step_eager(1)
-    e.capture(3, 2)
-    e.replay(2)
+    e.capture(2)
+    e.replay(3)
     counts = box_counts(nb, seed, 300, 2000)
+    coll = e.collision_counts()
     for b in (0, 3):
         dns = ForcedDNS.config(32, 0.01, 2e-3, eps=0.1, kf=2, precision="f32")
         dns.plan.set_tuning(e.fft_tuning["choice"])
@@ -67,10 +78,18 @@ def test_box_equals_the_same_seed_run_alone(torch):
         dns.attach(d, collider=col, sort_every=2)
         dns.step(7)
         torch.cuda.synchronize()
-        box = e.boxes[b]
-        db = box.droplets
-        assert box.nstep == dns.nstep == 7
-        assert torch.equal(box.uk, dns.uk)
-        assert np.array_equal(db.by_id(db.pos), d.by_id(d.pos))
-        assert np.array_equal(db.by_id(db.vel), d.by_id(d.vel))
-        assert int(box.collider.count.item()) == int(col.count.item())
+        uk, pe, ve = e.box_state(b)
+        assert torch.equal(uk, dns.uk[...])
+        assert np.array_equal(pe, d.by_id(d.pos))
+        assert np.array_equal(ve, d.by_id(d.vel))
+        assert coll[b] == int(col.count.item())
+
+
+def test_ensemble_autotune_and_status(torch):
+    e = _ens(9)
+    table = e.autotune(steps_per_graph=(3, 4), trial_graphs=1)
+    assert [r["steps_per_graph"] for r in table] == [3, 4]
+    assert e.steps_per_graph in (3, 4)
+    e.run(6)
+    assert e.check() == 0
+    assert all(c in (0, 1, 2, 3) for c in e.fft_tuning["choice"])
