@@ -102,14 +102,16 @@ LD_API int ld_rfft_mpi(ld_plan* plan, const void* u, void* fu, int ncomp, void* 
  * parts of the kz = 0 and kz = N/2 coefficients are ignored, as pocketfft's c2r does. */
 LD_API int ld_irfft_mpi(ld_plan* plan, const void* fu, void* u, int ncomp, void* stream);
 /* irfft_mpi without any allocation - no counterpart in the reference.  For callers that must not
- * allocate device memory: code running while a stream is captured into a CUDA graph in the
- * global capture mode (cudaMalloc is not permitted there) and host frameworks that hand out all
- * device memory from their own pool.  No plan: the scratch is a file-scope device array sized for
- * N <= 64 (64*64*33 complex floats, 1.08 MB, held by every GPU that loads the library until the
- * process exits) plus static twiddle tables.  FP32 only, N in {16, 32, 64}; larger N returns
- * LD_ERR_UNSUPPORTED.  fu (ncomp, N, N, N/2+1) complex float, u (ncomp, N, N, N) float.  The first
- * call on a device sets that device up (symbol-address lookup and a synchronous twiddle copy), so
- * make it before any stream capture.  Calls share the scratch: calls that overlap on the GPU race. */
+ * allocate device memory: host frameworks that hand out all device memory from their own pool
+ * and forbid driver allocations, and time-critical loops that may not allocate after set-up (an
+ * allocation can synchronise the device, take unbounded time or fail mid-run).  No plan: the
+ * scratch is a file-scope device array sized for N <= 64 (64*64*33 complex floats, 1.08 MB, held
+ * by every GPU that loads the library until the process exits) plus static twiddle tables.  FP32
+ * only, N in {16, 32, 64}; larger N returns LD_ERR_UNSUPPORTED.  fu (ncomp, N, N, N/2+1) complex
+ * float, u (ncomp, N, N, N) float.  The first call on a device sets that device up (symbol-address
+ * lookup and a synchronous twiddle copy) and the first call for each N launches that size's
+ * kernels for the first time, so make those first calls before any stream capture.  Calls share
+ * the scratch: calls that overlap on the GPU race. */
 LD_API int ld_irfft_mpi_noalloc(int n, const void* fu, void* u, int ncomp, void* stream);
 /* Dealiased transforms in the cube layout: the same transforms restricted to the modes of the
  * spherical mask (F:129) - the form every transform of the DNS step takes. */
@@ -199,6 +201,44 @@ LD_API int ld_step_epilogue(ld_plan* plan, void* uk, void* stream);
  * those stages this call completes the step epilogue (ld_step_epilogue there is also correct: it
  * projects the kz > 0 modes a second time). */
 LD_API int ld_step_epilogue_plane0(ld_plan* plan, void* uk, void* stream);
+
+/* ---- whole steps: the body of the time loop, F:571-623 ---------------------------------- */
+/* State of ld_step / ld_ensemble_step: caller-owned device buffers. */
+typedef struct ld_step_state {
+  void* uk;            /* (nbox, 3, Mx, My, Mzp) cube spectrum, advanced in place               */
+  void* ustar;         /* the same shape: RK2 stage scratch                                       */
+  void* acc;           /* the same shape: RK2 accumulator                                         */
+  void* u4;            /* (nbox, N, N, N, 4) physical velocity the droplet stages read            */
+  int64_t n;           /* droplets (0: flow only)                                                  */
+  double* pos;         /* (n, 3) FP64 positions                                                    */
+  void* vel;           /* (n, 3) velocities, plan precision                                        */
+  void* tau;           /* (n) Stokes times, plan precision                                         */
+  void* a1;            /* (n, 3) Heun stage scratch, plan precision                                */
+  double* radius;      /* (n) radii (collisions; nullable without them)                            */
+  int64_t* ids;        /* (n) droplet ids, permuted with the droplets (nullable)                   */
+  int32_t* box;        /* (n) box of each droplet: ld_ensemble_step; NULL for ld_step              */
+  int32_t method;      /* LD_INTERP_*                                                              */
+  double g;            /* settling acceleration along -z                                           */
+  int32_t sort_every;  /* re-sort into cell order every that many steps (0: never)                 */
+  uint32_t* order;     /* (n) permutation scratch of the re-sort                                   */
+  void* scratch;       /* n * 24 bytes of row scratch for the re-sort                              */
+  int32_t* pairs;      /* (pair_cap, 2) colliding pairs after every step; NULL: no collisions      */
+  int64_t pair_cap;
+  int64_t* pair_count; /* device: pairs of the last step                                           */
+  int64_t* box_counts; /* device (nbox), nullable: pairs per box                                   */
+  int64_t step;        /* steps done; sets the re-sort phase; incremented by every step            */
+} ld_step_state;
+/* nsteps whole steps of one box: RK2 + integrating factor stages with the droplet Heun stages
+ * between them, the plane epilogue (F:596-620), the re-sort every sort_every steps and the
+ * collision search - the sequence of the Python stepper, so the same kernels give the same
+ * bits.  The replacement of one pass of the reference's loop body (F:582-620) per step. */
+LD_API int ld_step(ld_plan* plan, ld_collider* collider, ld_step_state* state, const ld_flow_params* prm,
+                   int32_t nsteps, void* stream);
+/* The same for every box of a multi-box plan (ld_plan_create_boxes) with a multi-box collider
+ * (ld_collider_create_boxes); state->box gives each droplet's box.  No counterpart in the
+ * reference (one box per run there). */
+LD_API int ld_ensemble_step(ld_plan* plan, ld_collider* collider, ld_step_state* state, const ld_flow_params* prm,
+                            int32_t nsteps, void* stream);
 
 /* ---- droplets, P:52-111, P:435-511, P:817-837 ----------------------------------------- */
 /* Interpolate ncomp physical fields (ncomp, N, N, N) at n positions (n, 3) double:

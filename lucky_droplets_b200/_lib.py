@@ -30,12 +30,23 @@ class FlowParams(ctypes.Structure):
     _fields_ = [("dt", _c_d), ("nu", _c_d), ("f0", _c_d), ("kf_lo", _c_i32), ("kf_hi", _c_i32)]
 
 
+class StepState(ctypes.Structure):
+    """ld_step_state of include/ld.h."""
+    _fields_ = [("uk", _c_p), ("ustar", _c_p), ("acc", _c_p), ("u4", _c_p), ("n", _c_i64), ("pos", _c_p),
+                ("vel", _c_p), ("tau", _c_p), ("a1", _c_p), ("radius", _c_p), ("ids", _c_p), ("box", _c_p),
+                ("method", _c_i32), ("g", _c_d), ("sort_every", _c_i32), ("order", _c_p), ("scratch", _c_p),
+                ("pairs", _c_p), ("pair_cap", _c_i64), ("pair_count", _c_p), ("box_counts", _c_p),
+                ("step", _c_i64)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "ld_version": (_c_i, []),
     "ld_last_error": (ctypes.c_char_p, []),
     "ld_plan_create": (_c_i, [ctypes.POINTER(_c_p), _c_i, _c_i]),
     "ld_plan_create_boxes": (_c_i, [ctypes.POINTER(_c_p), _c_i, _c_i, _c_i]),
+    "ld_step": (_c_i, [_c_p, _c_p, ctypes.POINTER(StepState), ctypes.POINTER(FlowParams), _c_i32, _c_p]),
+    "ld_ensemble_step": (_c_i, [_c_p, _c_p, ctypes.POINTER(StepState), ctypes.POINTER(FlowParams), _c_i32, _c_p]),
     "ld_plan_boxes": (_c_i, [_c_p, ctypes.POINTER(_c_i32)]),
     "ld_droplet_stage_boxes": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_i, _c_d, _c_d, _c_p]),
     "ld_plan_destroy": (_c_i, [_c_p]),

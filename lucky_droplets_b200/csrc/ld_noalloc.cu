@@ -1,9 +1,9 @@
 // ld_irfft_mpi_noalloc: the inverse transform of ld_irfft_mpi for callers that must not allocate
 // device memory.  Two kinds of caller need it:
-//   * code that runs while a stream is being captured into a CUDA graph in the global capture
-//     mode, where cudaMalloc is not permitted, and
-//   * host frameworks that hand out all device memory from their own pool and forbid driver
-//     allocations behind their back.
+//   * host frameworks that hand out all device memory from their own pool, with a budget fixed
+//     at start-up, and forbid driver allocations behind their back, and
+//   * time-critical loops that may not allocate after their set-up, because an allocation can
+//     synchronise the device, take unbounded time or fail part-way through a run.
 // Such a caller cannot create an ld_plan (a plan allocates its twiddle tables and workspace), so
 // this entry point keeps its scratch in file-scope device arrays instead: one complex-float buffer
 // for an (N, N, N/2+1) spectrum with N <= 64 (64*64*33 complex floats, 1.08 MB) and the twiddle
@@ -12,8 +12,10 @@
 //
 // In host code the arrays' names are host-side stand-ins, not device addresses: the first call on
 // a device, with that device current, looks their device addresses up with cudaGetSymbolAddress
-// and fills the twiddle tables with a synchronous host-to-device copy.  That set-up must not be
-// inside a stream capture, so make the first call on each device before any capture.
+// and fills the twiddle tables with a synchronous host-to-device copy, and the first call for
+// each N launches that size's kernels for the first time (the driver loads them then).  Make the
+// first call on each device, and the first call for each N that will be used, before any stream
+// capture.
 //
 // All calls share the one scratch buffer of their device, and each call overwrites it completely
 // before reading it.  Calls that overlap on the GPU (different streams, no ordering) race on it.
@@ -68,7 +70,7 @@ int na_setup(NaDevice** out) {
 }
 
 // x pass (fu -> W), y pass in place on W, z C2R (W -> u): the launch sequence of ld_irfft_mpi
-// for one component at a time, with W the static scratch.
+// (Ops::irfft_full) for one component at a time, with W the static scratch.
 template <int N>
 int na_run(const float2* fu, float* u, int ncomp, float2* W, const float2* tw, cudaStream_t s) {
   using O = ld_impl::Ops<float, N>;
@@ -79,12 +81,13 @@ int na_run(const float2* fu, float* u, int ncomp, float2* W, const float2* tw, c
   for (int c = 0; c < ncomp; ++c) {
     auto xin = O::io(fu + c * per, per, 0, N * Nf, -1);
     auto xout = O::io(W, per, 0, N * Nf, -1);
-    if (int rc = O::template colpass<true>(nullptr, KID_XPASS, ld::LdRows<float, N>{xin}, ld::StRows<float, N>{xout},
-                                           N * Nf, 1, 1, tw, s))
+    // the loaders and storers of Ops::irfft_full (plain rows), so both paths run the same kernels
+    if (int rc = O::template colpass<true>(nullptr, KID_XPASS, ld::LdRowsC<float, N, false>{xin},
+                                           ld::StRowsC<float, N, false>{xout}, N * Nf, 1, 1, tw, s))
       return rc;
     auto yio = O::io(W, per, (long long)N * Nf, Nf, -1);
-    if (int rc = O::template colpass<true>(nullptr, KID_YINV, ld::LdRows<float, N>{yio}, ld::StRows<float, N>{yio},
-                                           Nf, 1, N, tw, s))
+    if (int rc = O::template colpass<true>(nullptr, KID_YINV, ld::LdRowsC<float, N, false>{yio},
+                                           ld::StRowsC<float, N, false>{yio}, Nf, 1, N, tw, s))
       return rc;
     if (int rc = O::z_c2r(nullptr, W, u + c * NN * N, NN, Nf, Nf, sc, NN * N, per, 1, tw, s)) return rc;
   }

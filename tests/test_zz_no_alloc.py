@@ -1,9 +1,9 @@
 """ld_irfft_mpi_noalloc against ld_irfft_mpi.
 
-The no-alloc entry point serves callers that must not allocate device memory - code running
-inside a CUDA-graph stream capture (global mode forbids cudaMalloc) and host frameworks that
-own all device memory through their own pool.  It keeps its scratch in a static device array
-(N <= 64), so it must give the same result as the plan-based transform, call after call.
+The no-alloc entry point serves callers that must not allocate device memory - host frameworks
+that own all device memory through their own pool, and time-critical loops that may not allocate
+after their set-up.  It keeps its scratch in a static device array (N <= 64), so it must give the
+same result as the plan-based transform, call after call.
 This file is collected last on purpose: a failure here leaves every other test already run.
 """
 import ctypes
