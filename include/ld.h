@@ -282,6 +282,13 @@ LD_API int ld_mlp_pack(const float* params, void* packed, void* stream);
  * out (n,3) = tricubic + scale * os * MLP(features). */
 LD_API int ld_mlp_infer(ld_plan* plan, const void* u4, const double* pos, int64_t n, const void* packed,
                         const float* params, void* out, void* stream);
+/* The same with the feature tiles in the caller's workspace (work, work_bytes; whole 128-droplet
+ * tiles per batch) instead of the plan's transform workspace, so that inference may run on another
+ * stream while the plan transforms (the droplet stage overlapping the next flow stage).
+ * ld_mlp_infer_workspace_bytes(n) is the size that takes n droplets in one batch. */
+LD_API int ld_mlp_infer_ws(ld_plan* plan, const void* u4, const double* pos, int64_t n, const void* packed,
+                           const float* params, void* out, void* work, int64_t work_bytes, void* stream);
+LD_API int64_t ld_mlp_infer_workspace_bytes(int64_t n);
 /* uk * exp(i k.(s dx)) for a cube-layout 3-vector: the field translated so that its grid values are
  * the original field's values at x_j + s dx (s in grid units). */
 LD_API int ld_phase_shift(ld_plan* plan, const void* uk, void* out, double sx, double sy, double sz, void* stream);

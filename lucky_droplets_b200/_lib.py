@@ -77,6 +77,8 @@ SIGNATURES = {
                             ctypes.POINTER(_c_i32)]),
     "ld_mlp_pack": (_c_i, [_c_p, _c_p, _c_p]),
     "ld_mlp_infer": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p]),
+    "ld_mlp_infer_ws": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_p]),
+    "ld_mlp_infer_workspace_bytes": (_c_i64, [_c_i64]),
     "ld_phase_shift": (_c_i, [_c_p, _c_p, _c_p, _c_d, _c_d, _c_d, _c_p]),
     "ld_mlp_samples": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_d, _c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_interleave3": (_c_i, [_c_p, _c_p, _c_p, _c_p]),

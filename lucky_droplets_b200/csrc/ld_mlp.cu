@@ -1130,7 +1130,17 @@ int ld_mlp_pack(const float* params, void* packed, void* stream) {
 
 int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const void* packed, const float* params,
                  void* out, void* stream) {
-  if (!p || !u4 || !packed || !params || n < 0 || (n > 0 && (!pos || !out)))
+  return ld_mlp_infer_ws(p, u4, pos, n, packed, params, out, nullptr, 0, stream);
+}
+
+int64_t ld_mlp_infer_workspace_bytes(int64_t n) {
+  const long long tiles = (n + TM - 1) / TM;
+  return tiles * (long long)TILE_X_BYTES + tiles * TM * (long long)sizeof(float) * 8;
+}
+
+int ld_mlp_infer_ws(ld_plan* p, const void* u4, const double* pos, int64_t n, const void* packed, const float* params,
+                    void* out, void* work, int64_t work_bytes, void* stream) {
+  if (!p || !u4 || !packed || !params || n < 0 || (n > 0 && (!pos || !out)) || (work && work_bytes <= 0))
     return ld_fail(LD_ERR_ARG, "ld_mlp_infer: bad arguments");
   if (p->N > 1024) return ld_fail(LD_ERR_ARG, "ld_mlp_infer: N > 1024 (stencil offsets are 32-bit)");
   if (p->N & (p->N - 1)) return ld_fail(LD_ERR_UNSUPPORTED, "ld_mlp_infer: N = %d (the stencil wrap needs a power of two)", p->N);
@@ -1138,13 +1148,14 @@ int ld_mlp_infer(ld_plan* p, const void* u4, const double* pos, int64_t n, const
   cudaStream_t s = (cudaStream_t)stream;
   const double L = 2.0 * M_PI;
   static_assert(SMEM_FWD <= 227 * 1024, "tensor-core forward exceeds shared memory");
-  // feature tiles and aux live in the plan's transform workspace (idle during droplet stages):
-  // droplets are taken in batches of whole tiles that fit it
+  // feature tiles and aux live in the caller's workspace, or in the plan's transform workspace
+  // (idle during droplet stages that do not overlap the flow's transforms): droplets are taken
+  // in batches of whole tiles that fit it
   const size_t per = sizeof(bf16) * K1 + sizeof(float) * 8;
-  long long cap = (long long)(p->work_bytes / per);
+  long long cap = (long long)((work ? (size_t)work_bytes : p->work_bytes) / per);
   cap -= cap % TM;
   if (cap < TM) return ld_fail(LD_ERR_CAPACITY, "ld_mlp_infer: no workspace");
-  unsigned char* X = (unsigned char*)p->work;
+  unsigned char* X = (unsigned char*)(work ? work : p->work);
   for (long long b0 = 0; b0 < n; b0 += cap) {
     const long long nb = n - b0 < cap ? n - b0 : cap;
     const long long tiles = (nb + TM - 1) / TM;

@@ -122,14 +122,24 @@ class LearnedInterp:
         check(_lib.lib().ld_mlp_pack(ptr(self.params), ptr(self.packed), stream_ptr()))
 
     # ---- inference ------------------------------------------------------------------------------
-    def infer(self, u4, pos, out=None, stream=None):
+    def infer(self, u4, pos, out=None, stream=None, work=None):
+        """Velocity (n, 3) at pos: tricubic + learned correction.  work (uint8 device tensor, see
+        workspace()) holds the feature tiles; without it the plan's transform workspace does, so the
+        call must not overlap the plan's transforms."""
         torch = _torch()
         n = int(pos.shape[0])
         if out is None:
             out = torch.empty((n, 3), dtype=self.plan.rdtype, device=self.plan.device)
-        check(_lib.lib().ld_mlp_infer(self.plan.handle, ptr(u4), ptr(pos), n, ptr(self.packed), ptr(self.params),
-                                      ptr(out), stream_ptr(stream)))
+        check(_lib.lib().ld_mlp_infer_ws(self.plan.handle, ptr(u4), ptr(pos), n, ptr(self.packed), ptr(self.params),
+                                         ptr(out), ptr(work), int(work.numel()) if work is not None else 0,
+                                         stream_ptr(stream)))
         return out
+
+    def workspace(self, n):
+        """A feature-tile workspace for inference of n droplets in one batch."""
+        torch = _torch()
+        return torch.empty(int(_lib.lib().ld_mlp_infer_workspace_bytes(int(n))), dtype=torch.uint8,
+                           device=self.plan.device)
 
     # ---- data -------------------------------------------------------------------------------------
     def interleaved(self, uk):

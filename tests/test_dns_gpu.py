@@ -319,3 +319,38 @@ def test_tricubic_droplet_step_on_mixed_radix_grid(torch, N):
     assert rel(dns.uk_full(), uk * grid.dealias) < 1e-12
     assert np.abs(d.pos.cpu().numpy() - p_).max() < 1e-13
     assert rel(d.vel.cpu().numpy(), v_) < 1e-12
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_overlapped_droplet_stream_equals_one_stream(torch, learned):
+    """The droplet work on a second stream (droplet stage 1 under the second flow stage, re-sort and
+    collisions under the next step's first stage, two velocity buffers) gives exactly the state of
+    everything on one stream - eagerly and from a captured graph."""
+    from lucky_droplets_b200.collide import Collider
+    from lucky_droplets_b200.dns import ForcedDNS, Droplets
+    from lucky_droplets_b200 import mlp as G
+    N = 32
+    prm = C.ConfigParams(N=N, nu=0.01, dt=2e-3, g=0.1)
+    uk0, u0 = C.init_flow(C.ConfigGrid(N), prm, seed=23)
+    pos, tau, rad = C.init_droplets(prm, 23, "uniform_tau", nd=3000)
+    rad = rad * 5.0
+    vel = C.gather(u0, pos, "tricubic")
+    runs = []
+    for overlap in (False, True, True):
+        dns = ForcedDNS.config(N, prm.nu, prm.dt, eps=prm.eps, kf=prm.kf, precision="f32", overlap=overlap)
+        dns.set_uk_full(uk0)
+        d = Droplets(dns.plan, pos, vel, tau, method="tricubic", g=prm.g, radius=rad)
+        dns.attach(d, collider=Collider(d.n, 2 * rad.max()), sort_every=3)
+        if learned:
+            d.use_learned(G.LearnedInterp(dns.plan, seed=3, tol=1.0))
+        runs.append((dns, d))
+    (a, da), (b, db), (c, dc) = runs
+    a.step(7)
+    b.step(7)
+    g = c.capture(7)
+    g.replay()
+    torch.cuda.synchronize()
+    for x, dx in ((b, db), (c, dc)):
+        assert torch.equal(a.uk, x.uk)
+        assert torch.equal(da.pos, dx.pos) and torch.equal(da.vel, dx.vel) and torch.equal(da.ids, dx.ids)
+        assert int(a.collider.count.item()) == int(x.collider.count.item())
