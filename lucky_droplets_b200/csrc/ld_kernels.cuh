@@ -781,8 +781,10 @@ k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict_
 // Shared memory per warp: 2 x 6 x Mzp staging + ZBUF exchange elements, then 3 mbarriers.
 constexpr unsigned kWaitLimit = 1u << 24;
 
+// FP32: 8 warps per CTA, two CTAs per SM at N = 256 (at most 128 registers; the 16-element rows
+// of N = 512 need more); FP64: 4 warps per CTA
 template <typename T, int N>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 256 : 128, (sizeof(T) == 4 && N <= 256) ? 2 : 1)
 k_z_cross_pipe(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
                int kc, T s, const cplx<T>* __restrict__ tw, unsigned* status, unsigned wait_limit,
                int stall, long long NR) {

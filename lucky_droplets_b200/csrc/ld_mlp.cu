@@ -211,19 +211,48 @@ __device__ __forceinline__ void tric_weights(const float* tc, float (&wh)[3][4])
   for (int k = 0; k < 3; ++k) tric_weight_axis(tc[k], wh[k]);
 }
 
+// A component's 64 taps live as 32 packed FP32 pairs: pair i holds tap i (canonical index
+// j0 j1 j2 with j0 < 2) in .x and tap i + 32 (j0 + 2) in .y.  Along axes 2 and 1 the lines of j0
+// and j0 + 2 are transformed together by packed instructions (__fadd2_rn / __ffma2_rn: each half
+// rounds exactly as the scalar operation), along axis 0 the four taps of a line sit in two pairs
+// and are transformed as scalars; every tap goes through exactly the operations of the scalar
+// transform, so the coefficients are bit-identical to it.
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ void poly4x2(float2* v, int stride) {
+  const float2 s0 = v[0], s1 = v[stride], s2 = v[2 * stride], s3 = v[3 * stride];
+  const float2 a = __fadd2_rn(s0, s3), b = __fadd2_rn(s1, s2), c = __fadd2_rn(s3, neg2(s0)), d = __fadd2_rn(s2, neg2(s1));
+  v[0] = __fadd2_rn(a, b);
+  v[stride] = __ffma2_rn(make_float2(3.f, 3.f), c, d);
+  v[2 * stride] = __fadd2_rn(a, neg2(b));
+  v[3 * stride] = __ffma2_rn(make_float2(-3.f, -3.f), d, c);
+}
+// tap j of the packed layout
+__device__ __forceinline__ float tap(const float2 (&v)[32], int j) { return j < 32 ? v[j].x : v[j - 32].y; }
+__device__ __forceinline__ void set_tap(float2 (&v)[32], int j, float x) {
+  if (j < 32) v[j].x = x;
+  else v[j - 32].y = x;
+}
+
 // One component's 64 taps (canonical order, in registers) -> its polynomial coefficients, then
 // the component's partial sums: squares, squares of total order >= 3, and its tricubic value.
 // The three components are combined as (c0 + c1) + c2 by every caller, so all paths round
 // identically; all indices are compile-time constants.
-__device__ __forceinline__ void comp_transform(float (&v)[64]) {
+__device__ __forceinline__ void comp_transform(float2 (&v)[32]) {
 #pragma unroll
-  for (int a = 0; a < 16; ++a) poly4(v + 4 * a, 1);                          // along axis 2
+  for (int a = 0; a < 8; ++a) poly4x2(v + 4 * a, 1);                         // along axis 2
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int q = 0; q < 4; ++q) poly4(v + 16 * a + q, 4);                    // along axis 1
+    for (int q = 0; q < 4; ++q) poly4x2(v + 16 * a + q, 4);                  // along axis 1
 #pragma unroll
-  for (int e = 0; e < 16; ++e) poly4(v + e, 16);                             // along axis 0
+  for (int e = 0; e < 16; ++e) {                                             // along axis 0
+    float w4[4] = {v[e].x, v[e + 16].x, v[e].y, v[e + 16].y};
+    poly4(w4, 1);
+    v[e].x = w4[0];
+    v[e + 16].x = w4[1];
+    v[e].y = w4[2];
+    v[e + 16].y = w4[3];
+  }
 }
 
 struct CompSums {
@@ -231,20 +260,21 @@ struct CompSums {
 };
 
 // need_ss: also the sum of all squares (scale mode 0); mode 1 needs only sh.
-__device__ __forceinline__ CompSums comp_sums(const float (&v)[64], const float (&wh)[3][4], bool need_ss = true) {
+__device__ __forceinline__ CompSums comp_sums(const float2 (&v)[32], const float (&wh)[3][4], bool need_ss = true) {
   CompSums p{0.f, 0.f, 0.f};
   if (need_ss) {
 #pragma unroll
-    for (int j = 0; j < 64; ++j) p.ss = fmaf(v[j], v[j], p.ss);
+    for (int j = 0; j < 64; ++j) p.ss = fmaf(tap(v, j), tap(v, j), p.ss);
   }
 #pragma unroll
   for (int j = 0; j < 64; ++j)
-    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh = fmaf(v[j], v[j], p.sh);
+    if ((j >> 4) + ((j >> 2) & 3) + (j & 3) >= 3) p.sh = fmaf(tap(v, j), tap(v, j), p.sh);
   // tricubic value by separable contraction: z, then y, then x
   float t1[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q)
-    t1[q] = fmaf(wh[2][3], v[4 * q + 3], fmaf(wh[2][2], v[4 * q + 2], fmaf(wh[2][1], v[4 * q + 1], wh[2][0] * v[4 * q])));
+    t1[q] = fmaf(wh[2][3], tap(v, 4 * q + 3), fmaf(wh[2][2], tap(v, 4 * q + 2),
+                 fmaf(wh[2][1], tap(v, 4 * q + 1), wh[2][0] * tap(v, 4 * q))));
   float tr = 0.f;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
@@ -261,22 +291,15 @@ __device__ __forceinline__ float scale_of(float ss0, float ss1, float ss2, float
   return (mode != 0.f ? sqrtf(sh / 162.f) : sqrtf(ss / 192.f)) + 1e-30f;
 }
 
-// The 64 features of one component as 32 packed bf16 pairs.
-__device__ __forceinline__ void comp_features(const float (&v)[64], const float* __restrict__ fs, float inv,
-                                              unsigned (&w)[32]) {
+// The 64 features of one component as 32 packed bf16 pairs: feature j = (tap j * inv) * fs[j],
+// the two products of a pair of taps (j, j + 32) as packed instructions.  fs2[i] = (fs[i], fs[i + 32]).
+__device__ __forceinline__ void comp_features(const float2 (&v)[32], const float2* fs2, float inv, unsigned (&w)[32]) {
+  float2 x[32];
+  const float2 inv2 = make_float2(inv, inv);
 #pragma unroll
-  for (int j = 0; j < 32; ++j)
-    w[j] = pack2(v[2 * j] * inv * fs[2 * j], v[2 * j + 1] * inv * fs[2 * j + 1]);
-}
-
-// The same, with the scales read four at a time (16-byte aligned copy in shared memory).
-__device__ __forceinline__ void comp_features4(const float (&v)[64], const float4* fs4, float inv, unsigned (&w)[32]) {
+  for (int i = 0; i < 32; ++i) x[i] = __fmul2_rn(__fmul2_rn(v[i], inv2), fs2[i]);
 #pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const float4 f = fs4[q];
-    w[2 * q] = pack2(v[4 * q] * inv * f.x, v[4 * q + 1] * inv * f.y);
-    w[2 * q + 1] = pack2(v[4 * q + 2] * inv * f.z, v[4 * q + 3] * inv * f.w);
-  }
+  for (int j = 0; j < 32; ++j) w[j] = pack2(tap(x, 2 * j), tap(x, 2 * j + 1));
 }
 
 // The offset part of a row (columns 192..207): t - 1/2 for the three canonical offsets, zeros.
@@ -305,7 +328,7 @@ __device__ __forceinline__ unsigned canon_offset(const int* ci, int code, int N,
 // symmetrically, so callers apply it exactly where it matters (features, canonical tricubic).
 template <typename T>
 __device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4, int N, const PtFrame& f, int c,
-                                                  float (&v)[64]) {
+                                                  float2 (&v)[32]) {
   const int d = frame_perm(f.code, c);
   const float sg = frame_sign(f.code, d);
   unsigned o0[4], o1[4], o2[4];
@@ -323,7 +346,7 @@ __device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4
     for (int j1 = 0; j1 < 4; ++j1) {
       const unsigned o01 = o0[j0] + o1[j1];
 #pragma unroll
-      for (int j2 = 0; j2 < 4; ++j2) v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (o01 + o2[j2])));
+      for (int j2 = 0; j2 < 4; ++j2) set_tap(v, 16 * j0 + 4 * j1 + j2, float(__ldg(base + (o01 + o2[j2]))));
     }
   return sg;
 }
@@ -332,7 +355,7 @@ __device__ __forceinline__ float gather_component(const vec4<T>* __restrict__ u4
 // computed elsewhere.
 template <typename T>
 __device__ __forceinline__ float gather_component_at(const vec4<T>* __restrict__ u4, const PtFrame& f, int c,
-                                                     const unsigned (&o)[3][4], float (&v)[64]) {
+                                                     const unsigned (&o)[3][4], float2 (&v)[32]) {
   const int d = frame_perm(f.code, c);
   const float sg = frame_sign(f.code, d);
   const T* base = reinterpret_cast<const T*>(u4);
@@ -342,7 +365,7 @@ __device__ __forceinline__ float gather_component_at(const vec4<T>* __restrict__
     for (int j1 = 0; j1 < 4; ++j1) {
       const unsigned o01 = o[0][j0] + (unsigned)d + o[1][j1];
 #pragma unroll
-      for (int j2 = 0; j2 < 4; ++j2) v[16 * j0 + 4 * j1 + j2] = float(__ldg(base + (o01 + o[2][j2])));
+      for (int j2 = 0; j2 < 4; ++j2) set_tap(v, 16 * j0 + 4 * j1 + j2, float(__ldg(base + (o01 + o[2][j2]))));
     }
   return sg;
 }
@@ -361,23 +384,26 @@ __device__ __forceinline__ float point_features(const vec4<T>* __restrict__ u4, 
   CompSums cs[3];
   float sgc[3];
   for (int c = 0; c < 3; ++c) {
-    float v[64];
+    float2 v[32];
     sgc[c] = gather_component<T>(u4, N, f, c, v);
     comp_transform(v);
     cs[c] = comp_sums(v, wh);
 #pragma unroll
-    for (int j = 0; j < 64; ++j) st[64 * c + j] = v[j];
+    for (int j = 0; j < 64; ++j) st[64 * c + j] = tap(v, j);
   }
   const float scale = scale_of(cs[0].ss, cs[1].ss, cs[2].ss, cs[0].sh, cs[1].sh, cs[2].sh, params[OFF_OS + 1]);
   const float inv = 1.f / scale;
   const float* fs = params + OFF_FS;
+  float2 fs2[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) fs2[i] = make_float2(fs[i], fs[i + 32]);
   unsigned* rw = reinterpret_cast<unsigned*>(row);
   for (int c = 0; c < 3; ++c) {
-    float v[64];
+    float2 v[32];
 #pragma unroll
-    for (int j = 0; j < 64; ++j) v[j] = st[64 * c + j];
+    for (int j = 0; j < 64; ++j) set_tap(v, j, st[64 * c + j]);
     unsigned w[32];
-    comp_features(v, fs, sgc[c] * inv, w);
+    comp_features(v, fs2, sgc[c] * inv, w);
 #pragma unroll
     for (int j = 0; j < 32; ++j) rw[32 * c + j] = w[j];
   }
@@ -499,8 +525,8 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
   const int lane = threadIdx.x & 31;
   const int r = lane < 3 * FDROP ? lane / 3 : FDROP - 1;
   const int c = lane < 3 * FDROP ? lane - 3 * r : 0;
-  __shared__ __align__(16) float fs[64];  // feature scales, read as warp-uniform float4
-  if (threadIdx.x < 64) fs[threadIdx.x] = params[OFF_FS + threadIdx.x];
+  __shared__ __align__(16) float2 fs2[32];  // feature scales as pairs (fs[i], fs[i + 32]), warp-uniform reads
+  if (threadIdx.x < 32) fs2[threadIdx.x] = make_float2(params[OFF_FS + threadIdx.x], params[OFF_FS + 32 + threadIdx.x]);
   __syncthreads();
   const float mode = params[OFF_OS + 1];
   const long long ngroups = (n + FDROP - 1) / FDROP;
@@ -547,7 +573,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
           wh[k][j] = __shfl_sync(0xffffffffu, wc[j], b0 + k);
         }
     }
-    float v[64];
+    float2 v[32];
     const float sg = gather_component_at<T>(u4, f, c, o, v);
     comp_transform(v);
     const CompSums cs = comp_sums(v, wh, mode == 0.f);
@@ -559,7 +585,7 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
     const float scale = scale_of(ss0, ss1, ss2, sh0, sh1, sh2, mode);
     if (lane < 3 * FDROP && i < n) {
       unsigned w[32];
-      comp_features4(v, reinterpret_cast<const float4*>(fs), sg * (1.f / scale), w);
+      comp_features(v, fs2, sg * (1.f / scale), w);
       unsigned char* tb = reinterpret_cast<unsigned char*>(Xg) + (i / TM) * TILE_X_BYTES;
       const int rr = (int)(i % TM);
 #pragma unroll
