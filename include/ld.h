@@ -354,7 +354,10 @@ LD_API int ld_deposit_pull(const uint32_t* sval, const int32_t* cs, const double
 
 /* ---- collisions (no counterpart in the reference: droplets there never collide) ----------- */
 /* A collider owns the workspace of the cell-list search for up to nmax droplets on an
- * nc x nc x nc cell grid (nc = floor(L / cell_size), cell_size >= 2 * max radius, nc >= 1). */
+ * nc x nc x nc cell grid (nc = floor(L / cell_size), nc >= 1).  Any cell size gives the same
+ * pairs: with nc >= 3, a droplet whose diameter exceeds the cell width L / nc also searches the
+ * cells within its diameter (its partners with ri + rj > L / nc), so cells narrower than the
+ * largest diameter cut the candidates of a wide radius distribution. */
 LD_API int ld_collider_create(ld_collider** collider, int64_t nmax, int32_t nc);
 /* A collider for the droplets of nbox independent boxes (each an nc^3 cell grid of the same side
  * L; no counterpart in the reference): cells are keyed box-major, so one sort and one search

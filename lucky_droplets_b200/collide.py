@@ -15,7 +15,10 @@ def _torch():
 
 
 class Collider:
-    """Workspace for the collision search of up to ``nmax`` droplets with cells >= cell_size."""
+    """Workspace for the collision search of up to ``nmax`` droplets with cells >= cell_size.
+    Any cell size gives the same pairs; cells near the typical diameter (rather than the largest)
+    test far fewer candidates when the radii spread widely, the few droplets wider than a cell
+    searching further out."""
 
     def __init__(self, nmax, cell_size, L=TWO_PI, device=None, nbox=1):
         """nbox > 1: one collider for the droplets of nbox independent boxes of side L (cells keyed
@@ -91,9 +94,10 @@ class Collider:
 
 def main(argv=None):
     """Time the collision search alone on seeded droplets (uniform positions, lognormal radii
-    r = 0.002 2pi exp(0.3 Z), cells of 2 r_max: about 5 droplets per cell at 1e6 droplets).
+    r = 0.002 2pi exp(0.3 Z); cells of 2 r_max by default: about 5 droplets per cell at 1e6
+    droplets; --cell sets the cell size).
 
-        python -m lucky_droplets_b200.collide [--n 1000000] [--calls 20]
+        python -m lucky_droplets_b200.collide [--n 1000000] [--calls 20] [--cell C]
     """
     import argparse
     import json
@@ -103,12 +107,13 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--calls", type=int, default=20)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cell", type=float, default=None)
     a = ap.parse_args(argv)
     rng = np.random.default_rng(a.seed)
     pos = torch.as_tensor(rng.uniform(0, TWO_PI, (a.n, 3))).cuda()
     rad_np = 0.002 * TWO_PI * np.exp(0.3 * rng.standard_normal(a.n))
     rad = torch.as_tensor(rad_np).cuda()
-    col = Collider(a.n, 2 * float(rad_np.max()))
+    col = Collider(a.n, a.cell or 2 * float(rad_np.max()))
     pairs = torch.empty((max(1024, 4 * a.n), 2), dtype=torch.int32, device="cuda")
     for _ in range(3):
         col.collide(pos, rad, pairs)
@@ -120,8 +125,8 @@ def main(argv=None):
                                     ptr(col.count), stream_ptr(None)))
     e1.record()
     torch.cuda.synchronize()
-    print(json.dumps({"n": a.n, "cells_per_side": col.nc, "pairs": int(col.count.item()),
-                      "ms_per_call": e0.elapsed_time(e1) / a.calls}), flush=True)
+    print(json.dumps({"n": a.n, "cells_per_side": col.nc, "wide": int((rad_np > 0.5 * col.L / col.nc).sum()),
+                      "pairs": int(col.count.item()), "ms_per_call": e0.elapsed_time(e1) / a.calls}), flush=True)
 
 
 if __name__ == "__main__":

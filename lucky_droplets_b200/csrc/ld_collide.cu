@@ -11,6 +11,9 @@
 //   count     per sorted droplet: partners among the cell itself and its 13 forward neighbours
 //             (the first KEEP of them recorded)
 //   scan      exclusive scan of the counts in sorted order -> offsets, total
+//   wide      droplets with 2 r > cell width ("wide"; none when the cell width is at least twice
+//             the largest radius) also search the cells within 2 r of them for the partners
+//             with ri + rj > cell width, which the neighbour search leaves out (below)
 //   emit      pairs at offset + t in the fixed visiting order (copied from the record, or searched
 //             again for droplets with more partners), then mapped to droplet ids (i < j)
 // The FP64 arithmetic (wrap, cell index, minimum image, squared distance) is done with explicit
@@ -74,10 +77,21 @@ __global__ void k_cell_scatter(const unsigned* __restrict__ key, const unsigned*
     run[cs[key[i]] + rank[i]] = (unsigned)i;
 }
 
+// Wide droplets (radius above half the cell width), listed by sorted index while sorting.
+struct WideList {
+  double hw;        // half the cell width
+  unsigned* list;   // sorted indices, in no particular order
+  unsigned* count;  // zeroed before the sort
+};
+
+__device__ __forceinline__ void note_wide(const WideList& w, long long s, double r) {
+  if (r > w.hw) w.list[atomicAdd(w.count, 1u)] = (unsigned)s;
+}
+
 // Sorted copies of one sorted slot: cell key, wrapped FP64 position + radius, FP32 copy.
 __device__ __forceinline__ void sorted_slot(long long s, unsigned k, unsigned i, const double* __restrict__ pos,
                                             const double* __restrict__ rad, double L, unsigned* __restrict__ skey,
-                                            double4* __restrict__ sp, float4* __restrict__ spf) {
+                                            double4* __restrict__ sp, float4* __restrict__ spf, const WideList& w) {
   double4 q;
   q.x = wrapL(pos[3 * (long long)i], L);
   q.y = wrapL(pos[3 * (long long)i + 1], L);
@@ -86,6 +100,7 @@ __device__ __forceinline__ void sorted_slot(long long s, unsigned k, unsigned i,
   skey[s] = k;
   sp[s] = q;
   spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+  note_wide(w, s, q.w);
 }
 
 constexpr int kSmallCell = 64;  // cells up to this occupancy are placed by rank counting
@@ -98,7 +113,7 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
                              const unsigned* __restrict__ run, long long n, const double* __restrict__ pos,
                              const double* __restrict__ rad, double L, unsigned* __restrict__ sval,
                              unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf,
-                             unsigned* __restrict__ big, unsigned* __restrict__ nbig) {
+                             unsigned* __restrict__ big, unsigned* __restrict__ nbig, WideList wide) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const unsigned k = key[i];
     const int s0 = cs[k], s1 = cs[k + 1];
@@ -110,7 +125,7 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
     for (int j = s0; j < s1; ++j) r += run[j] < (unsigned)i ? 1 : 0;
     const int s = s0 + r;
     sval[s] = (unsigned)i;
-    sorted_slot(s, k, (unsigned)i, pos, rad, L, skey, sp, spf);
+    sorted_slot(s, k, (unsigned)i, pos, rad, L, skey, sp, spf, wide);
   }
 }
 
@@ -120,7 +135,8 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
 __global__ void __launch_bounds__(512)
 k_cell_big(const int* __restrict__ cs, const unsigned* __restrict__ big, const unsigned* __restrict__ nbig,
            unsigned* __restrict__ run, const double* __restrict__ pos, const double* __restrict__ rad, double L,
-           unsigned* __restrict__ sval, unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf) {
+           unsigned* __restrict__ sval, unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf,
+           WideList wide) {
   const unsigned nb = *nbig;
   for (unsigned b = blockIdx.x; b < nb; b += gridDim.x) {
     const unsigned k = big[b];
@@ -143,7 +159,7 @@ k_cell_big(const int* __restrict__ cs, const unsigned* __restrict__ big, const u
     }
     for (int x = threadIdx.x; x < m; x += blockDim.x) {
       sval[s0 + x] = v[x];
-      sorted_slot(s0 + x, k, v[x], pos, rad, L, skey, sp, spf);
+      sorted_slot(s0 + x, k, v[x], pos, rad, L, skey, sp, spf, wide);
     }
     __syncthreads();
   }
@@ -270,7 +286,7 @@ __global__ void k_cell_starts(const unsigned* __restrict__ skey, long long n, lo
 
 __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __restrict__ rad,
                               const unsigned* __restrict__ sval, long long n, double L, double4* __restrict__ sp,
-                              float4* __restrict__ spf) {
+                              float4* __restrict__ spf, WideList wide) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const unsigned i = sval[s];
     double4 q;
@@ -280,6 +296,7 @@ __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __re
     q.w = rad[i];
     sp[s] = q;
     spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
+    note_wide(wide, s, q.w);
   }
 }
 
@@ -297,6 +314,12 @@ __device__ __forceinline__ bool overlap(const double4 a, const double4 b, double
   const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
   const double rs = __dadd_rn(a.w, b.w);
   return d2 < __dmul_rn(rs, rs);
+}
+
+// The pairs the neighbour-cell search reports: overlapping with ri + rj <= cw (always true when
+// cw >= 2 max radius; the others are found by the wide droplets' search).
+__device__ __forceinline__ bool overlap_near(const double4 a, const double4 b, double L, double cw) {
+  return !(__dadd_rn(a.w, b.w) > cw) && overlap(a, b, L);
 }
 
 // MODE 0: count partners per droplet id; MODE 1: emit pairs.  DEDUP: nc < 3, where the 27
@@ -402,8 +425,8 @@ __device__ __forceinline__ void col_offset(int q, int& ox, int& oy) {
 template <bool STAGED>
 __device__ __forceinline__ void col_visit(int i, int t, const double4* __restrict__ sp, const float4* __restrict__ spf,
                                           const float4* colbuf, const int* cst, const int* dl, const float* shx,
-                                          const float* shy, int cz, int nc, double L, float Lf, float margin,
-                                          unsigned* __restrict__ cnt, int* __restrict__ scr) {
+                                          const float* shy, int cz, int nc, double L, double cw, float Lf,
+                                          float margin, unsigned* __restrict__ cnt, int* __restrict__ scr) {
   const float4 mf = STAGED ? colbuf[t] : spf[i];
   const float mar = margin + 1e-6f * mf.w;
   unsigned c = 0;
@@ -437,7 +460,7 @@ __device__ __forceinline__ void col_visit(int i, int t, const double4* __restric
       const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
       const float rr = mf.w + b.w + mar;
       if (dxf * dxf + dyf * dyf + dzf * dzf >= rr * rr) continue;
-      if (!overlap(sp[i], sp[g], L)) continue;
+      if (!overlap_near(sp[i], sp[g], L, cw)) continue;
       if (c < KEEP) scr[(long long)KEEP * i + c] = g;
       ++c;
     }
@@ -448,8 +471,8 @@ __device__ __forceinline__ void col_visit(int i, int t, const double4* __restric
 template <int CT>  // threads per block: fewer for sparse columns (a multi-box collider's small boxes)
 __global__ void __launch_bounds__(CT)
 k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
-            const int* __restrict__ cs, int nc, int parts, double L, int cap_smem, unsigned* __restrict__ cnt,
-            int* __restrict__ scr) {
+            const int* __restrict__ cs, int nc, int parts, double L, double cw, int cap_smem,
+            unsigned* __restrict__ cnt, int* __restrict__ scr) {
   extern __shared__ __align__(16) unsigned char cp_smem[];
   float4* colbuf = reinterpret_cast<float4*>(cp_smem);
   int* cst = reinterpret_cast<int*>(cp_smem + sizeof(float4) * (size_t)cap_smem);  // 5 x (nc + 1) cell starts
@@ -499,15 +522,16 @@ k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, cons
   for (int t = part * CT + threadIdx.x; t < len0; t += parts * CT) {
     const int i = lo[0] + t;
     const int cz = (int)(skey[i] - (unsigned)kq[0]);
-    if (staged) col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, Lf, margin, cnt, scr);
-    else col_visit<false>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, Lf, margin, cnt, scr);
+    if (staged) col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr);
+    else col_visit<false>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr);
   }
 }
 
 // Pairs of sorted droplet i at off[i]..: copied from scr when it has at most KEEP partners,
-// otherwise found again from global memory in the same visiting order.
+// otherwise found again from global memory in the same visiting order.  Wide droplets (scr
+// marked by k_wide_count) are left to k_wide_emit.
 __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf,
-                             const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc, double L,
+                             const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc, double L, double cw,
                              long long n, const unsigned* __restrict__ off, const int* __restrict__ scr,
                              int* __restrict__ pairs, long long cap) {
   const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
@@ -515,6 +539,7 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
     const int i = (int)ii;
     const long long o0 = off[i];
     const unsigned cnt = off[i + 1] - off[i];
+    if (cnt == 0 || scr[(long long)KEEP * i] < 0) continue;
     if (cnt <= (unsigned)KEEP) {
       for (unsigned k = 0; k < cnt; ++k)
         if (o0 + k < cap) { pairs[2 * (o0 + k)] = i; pairs[2 * (o0 + k) + 1] = scr[(long long)KEEP * i + k]; }
@@ -539,11 +564,164 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
       const int g1 = cs[k + 1];
       for (int g = r == 0 ? i + 1 : cs[k]; g < g1; ++g) {
         if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
-        if (!overlap(me, sp[g], L)) continue;
+        if (!overlap_near(me, sp[g], L, cw)) continue;
         if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
         ++o;
       }
     }
+  }
+}
+
+// ---- wide droplets ------------------------------------------------------------------------------
+// A pair with ri + rj > cw (cw the cell width) has at least one droplet with 2 r > cw, a wide
+// droplet.  It is reported once, by its owner: the droplet of larger radius (equal radii: the
+// smaller sorted index), which is wide.  The owner s searches every cell within R = floor(2 rs /
+// cw) + 1 cells of its own along each axis (all nc when 2 R + 1 >= nc), since its partner is closer
+// than rs + rt <= 2 rs.  The owner's pairs follow the pairs of its neighbour-cell search in its
+// run of the output.  Work items of a wide droplet: the 14 cells of the neighbour search (emit
+// only), then the cells of the wide search in (x, y, z) order; a block of WIDE_THREADS threads
+// takes them in contiguous runs, counts, scans the counts and writes, so the order is that of a
+// serial visit.
+constexpr int WIDE_THREADS = 128;
+constexpr int kWideBlocks = 2 * 148;
+
+struct WideCell {
+  long long kb;  // the box's first cell
+  int cx, cy, cz, R, ax;  // home cell, reach, cells per axis visited
+};
+
+__device__ __forceinline__ WideCell wide_cell(unsigned key, int nc, double r, double cw) {
+  WideCell w;
+  const unsigned nc3 = (unsigned)nc * nc * nc;
+  w.kb = (long long)(key / nc3) * nc3;
+  w.cz = (int)(key % (unsigned)nc);
+  w.cy = (int)((key / nc) % nc);
+  w.cx = (int)((key / ((unsigned)nc * nc)) % nc);
+  const double rr = floor(__ddiv_rn(__dadd_rn(r, r), cw));
+  w.R = rr < (double)nc ? (int)rr + 1 : nc;
+  w.ax = 2 * w.R + 1 >= nc ? nc : 2 * w.R + 1;
+  return w;
+}
+
+// Visit work item `it` of wide droplet s: WRITE 0 counts, 1 writes at pairs[o...]; returns the hits.
+template <bool WRITE>
+__device__ unsigned wide_item(int it, bool with_near, int s, const WideCell& w, const double4& me, const float4& mf,
+                              const double4* __restrict__ sp, const float4* __restrict__ spf, const int* __restrict__ cs,
+                              int nc, double L, double cw, float Lf, float hf, float mar, int* __restrict__ pairs,
+                              long long o, long long cap) {
+  unsigned c = 0;
+  if (with_near && it < 14) {  // the neighbour search of k_emit_pairs, segment r = it
+    const int r = it;
+    const int q = r < 2 ? 0 : 1 + (r - 2) / 3;
+    const int dz = r < 2 ? r : (r - 2) % 3 - 1;
+    const int z = (w.cz + dz + nc) % nc;
+    const int ox = q < 2 ? 0 : 1;
+    const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+    const long long k = w.kb + ((long long)((w.cx + ox) % nc) * nc + (w.cy + oy + nc) % nc) * nc + z;
+    const int g1 = cs[k + 1];
+    for (int g = r == 0 ? s + 1 : cs[k]; g < g1; ++g) {
+      if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
+      if (!overlap_near(me, sp[g], L, cw)) continue;
+      if (WRITE && o + c < cap) { pairs[2 * (o + c)] = s; pairs[2 * (o + c) + 1] = g; }
+      ++c;
+    }
+    return c;
+  }
+  const int m = with_near ? it - 14 : it;
+  const int wz = m % w.ax, wy = (m / w.ax) % w.ax, wx = m / (w.ax * w.ax);
+  const int x = w.ax == nc ? wx : (w.cx - w.R + wx + nc) % nc;
+  const int y = w.ax == nc ? wy : (w.cy - w.R + wy + nc) % nc;
+  const int z = w.ax == nc ? wz : (w.cz - w.R + wz + nc) % nc;
+  const long long k = w.kb + ((long long)x * nc + y) * nc + z;
+  const int g1 = cs[k + 1];
+  for (int g = cs[k]; g < g1; ++g) {
+    if (g == s || !near_f(mf, spf[g], Lf, hf, mar)) continue;
+    const double4 b = sp[g];
+    if (!(__dadd_rn(me.w, b.w) > cw)) continue;  // reported by the neighbour search
+    if (b.w > 0.5 * cw && (b.w > me.w || (b.w == me.w && g < s))) continue;  // g owns the pair
+    if (!overlap(me, b, L)) continue;
+    if (WRITE && o + c < cap) { pairs[2 * (o + c)] = s; pairs[2 * (o + c) + 1] = g; }
+    ++c;
+  }
+  return c;
+}
+
+// Block-wide exclusive scan of one count per thread (WIDE_THREADS threads); returns the prefix,
+// *total the sum.
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsum, unsigned* total) {
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  unsigned x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += y;
+  }
+  if (lane == 31) wsum[wp] = x;
+  __syncthreads();
+  unsigned before = 0, all = 0;
+#pragma unroll
+  for (int q = 0; q < WIDE_THREADS / 32; ++q) {
+    before += q < wp ? wsum[q] : 0u;
+    all += wsum[q];
+  }
+  __syncthreads();
+  *total = all;
+  return before + x - v;
+}
+
+// Block per wide droplet (grid-stride over the list): its wide-search partners are added to its
+// count, and its record is marked (scr = -1) so that k_emit_pairs leaves it to k_wide_emit.
+__global__ void __launch_bounds__(WIDE_THREADS)
+k_wide_count(const unsigned* __restrict__ wlist, const unsigned* __restrict__ nwide, const double4* __restrict__ sp,
+             const float4* __restrict__ spf, const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc,
+             double L, double cw, unsigned* __restrict__ cnt, int* __restrict__ scr) {
+  __shared__ unsigned wsum[WIDE_THREADS / 32];
+  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
+  const unsigned nw = *nwide;
+  for (unsigned e = blockIdx.x; e < nw; e += gridDim.x) {
+    const int s = (int)wlist[e];
+    const double4 me = sp[s];
+    const float4 mf = spf[s];
+    const WideCell w = wide_cell(skey[s], nc, me.w, cw);
+    const int items = w.ax * w.ax * w.ax;
+    const int per = (items + WIDE_THREADS - 1) / WIDE_THREADS;
+    unsigned c = 0;
+    for (int it = threadIdx.x * per; it < items && it < (int)(threadIdx.x + 1) * per; ++it)
+      c += wide_item<false>(it, false, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, margin + 1e-6f * mf.w, nullptr,
+                            0, 0);
+    unsigned total;
+    block_excl_scan(c, wsum, &total);
+    if (threadIdx.x == 0) {
+      cnt[s] += total;
+      scr[(long long)KEEP * s] = -1;
+    }
+  }
+}
+
+// Block per wide droplet: all its pairs (neighbour search, then wide search) at off[s]...
+__global__ void __launch_bounds__(WIDE_THREADS)
+k_wide_emit(const unsigned* __restrict__ wlist, const unsigned* __restrict__ nwide, const double4* __restrict__ sp,
+            const float4* __restrict__ spf, const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc,
+            double L, double cw, const unsigned* __restrict__ off, int* __restrict__ pairs, long long cap) {
+  __shared__ unsigned wsum[WIDE_THREADS / 32];
+  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
+  const unsigned nw = *nwide;
+  for (unsigned e = blockIdx.x; e < nw; e += gridDim.x) {
+    const int s = (int)wlist[e];
+    const double4 me = sp[s];
+    const float4 mf = spf[s];
+    const float mar = margin + 1e-6f * mf.w;
+    const WideCell w = wide_cell(skey[s], nc, me.w, cw);
+    const int items = 14 + w.ax * w.ax * w.ax;
+    const int per = (items + WIDE_THREADS - 1) / WIDE_THREADS;
+    const int i0 = threadIdx.x * per, i1 = i0 + per < items ? i0 + per : items;
+    unsigned c = 0;
+    for (int it = i0; it < i1; ++it)
+      c += wide_item<false>(it, true, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, mar, nullptr, 0, 0);
+    unsigned total;
+    long long o = (long long)off[s] + block_excl_scan(c, wsum, &total);
+    for (int it = i0; it < i1; ++it)
+      o += wide_item<true>(it, true, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, mar, pairs, o, cap);
   }
 }
 
@@ -612,6 +790,8 @@ struct ld_collider {
   int* scr = nullptr;  // first KEEP partners of each sorted droplet
   unsigned* status = nullptr;
   unsigned* nbig = nullptr;  // number of cells above kSmallCell droplets (counting sort)
+  unsigned* wide = nullptr;  // sorted indices of the wide droplets (radius above half a cell)
+  unsigned* nwide = nullptr;
   unsigned* sums = nullptr;  // scan tile totals
   int nblocks = 0;
   ld_plan* trace = nullptr;  // plan whose event trace records this collider's launches
@@ -663,6 +843,8 @@ int ld_collider_create_boxes(ld_collider** out, int64_t nmax, int32_t nc, int32_
   A((void**)&c->scr, sizeof(int) * KEEP * nmax);
   A((void**)&c->status, sizeof(unsigned));
   A((void**)&c->nbig, sizeof(unsigned));
+  A((void**)&c->wide, sizeof(unsigned) * nmax);
+  A((void**)&c->nwide, sizeof(unsigned));
   {
     long long m = (nmax + 1) > (long long)RADIX * c->nblocks ? (nmax + 1) : (long long)RADIX * c->nblocks;
     if (ncell + 1 > m) m = ncell + 1;
@@ -683,6 +865,8 @@ int ld_collider_destroy(ld_collider* c) {
   cudaFree(c->key); cudaFree(c->val); cudaFree(c->key2); cudaFree(c->val2); cudaFree(c->hist);
   cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->scr); cudaFree(c->status);
   cudaFree(c->nbig);
+  cudaFree(c->wide);
+  cudaFree(c->nwide);
   cudaFree(c->sums);
   delete c;
   return LD_OK;
@@ -733,8 +917,10 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
     LD_CUDA_CHECK(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
     return LD_OK;
   }
+  const WideList wide{0.5 * cw, c->wide, c->nwide};
   {
     ProfScope ps(c->trace, KID_COLL_SORT, s);
+    LD_CUDA_CHECK(cudaMemsetAsync(c->nwide, 0, sizeof(unsigned), s));
     if (ncell + 1 > (long long)SCAN_TILE * SCAN_TILE) {
       // more cells than one scan handles: stable radix sort of the keys, starts by binary search
       k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val, box);
@@ -742,7 +928,7 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
       while ((1LL << bits) < ncell) ++bits;
       if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
       k_cell_starts<<<gridn(ncell + 1, 256), 256, 0, s>>>(c->key, n, ncell, c->start);
-      k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf);
+      k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf, wide);
     } else {
       // counting sort by cell (the same order): keys (c->key2) and arrival ranks (c->val2),
       // occupancies -> starts in c->start, unordered runs scattered into c->cnt, then every
@@ -755,9 +941,9 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
       if (int rc = scan_u32(c, occ, ncell + 1, s)) return rc;
       k_cell_scatter<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->val2, c->start, n, c->cnt);
       k_cell_place<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->start, c->cnt, n, pos, radius, L, c->val, c->key, c->sp,
-                                                 c->spf, c->val2, c->nbig);
+                                                 c->spf, c->val2, c->nbig, wide);
       k_cell_big<<<148, 512, 0, s>>>(c->start, c->val2, c->nbig, c->cnt, pos, radius, L, c->val, c->key, c->sp,
-                                     c->spf);
+                                     c->spf, wide);
     }
   }
   ProfScope ps(c->trace, KID_COLL_PAIRS, s);
@@ -782,20 +968,26 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
     if (per_col <= 64) {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_col_pairs<64><<<(unsigned)(ncol * parts), 64, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
-                                                                 cap_smem, c->cnt, c->scr);
+                                                                 cw, cap_smem, c->cnt, c->scr);
     } else if (per_col <= 128) {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_col_pairs<128><<<(unsigned)(ncol * parts), 128, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
-                                                                   cap_smem, c->cnt, c->scr);
+                                                                   cw, cap_smem, c->cnt, c->scr);
     } else {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<COL_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
       k_col_pairs<COL_THREADS><<<(unsigned)(ncol * parts), COL_THREADS, smem, s>>>(
-          c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cap_smem, c->cnt, c->scr);
+          c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cw, cap_smem, c->cnt, c->scr);
     }
+    // wide droplets (a block each; none unless the cells are narrower than twice the largest
+    // radius): their partners beyond the neighbour cells
+    k_wide_count<<<kWideBlocks, WIDE_THREADS, 0, s>>>(c->wide, c->nwide, c->sp, c->spf, c->key, c->start, nc, L, cw,
+                                                      c->cnt, c->scr);
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
-    k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, n, c->cnt, c->scr, pairs,
+    k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, cw, n, c->cnt, c->scr, pairs,
                                                cap);
+    k_wide_emit<<<kWideBlocks, WIDE_THREADS, 0, s>>>(c->wide, c->nwide, c->sp, c->spf, c->key, c->start, nc, L, cw,
+                                                     c->cnt, pairs, cap);
     k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + n, cap, c->val, pairs);
     if (box_counts)
       k_box_counts_sorted<<<(c->nbox + 255) / 256, 256, 0, s>>>(c->cnt, c->start, nc3, c->nbox, box_counts);

@@ -97,8 +97,6 @@ __device__ __forceinline__ float silu(float z) {
   const float h = 0.5f * z;
   return fmaf(h, tanh_fast(h), h);
 }
-// SiLU given h = z / 2 (the same arithmetic as silu(z) from there on).
-__device__ __forceinline__ float silu_half(float h) { return fmaf(h, tanh_fast(h), h); }
 __device__ __forceinline__ float dsilu(float z) {
   const float s = sigm(z);
   return s * (1.f + z * (1.f - s));
@@ -793,9 +791,17 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
           unsigned w[16];
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
+            // h = fma(0.5, acc, b / 2) and SiLU = fma(h, tanh(h), h) two columns at a time (packed
+            // FP32 pairs: the same roundings as the scalar forms)
             const float4 b4 = b4p[j];
-            w[2 * j] = pack2(silu_half(fmaf(0.5f, v[4 * j], b4.x)), silu_half(fmaf(0.5f, v[4 * j + 1], b4.y)));
-            w[2 * j + 1] = pack2(silu_half(fmaf(0.5f, v[4 * j + 2], b4.z)), silu_half(fmaf(0.5f, v[4 * j + 3], b4.w)));
+            const float2 h0 = __ffma2_rn(make_float2(0.5f, 0.5f), make_float2(v[4 * j], v[4 * j + 1]),
+                                         make_float2(b4.x, b4.y));
+            const float2 h1 = __ffma2_rn(make_float2(0.5f, 0.5f), make_float2(v[4 * j + 2], v[4 * j + 3]),
+                                         make_float2(b4.z, b4.w));
+            const float2 s0 = __ffma2_rn(h0, make_float2(tanh_fast(h0.x), tanh_fast(h0.y)), h0);
+            const float2 s1 = __ffma2_rn(h1, make_float2(tanh_fast(h1.x), tanh_fast(h1.y)), h1);
+            w[2 * j] = pack2(s0.x, s0.y);
+            w[2 * j + 1] = pack2(s1.x, s1.y);
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q)

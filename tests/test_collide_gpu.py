@@ -249,3 +249,85 @@ def test_multi_box_collider_matches_each_box_alone():
         col.cell_order_boxes(P, Bx, order)
         ob = box[order.cpu().numpy()]
         assert (np.diff(ob) >= 0).all()
+
+
+@pytest.mark.parametrize("case", ["lognormal", "equal_radii", "huge_droplet"])
+def test_narrow_cells_find_every_pair(torch, case):
+    """Cells narrower than twice the largest radius: droplets with 2 r above the cell width search
+    the cells within 2 r of them for the partners the neighbour cells leave out.  The list equals
+    the FP64 rule's (computed with cells of 2 r_max), is the same from call to call, and matches
+    the oracle's restatement of the narrow-cell search."""
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng({"lognormal": 61, "equal_radii": 62, "huge_droplet": 63}[case])
+    n = 30000
+    pos = rng.uniform(-1.0, TWO_PI + 1.0, (n, 3))
+    if case == "lognormal":
+        rad = 0.02 * np.exp(0.5 * rng.standard_normal(n))
+    elif case == "equal_radii":
+        rad = np.full(n, 0.03)
+    else:
+        rad = 0.01 + 0.01 * rng.random(n)
+        rad[[5, 900, 20000]] = [1.1, 0.4, 0.4]
+    # cells of 2 r_max; with the droplet of radius 1.1 (fewer than three cells per side: an
+    # all-pairs search) the oracle's narrow-cell restatement, pinned to all pairs on the CPU
+    ref = (K.collide(pos, rad, 2 * rad.max()) if case != "huge_droplet"
+           else K.collide_wide(pos, rad, 4 * np.median(rad)))
+    assert len(ref) > 500
+    p, r = torch.as_tensor(pos).cuda(), torch.as_tensor(rad).cuda()
+    for cell in (rad.max(), 1.5 * np.median(rad), 1.1 * np.median(rad)):
+        nc = K.cell_count(TWO_PI, cell)
+        assert nc >= 3 and (rad > 0.5 * TWO_PI / nc).any()
+        got, c = gpu_pairs(torch, pos, rad, cell, cap=4 * len(ref))
+        assert got.shape == ref.shape and np.array_equal(got, ref), cell
+        a = c.collide(p, r, cap=4 * len(ref)).cpu().numpy()
+        b = c.collide(p, r, cap=4 * len(ref)).cpu().numpy()
+        assert np.array_equal(a, b)
+    assert np.array_equal(K.collide_wide(pos[:2000], rad[:2000], 1.5 * np.median(rad)),
+                          gpu_pairs(torch, pos[:2000], rad[:2000], 1.5 * np.median(rad))[0])
+
+
+def test_narrow_cells_multi_box_and_overflow(torch):
+    """Narrow cells in a multi-box collider: wide droplets search only their own box, the per-box
+    counts include their pairs; a capacity below the total raises the overflow flag."""
+    from lucky_droplets_b200.collide import Collider
+    rng = np.random.default_rng(71)
+    sizes = [4000, 2500, 0, 6000]
+    pos = [rng.uniform(0.0, TWO_PI, (m, 3)) for m in sizes]
+    rad = [0.04 * np.exp(0.6 * rng.standard_normal(m)) for m in sizes]
+    box = np.concatenate([np.full(m, j, np.int32) for j, m in enumerate(sizes)])
+    P = torch.as_tensor(np.concatenate(pos)).cuda()
+    R = torch.as_tensor(np.concatenate(rad)).cuda()
+    Bx = torch.as_tensor(box).cuda()
+    n = int(P.shape[0])
+    cell = 2.0 * float(np.median(np.concatenate(rad)))
+    col = Collider(n, cell, nbox=len(sizes))
+    pairs = torch.empty((8 * n, 2), dtype=torch.int32, device="cuda")
+    col.collide_boxes(P, R, Bx, pairs)
+    m = int(col.count.item())
+    got = pairs[:m].cpu().numpy().astype(np.int64)
+    assert (box[got[:, 0]] == box[got[:, 1]]).all()
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    bc = col.box_counts.cpu().numpy()
+    total = 0
+    for j, nj in enumerate(sizes):
+        sel = np.sort(got[box[got[:, 0]] == j] - off[j], axis=1)
+        sel = sel[np.lexsort((sel[:, 1], sel[:, 0]))] if len(sel) else sel.reshape(0, 2)
+        ref = K.collide(pos[j], rad[j], 2 * rad[j].max()) if nj else np.zeros((0, 2), np.int64)
+        assert np.array_equal(sel, ref), j
+        assert bc[j] == len(ref)
+        total += len(ref)
+    assert m == total > 100
+    # overflow: the count is still the total, the flag is raised, nothing is written past cap
+    small = torch.full((total // 2, 2), -7, dtype=torch.int32, device="cuda")
+    guard = torch.full((64, 2), -7, dtype=torch.int32, device="cuda")
+    buf = torch.cat([small, guard])
+    col.status()
+    col.collide_boxes(P, R, Bx, buf[: total // 2])
+    assert int(col.count.item()) == total
+    assert col.status() & _lib_status_overflow()
+    assert (buf[total // 2:] == -7).all()
+
+
+def _lib_status_overflow():
+    from lucky_droplets_b200 import _lib
+    return _lib.STATUS_PAIR_OVERFLOW

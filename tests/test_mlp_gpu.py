@@ -161,3 +161,42 @@ def test_training_beats_tricubic(torch):
     li.rule = "tolerance"
     li.judge(cube, li.interleaved(cube), pos)
     assert not li.enabled  # the default rule: off above the tolerance
+
+
+def test_inference_features_equal_training_features(torch):
+    """The warp-cooperative inference kernel (three lanes per droplet, one canonical component
+    each, sums exchanged by shuffles) and the thread-per-sample training kernel produce the same
+    feature rows, tricubic values and scales, bit for bit, at the same points."""
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    N, per = 32, 3000
+    prm = C.ConfigParams(N=N, nu=0.01, dt=1e-3)
+    uk, _ = C.init_flow(C.ConfigGrid(N), prm, seed=11)
+    plan = Plan(N, "f32")
+    li = G.LearnedInterp(plan, seed=2)
+    cube = plan.to_cube(torch.as_tensor(uk).to("cuda", plan.cdtype).contiguous())
+    seed = 5
+    X, _, _, aux = li.make_samples(cube, 1, per, seed=seed)
+    rng = np.random.default_rng(seed)
+    s = rng.uniform(0.0, 1.0, 3)
+    idx = rng.integers(0, N ** 3, per, dtype=np.int64)
+    j = np.stack([idx // (N * N), (idx // N) % N, idx % N], axis=1).astype(np.float64)
+    pos = (j + s) * (2.0 * np.pi / N)
+    work = li.workspace(per)
+    li.infer(li.interleaved(cube), torch.as_tensor(pos).cuda(), work=work)
+    torch.cuda.synchronize()
+    wb = work.cpu().numpy()
+    tile_bytes = 128 * G.K1 * 2
+    tiles = (per + 127) // 128
+    rows = np.arange(per)
+    t, rr = rows // 128, rows % 128
+    feat = np.empty((per, G.K1), np.uint16)
+    for kc in range(G.K1 // 8):
+        off = t * tile_bytes + (kc * 16 + rr // 8) * 128 + (rr % 8) * 16  # the tile layout
+        chunk = wb[off[:, None] + np.arange(16)[None, :]]
+        feat[:, 8 * kc:8 * kc + 8] = chunk.view(np.uint16).reshape(per, 8)
+    ref = X.view(torch.int16).cpu().numpy().view(np.uint16)
+    assert np.array_equal(feat, ref)
+    ax = wb[tiles * tile_bytes:].view(np.float32)[:8 * per].reshape(per, 8)
+    a = aux.cpu().numpy()
+    assert np.array_equal(ax[:, :3], a[:, :3]) and np.array_equal(ax[:, 3], a[:, 3])

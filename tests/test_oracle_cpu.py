@@ -1,7 +1,7 @@
 """CPU checks of two oracles the GPU parity tests rest on: the cell-list collision search of
 oracle/collide_np.py returns exactly the pairs of its all-pairs FP64 rule (empty and single
 inputs, 1, 2, 3 and many cells per axis, droplets outside [0, L), pairs across the periodic
-faces, coincident droplets), and the direct Fourier sum of oracle/exact_np.py equals the inverse
+faces, coincident droplets, cells narrower than twice the largest radius), and the direct Fourier sum of oracle/exact_np.py equals the inverse
 transform at grid points and moves with a phase shift of the spectrum."""
 import numpy as np
 import pytest
@@ -39,6 +39,36 @@ def test_pairs_across_periodic_faces_and_coincident_droplets():
     got = K.collide(pos, rad, 2 * r)
     assert np.array_equal(got, K.collide_bruteforce(pos, rad))
     assert [tuple(p) for p in got] == [(0, 1), (2, 3), (4, 5), (6, 7)]
+
+
+@pytest.mark.parametrize("case", ["lognormal", "equal_radii", "huge_droplet", "dense"])
+def test_narrow_cells_equal_all_pairs(case):
+    """Cells narrower than twice the largest radius (collide_wide): the neighbour-cell search plus
+    the wide droplets' owner search give exactly the all-pairs list; equal radii exercise the
+    owner tie rule, a droplet of radius L/3 a search over every cell."""
+    rng = np.random.default_rng({"lognormal": 1, "equal_radii": 2, "huge_droplet": 3, "dense": 4}[case])
+    n = 2500
+    pos = rng.uniform(-1.0, L + 1.0, (n, 3))
+    if case == "lognormal":
+        rad = 0.05 * np.exp(0.6 * rng.standard_normal(n))
+    elif case == "equal_radii":
+        rad = np.full(n, 0.12)
+    elif case == "huge_droplet":
+        rad = 0.03 * rng.random(n) + 0.01
+        rad[7] = L / 3
+    else:
+        pos = rng.uniform(1.0, 2.0, (n, 3))
+        rad = 0.03 * np.exp(0.4 * rng.standard_normal(n))
+    ref = K.collide_bruteforce(pos, rad)
+    assert len(ref) > 50
+    wide = 0
+    for cell in (rad.max(), 2.5 * np.median(rad), 1.2 * np.median(rad)):
+        nc = K.cell_count(L, cell)
+        if nc < 3:
+            continue
+        wide += int((rad > 0.5 * L / nc).sum())
+        assert np.array_equal(K.collide_wide(pos, rad, cell), ref), cell
+    assert wide > 0
 
 
 def _flow(N, seed):
