@@ -307,9 +307,11 @@ def build_workload(a, seed, precision=None, interp=None, droplets=True, N=None):
         u = dns.velocity()
         d.vel.copy_(d.gather(u))  # droplets start at the interpolated fluid velocity
         del u
-        # collision cells of 2 max radius; colliding pairs found after every step; droplets
-        # re-sorted into that cell order every sort_every steps
-        col = Collider(a.nd, 2.0 * float(radius.max()), device=dns.plan.device)
+        # collision cells of twice the 0.9999 radius quantile (the few wider droplets search the
+        # cells within their diameter); colliding pairs found after every step; droplets
+        # re-sorted into cell order every sort_every steps
+        from lucky_droplets_b200.collide import cell_size_for
+        col = Collider(a.nd, cell_size_for(radius), device=dns.plan.device)
         dns.attach(d, collider=col, sort_every=a.sort_every)
     torch.cuda.synchronize()
     return dns, d

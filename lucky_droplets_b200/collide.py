@@ -14,6 +14,18 @@ def _torch():
     return torch
 
 
+def cell_size_for(radius, n=None, L=TWO_PI, wide_fraction=1e-4):
+    """A cell size for radii spread like ``radius`` (array): twice the radius below which all but
+    ``wide_fraction`` of the droplets lie, so that few droplets are wide, kept to at least 3 and
+    at most about (4 n)^(1/3) cells per side."""
+    import numpy as np
+    r = np.asarray(radius, dtype=np.float64)
+    n = int(n if n is not None else r.size)
+    cell = 2.0 * float(np.quantile(r, 1.0 - wide_fraction)) if r.size else L / 3
+    nc_max = max(3, int(round((4.0 * max(n, 1)) ** (1.0 / 3.0))))
+    return min(max(cell, L / nc_max), L / 3)
+
+
 class Collider:
     """Workspace for the collision search of up to ``nmax`` droplets with cells >= cell_size.
     Any cell size gives the same pairs; cells near the typical diameter (rather than the largest)

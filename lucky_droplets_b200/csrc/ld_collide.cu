@@ -582,8 +582,8 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
 // only), then the cells of the wide search in (x, y, z) order; a block of WIDE_THREADS threads
 // takes them in contiguous runs, counts, scans the counts and writes, so the order is that of a
 // serial visit.
-constexpr int WIDE_THREADS = 128;
-constexpr int kWideBlocks = 2 * 148;
+constexpr int WIDE_THREADS = 256;  // one work item per thread for reaches up to two cells
+constexpr int kWideBlocks = 148;
 
 struct WideCell {
   long long kb;  // the box's first cell
