@@ -138,17 +138,30 @@ struct SyncWarp {
 };
 
 // Shared-memory slot of element p of a row buffer (sstride = 1) when PAD is set.
-//   8-byte elements (complex float): p ^ ((p >> 4) & 15), a permutation inside each 128-byte line
+//   8-byte elements (complex float): p ^ mask(p / 16), a permutation inside each 128-byte line
 //   (16 elements) keyed by the line index: the contiguous reads of every stage stay on whole
 //   lines (two wavefronts per warp) and the stride-E writes of stage 0 and the grouped writes of
-//   the middle stages spread over all 32 banks (two wavefronts for N = 256, E = 8).
+//   the middle stages spread over the banks.  A warp's 8-byte accesses are served half a warp at
+//   a time, so the sixteen elements of each half must fall in distinct bank pairs: mask = the
+//   line index (p >> 4) & 15 achieves it for every access but the stage-1 writes of N = 256,
+//   E = 8 (two-way conflicts), which the mixed mask below removes for that size.
 //   16-byte elements (complex double): one spare slot per E elements (p + p / E), which spreads
 //   the stride-E writes; a warp needs four wavefronts for these anyway.
 // Without PAD: p (column buffers, sstride = columns per block).
-template <typename T, int E, bool PAD> __device__ __forceinline__ int sidx(int p) {
-  if constexpr (!PAD) return p;
-  else if constexpr (sizeof(T) == 4) return p ^ ((p >> 4) & 15);
-  else return p + (p >> ilog2(E));
+template <typename T, int N, int E, bool PAD> __device__ __forceinline__ int sidx(int p) {
+  if constexpr (!PAD) {
+    return p;
+  } else if constexpr (sizeof(T) == 4 && N == 256 && E == 8) {
+    // 256-point rows of 32 threads (the fused z pass at 256^3): the line index b mixed with b << 1
+    // (checked over that row's accesses of 8-byte elements — stage-0 and stage-1 writes, stage-1
+    // and stage-2 reads, the forward pair's split — by enumerating each half-warp's bank pairs)
+    const int b = (p >> 4) & 15;
+    return p ^ ((b ^ (b << 1)) & 15);
+  } else if constexpr (sizeof(T) == 4) {
+    return p ^ ((p >> 4) & 15);
+  } else {
+    return p + (p >> ilog2(E));
+  }
 }
 
 // In-place length-3 and length-5 DFTs (forward sign exp(-2 pi i jk / R); INV conjugates).  The
@@ -235,7 +248,7 @@ __device__ __forceinline__ void fft_stage_mr(cplx<T>* a, cplx<T>* sbuf, int sstr
     const int b = j + NT * q;
     if (FULL || b < NB) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, E, PAD>(b + r * NB) * sstride];
+      for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, N, E, PAD>(b + r * NB) * sstride];
     }
   }
   sync();
@@ -252,7 +265,7 @@ __device__ __forceinline__ void fft_stage_mr(cplx<T>* a, cplx<T>* sbuf, int sstr
       const int base = LAST ? b : (b / Ns) * Ns * R + k;
       constexpr int step = LAST ? NB : Ns;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sbuf[sidx<T, E, PAD>(base + r * step) * sstride] = x[q * R + r];
+      for (int r = 0; r < R; ++r) sbuf[sidx<T, N, E, PAD>(base + r * step) * sstride] = x[q * R + r];
     }
   }
   sync();
@@ -260,7 +273,7 @@ __device__ __forceinline__ void fft_stage_mr(cplx<T>* a, cplx<T>* sbuf, int sstr
     fft_stage_mr<T, N, E, INV, PAD, s + 1>(a, sbuf, sstride, j, tw, sync);
   } else {
 #pragma unroll
-    for (int m = 0; m < E; ++m) a[m] = sbuf[sidx<T, E, PAD>(j + NT * m) * sstride];
+    for (int m = 0; m < E; ++m) a[m] = sbuf[sidx<T, N, E, PAD>(j + NT * m) * sstride];
   }
 }
 
@@ -279,7 +292,7 @@ __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride
   for (int q = 0; q < Q; ++q) {
     const int b = j + NT * q;
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, E, PAD>(b + r * (N / R)) * sstride];
+    for (int r = 0; r < R; ++r) x[q * R + r] = sbuf[sidx<T, N, E, PAD>(b + r * (N / R)) * sstride];
   }
   sync();
 #pragma unroll
@@ -292,7 +305,7 @@ __device__ __forceinline__ void fft_stage(cplx<T>* a, cplx<T>* sbuf, int sstride
     if constexpr (s < S - 1) {
       const int base = (b / Ns) * Ns * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sbuf[sidx<T, E, PAD>(base + r * Ns) * sstride] = x[q * R + r];
+      for (int r = 0; r < R; ++r) sbuf[sidx<T, N, E, PAD>(base + r * Ns) * sstride] = x[q * R + r];
     } else {
 #pragma unroll
       for (int r = 0; r < R; ++r) a[q + r * Q] = x[q * R + r];
@@ -314,14 +327,14 @@ __device__ __forceinline__ void fft_run(cplx<T>* a, cplx<T>* sbuf, int sstride, 
     using Sh = FftShape<N, E>;
     if constexpr (Sh::S > 1) {
 #pragma unroll
-      for (int r = 0; r < E; ++r) sbuf[sidx<T, E, PAD>(j * E + r) * sstride] = a[r];
+      for (int r = 0; r < E; ++r) sbuf[sidx<T, N, E, PAD>(j * E + r) * sstride] = a[r];
       sync();
       fft_stage<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
     }
   } else {
     static_assert(MrShape<N, E>::S > 1, "mixed-radix lengths have later stages");
 #pragma unroll
-    for (int r = 0; r < E; ++r) sbuf[sidx<T, E, PAD>(j * E + r) * sstride] = a[r];
+    for (int r = 0; r < E; ++r) sbuf[sidx<T, N, E, PAD>(j * E + r) * sstride] = a[r];
     sync();
     fft_stage_mr<T, N, E, INV, PAD, 1>(a, sbuf, sstride, j, tw, sync);
   }

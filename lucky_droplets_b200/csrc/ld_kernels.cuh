@@ -558,7 +558,7 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
 template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ == 32), SyncWarp, SyncBlock>::type;
 // Row-buffer slot of element i: the same map as the FFT exchange of the row (sidx with PAD).
 template <typename T, int N> struct ZIdx {
-  static __device__ __forceinline__ int p(int i) { return sidx<T, Cfg<N>::EZ, true>(i); }
+  static __device__ __forceinline__ int p(int i) { return sidx<T, N, Cfg<N>::EZ, true>(i); }
 };
 
 // Hermitian-extended load of Y[k] = A[k] + i B[k] (k = j + NT m), A/B spectral rows with Kin
@@ -597,7 +597,8 @@ __device__ __forceinline__ void zload_pair(cplx<T>* a, const cplx<T>* A, const c
 }
 
 // After a forward FFT of (a + i b): split Y into A[k], B[k] for k < Kout (zero for k >= Kval).
-// Writes Y to the row buffer first; caller must have synced the buffer.
+// Rows of one warp exchange the mirrored coefficients by shuffles; narrower rows write Y to the
+// row buffer first (the caller must have synced the buffer).
 template <typename T, int N, class Sync>
 __device__ __forceinline__ void zstore_pair(const cplx<T>* a, cplx<T>* sb, cplx<T>* A, cplx<T>* B,
                                             int Kout, int Kval, int j, bool ok, Sync sync) {
@@ -607,6 +608,29 @@ __device__ __forceinline__ void zstore_pair(const cplx<T>* a, cplx<T>* sb, cplx<
     for (int m = 0; m < E; ++m) {
       const int k = j + NT * m;
       if (ok && k < Kout) A[k] = k < Kval ? a[m] : czero<cplx<T>>();
+    }
+    return;
+  }
+  if constexpr (NT == 32) {
+    // a row per warp: Y[N - k] (Y[0] for k = 0) is register E - 1 - m of lane 32 - j (j > 0), or
+    // register (E - m) % E of lane 0 (j = 0), fetched by shuffles instead of through the buffer
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int k = j + NT * m;
+      cplx<T> z;
+      z.x = __shfl_sync(0xffffffffu, a[E - 1 - m].x, (NT - j) & (NT - 1));
+      z.y = __shfl_sync(0xffffffffu, a[E - 1 - m].y, (NT - j) & (NT - 1));
+      if (j == 0) z = a[(E - m) % E];
+      if (ok && k < Kout) {
+        cplx<T> ra = czero<cplx<T>>(), rb = czero<cplx<T>>();
+        if (k < Kval) {
+          const cplx<T> y = a[m];
+          ra = cmk(T(0.5) * (y.x + z.x), T(0.5) * (y.y - z.y));
+          rb = cmk(T(0.5) * (y.y + z.y), T(-0.5) * (y.x - z.x));
+        }
+        A[k] = ra;
+        B[k] = rb;
+      }
     }
     return;
   }
