@@ -77,7 +77,6 @@ template <typename T> struct RowsIO {
   long long fs, os;
   int rs;
   int kc;  // < 0: identity row map
-  T scale;
   __device__ __forceinline__ long long at(int f, int o, int r, int col) const {
     return (long long)f * fs + (long long)o * os + (long long)r * rs + col;
   }
@@ -91,8 +90,7 @@ template <typename T, int N> struct LdRows {
   __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
     const int r = io.kc < 0 ? n : crow(n, N, io.kc);
     if (r < 0) return czero<cplx<T>>();
-    cplx<T> v = io.p[io.at(f, o, r, col)];
-    return cscale(v, io.scale);
+    return io.p[io.at(f, o, r, col)];
   }
 };
 
@@ -105,15 +103,13 @@ template <typename T, int N> struct StRows {
   }
 };
 
-// Strided row loader: rows mapped to compact cube rows through crow (MAP) or taken as they are,
-// scaled by io.scale.
+// Strided row loader: rows mapped to compact cube rows through crow (MAP) or taken as they are.
 template <typename T, int N, bool MAP> struct LdRowsC {
   RowsIO<T> io;
   __device__ __forceinline__ cplx<T> operator()(int f, int o, int n, int col) const {
     const int r = MAP ? crow(n, N, Cfg<N>::KC) : n;  // io.kc == Cfg<N>::KC for cube rows
     if (r < 0) return czero<cplx<T>>();
-    cplx<T> v = io.p[io.at(f, o, r, col)];
-    return cscale(v, io.scale);
+    return io.p[io.at(f, o, r, col)];
   }
 };
 
@@ -291,7 +287,7 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
     for (int m = 0; m < E; ++m) {
       const int n = j + NT * m;
       const int r = IN_MAP ? crow(n, N, in.kc) : n;
-      a[m] = (ok && r >= 0) ? cscale(cur[n * TB + c], in.scale) : czero<cplx<T>>();
+      a[m] = (ok && r >= 0) ? cur[n * TB + c] : czero<cplx<T>>();
     }
     __syncthreads();  // every value is in registers: cur becomes the exchange buffer
     const unsigned nx = it + gridDim.x;

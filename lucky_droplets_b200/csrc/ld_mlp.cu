@@ -686,19 +686,24 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   // bar_mma; each counter has one writer (a group leader; cnt[0] leaves out the first copy, which
   // thread 0 issues before the loop) and thread 0 reads them after the final barrier
   unsigned* cnt = reinterpret_cast<unsigned*>(sm + SM_CNT);  // [x_issued 2][x_waited 2][mma_commit 2][mma_wait 2]
-  // weights into the tile layout (from the packed, row-padded copies)
+  // weights into the tile layout (from the packed, row-padded copies); consecutive threads take
+  // consecutive rows of one 16-byte K chunk, so that eight of them fill one 128-byte core-matrix
+  // line (a quarter-warp's stores on distinct banks; with chunks fastest the stores of a warp
+  // fell 2 KB apart, on the same banks)
+#pragma unroll 4
   for (int e = tid; e < H * (K1 / 8); e += FT_THREADS) {
-    const int nrow = e / (K1 / 8), kc = e % (K1 / 8);
+    const int nrow = e % H, kc = e / H;
     *reinterpret_cast<uint4*>(sm + SM_W1 + blk_off(nrow, kc, H)) =
         *reinterpret_cast<const uint4*>(packed + P_W1T + nrow * KP1 + 8 * kc);
   }
+#pragma unroll 4
   for (int e = tid; e < H * (H / 8); e += FT_THREADS) {
-    const int nrow = e / (H / 8), kc = e % (H / 8);
+    const int nrow = e % H, kc = e / H;
     *reinterpret_cast<uint4*>(sm + SM_W2 + blk_off(nrow, kc, H)) =
         *reinterpret_cast<const uint4*>(packed + P_W2T + nrow * KP2 + 8 * kc);
   }
   for (int e = tid; e < N3P * (H / 8); e += FT_THREADS) {
-    const int nrow = e / (H / 8), kc = e % (H / 8);
+    const int nrow = e % N3P, kc = e / N3P;
     uint4 v = make_uint4(0u, 0u, 0u, 0u);
     if (nrow < N3) v = *reinterpret_cast<const uint4*>(packed + P_W3T + nrow * KP2 + 8 * kc);
     *reinterpret_cast<uint4*>(sm + SM_W3 + blk_off(nrow, kc, N3P)) = v;

@@ -81,9 +81,9 @@ template <typename T, int N> struct Ops {
     }
   }
 
-  static RowsIO<T> io(const void* p, long long fs, long long os, int rs, int kc, T scale = T(1)) {
+  static RowsIO<T> io(const void* p, long long fs, long long os, int rs, int kc) {
     RowsIO<T> r;
-    r.p = (C*)p; r.fs = fs; r.os = os; r.rs = rs; r.kc = kc; r.scale = scale;
+    r.p = (C*)p; r.fs = fs; r.os = os; r.rs = rs; r.kc = kc;
     return r;
   }
 
