@@ -256,18 +256,26 @@ k_colfft_pipe(RowsIO<T> in, St st, int ncols, int nf, int nouter, const cplx<T>*
     const unsigned fo = rest / (unsigned)nf;
     return Item{(int)(it - rest * ncb), (int)(rest - fo * (unsigned)nf), (int)fo};
   };
+  // each thread copies one fixed 16-byte chunk k of rows threadIdx / CPR + (THREADS / CPR) i
+  constexpr int THREADS = Cfg<N>::COL_THREADS;
+  static_assert(THREADS % CPR == 0 && (N * CPR) % THREADS == 0, "whole rows per pass of the block");
+  const int kq = threadIdx.x % CPR, n0 = threadIdx.x / CPR;
   auto prefetch = [&](const Item& itm, cplx<T>* dst) {
     const int col0 = itm.cb * TB;
     const int w = ncols - col0 < TB ? ncols - col0 : TB;
     const int cpr = w * (int)sizeof(cplx<T>) / 16;
-    for (int q = threadIdx.x; q < N * CPR; q += blockDim.x) {
-      const int n = q / CPR, k = q - n * CPR;
-      if (k >= cpr) continue;
-      const int r = IN_MAP ? crow(n, N, in.kc) : n;
-      if (r < 0) continue;
-      const char* src = reinterpret_cast<const char*>(in.p + in.at(itm.f, itm.o, r, col0)) + 16 * k;
-      const unsigned d = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst + n * TB) + 16 * k);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    if (kq < cpr) {
+      const char* src0 = reinterpret_cast<const char*>(in.p + in.at(itm.f, itm.o, 0, col0)) + 16 * kq;
+      const unsigned d0 = (unsigned)__cvta_generic_to_shared(reinterpret_cast<char*>(dst) + 16 * kq);
+#pragma unroll
+      for (int i = 0; i < N * CPR / THREADS; ++i) {
+        const int n = n0 + (THREADS / CPR) * i;
+        const int r = IN_MAP ? crow(n, N, in.kc) : n;
+        if (r < 0) continue;
+        const char* src = src0 + (long long)r * in.rs * (long long)sizeof(cplx<T>);
+        const unsigned d = d0 + (unsigned)(n * TB * (int)sizeof(cplx<T>));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+      }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
