@@ -13,7 +13,8 @@
 //   scan      exclusive scan of the counts in sorted order -> offsets, total
 //   wide      droplets with 2 r > cell width ("wide"; none when the cell width is at least twice
 //             the largest radius) also search the cells within 2 r of them for the partners
-//             with ri + rj > cell width, which the neighbour search leaves out (below)
+//             with ri + rj > cell width, which the neighbour search leaves out: counted by the
+//             block of the column visit that meets them, emitted by the block of the emit pass
 //   emit      pairs at offset + t in the fixed visiting order (copied from the record, or searched
 //             again for droplets with more partners), then mapped to droplet ids (i < j)
 // The FP64 arithmetic (wrap, cell index, minimum image, squared distance) is done with explicit
@@ -77,21 +78,10 @@ __global__ void k_cell_scatter(const unsigned* __restrict__ key, const unsigned*
     run[cs[key[i]] + rank[i]] = (unsigned)i;
 }
 
-// Wide droplets (radius above half the cell width), listed by sorted index while sorting.
-struct WideList {
-  double hw;        // half the cell width
-  unsigned* list;   // sorted indices, in no particular order
-  unsigned* count;  // zeroed before the sort
-};
-
-__device__ __forceinline__ void note_wide(const WideList& w, long long s, double r) {
-  if (r > w.hw) w.list[atomicAdd(w.count, 1u)] = (unsigned)s;
-}
-
 // Sorted copies of one sorted slot: cell key, wrapped FP64 position + radius, FP32 copy.
 __device__ __forceinline__ void sorted_slot(long long s, unsigned k, unsigned i, const double* __restrict__ pos,
                                             const double* __restrict__ rad, double L, unsigned* __restrict__ skey,
-                                            double4* __restrict__ sp, float4* __restrict__ spf, const WideList& w) {
+                                            double4* __restrict__ sp, float4* __restrict__ spf) {
   double4 q;
   q.x = wrapL(pos[3 * (long long)i], L);
   q.y = wrapL(pos[3 * (long long)i + 1], L);
@@ -100,7 +90,6 @@ __device__ __forceinline__ void sorted_slot(long long s, unsigned k, unsigned i,
   skey[s] = k;
   sp[s] = q;
   spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
-  note_wide(w, s, q.w);
 }
 
 constexpr int kSmallCell = 64;  // cells up to this occupancy are placed by rank counting
@@ -113,7 +102,7 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
                              const unsigned* __restrict__ run, long long n, const double* __restrict__ pos,
                              const double* __restrict__ rad, double L, unsigned* __restrict__ sval,
                              unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf,
-                             unsigned* __restrict__ big, unsigned* __restrict__ nbig, WideList wide) {
+                             unsigned* __restrict__ big, unsigned* __restrict__ nbig) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const unsigned k = key[i];
     const int s0 = cs[k], s1 = cs[k + 1];
@@ -125,7 +114,7 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
     for (int j = s0; j < s1; ++j) r += run[j] < (unsigned)i ? 1 : 0;
     const int s = s0 + r;
     sval[s] = (unsigned)i;
-    sorted_slot(s, k, (unsigned)i, pos, rad, L, skey, sp, spf, wide);
+    sorted_slot(s, k, (unsigned)i, pos, rad, L, skey, sp, spf);
   }
 }
 
@@ -135,8 +124,7 @@ __global__ void k_cell_place(const unsigned* __restrict__ key, const int* __rest
 __global__ void __launch_bounds__(512)
 k_cell_big(const int* __restrict__ cs, const unsigned* __restrict__ big, const unsigned* __restrict__ nbig,
            unsigned* __restrict__ run, const double* __restrict__ pos, const double* __restrict__ rad, double L,
-           unsigned* __restrict__ sval, unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf,
-           WideList wide) {
+           unsigned* __restrict__ sval, unsigned* __restrict__ skey, double4* __restrict__ sp, float4* __restrict__ spf) {
   const unsigned nb = *nbig;
   for (unsigned b = blockIdx.x; b < nb; b += gridDim.x) {
     const unsigned k = big[b];
@@ -159,7 +147,7 @@ k_cell_big(const int* __restrict__ cs, const unsigned* __restrict__ big, const u
     }
     for (int x = threadIdx.x; x < m; x += blockDim.x) {
       sval[s0 + x] = v[x];
-      sorted_slot(s0 + x, k, v[x], pos, rad, L, skey, sp, spf, wide);
+      sorted_slot(s0 + x, k, v[x], pos, rad, L, skey, sp, spf);
     }
     __syncthreads();
   }
@@ -286,7 +274,7 @@ __global__ void k_cell_starts(const unsigned* __restrict__ skey, long long n, lo
 
 __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __restrict__ rad,
                               const unsigned* __restrict__ sval, long long n, double L, double4* __restrict__ sp,
-                              float4* __restrict__ spf, WideList wide) {
+                              float4* __restrict__ spf) {
   for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < n; s += (long long)gridDim.x * blockDim.x) {
     const unsigned i = sval[s];
     double4 q;
@@ -296,7 +284,6 @@ __global__ void k_sorted_copy(const double* __restrict__ pos, const double* __re
     q.w = rad[i];
     sp[s] = q;
     spf[s] = make_float4((float)q.x, (float)q.y, (float)q.z, (float)q.w);
-    note_wide(wide, s, q.w);
   }
 }
 
@@ -422,8 +409,10 @@ __device__ __forceinline__ void col_offset(int q, int& ox, int& oy) {
 }
 
 // The visit of one droplet (sorted index i, t-th of its column); STAGED: positions from colbuf.
+// Returns whether the droplet is wide (2 r > cw: its partners beyond the neighbour cells are
+// counted by the block afterwards).
 template <bool STAGED>
-__device__ __forceinline__ void col_visit(int i, int t, const double4* __restrict__ sp, const float4* __restrict__ spf,
+__device__ __forceinline__ bool col_visit(int i, int t, const double4* __restrict__ sp, const float4* __restrict__ spf,
                                           const float4* colbuf, const int* cst, const int* dl, const float* shx,
                                           const float* shy, int cz, int nc, double L, double cw, float Lf,
                                           float margin, unsigned* __restrict__ cnt, int* __restrict__ scr) {
@@ -466,110 +455,8 @@ __device__ __forceinline__ void col_visit(int i, int t, const double4* __restric
     }
   }
   cnt[i] = c;
-}
-
-template <int CT>  // threads per block: fewer for sparse columns (a multi-box collider's small boxes)
-__global__ void __launch_bounds__(CT)
-k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
-            const int* __restrict__ cs, int nc, int parts, double L, double cw, int cap_smem,
-            unsigned* __restrict__ cnt, int* __restrict__ scr) {
-  extern __shared__ __align__(16) unsigned char cp_smem[];
-  float4* colbuf = reinterpret_cast<float4*>(cp_smem);
-  int* cst = reinterpret_cast<int*>(cp_smem + sizeof(float4) * (size_t)cap_smem);  // 5 x (nc + 1) cell starts
-  __shared__ long long kq[5];
-  __shared__ int lo[5], so[6], dl[5];
-  __shared__ float shx[5], shy[5];
-  const long long colg = blockIdx.x / parts;  // (box, cx, cy) of a multi-box collider
-  const int part = (int)(blockIdx.x % parts);
-  const long long ncol = (long long)nc * nc;
-  const long long bbase = (colg / ncol) * ncol * nc;  // the box's first cell
-  const long long col = colg % ncol;
-  const int cx = (int)(col / nc), cy = (int)(col % nc);
-  const float Lf = (float)L, margin = (float)(1e-6 * L);
-  if (threadIdx.x < 5) {
-    int ox, oy;
-    col_offset(threadIdx.x, ox, oy);
-    kq[threadIdx.x] = bbase + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
-    shx[threadIdx.x] = (cx + ox >= nc) ? -Lf : 0.f;
-    shy[threadIdx.x] = (cy + oy >= nc) ? -Lf : ((cy + oy < 0) ? Lf : 0.f);
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < 5 * (nc + 1); e += CT) {
-    const int q = e / (nc + 1), z = e - q * (nc + 1);
-    cst[e] = cs[kq[q] + z];
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int acc = 0;
-    for (int q = 0; q < 5; ++q) {
-      lo[q] = cst[q * (nc + 1)];
-      so[q] = acc;
-      acc += cst[q * (nc + 1) + nc] - lo[q];
-    }
-    so[5] = acc;
-  }
-  __syncthreads();
-  const bool staged = so[5] <= cap_smem;  // block-uniform
-  if (threadIdx.x < 5) dl[threadIdx.x] = staged ? lo[threadIdx.x] - so[threadIdx.x] : 0;
-  if (staged) {
-    for (int q = 0; q < 5; ++q) {
-      const int n_q = so[q + 1] - so[q];
-      for (int t = threadIdx.x; t < n_q; t += CT) colbuf[so[q] + t] = spf[lo[q] + t];
-    }
-  }
-  __syncthreads();
-  const int len0 = so[1] - so[0];
-  for (int t = part * CT + threadIdx.x; t < len0; t += parts * CT) {
-    const int i = lo[0] + t;
-    const int cz = (int)(skey[i] - (unsigned)kq[0]);
-    if (staged) col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr);
-    else col_visit<false>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr);
-  }
-}
-
-// Pairs of sorted droplet i at off[i]..: copied from scr when it has at most KEEP partners,
-// otherwise found again from global memory in the same visiting order.  Wide droplets (scr
-// marked by k_wide_count) are left to k_wide_emit.
-__global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf,
-                             const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc, double L, double cw,
-                             long long n, const unsigned* __restrict__ off, const int* __restrict__ scr,
-                             int* __restrict__ pairs, long long cap) {
-  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
-  for (long long ii = blockIdx.x * (long long)blockDim.x + threadIdx.x; ii < n; ii += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)ii;
-    const long long o0 = off[i];
-    const unsigned cnt = off[i + 1] - off[i];
-    if (cnt == 0 || scr[(long long)KEEP * i] < 0) continue;
-    if (cnt <= (unsigned)KEEP) {
-      for (unsigned k = 0; k < cnt; ++k)
-        if (o0 + k < cap) { pairs[2 * (o0 + k)] = i; pairs[2 * (o0 + k) + 1] = scr[(long long)KEEP * i + k]; }
-      continue;
-    }
-    const unsigned key = skey[i];
-    const unsigned nc3 = (unsigned)nc * nc * nc;
-    const long long kb = (long long)(key / nc3) * nc3;  // the box's first cell
-    const int cz = (int)(key % (unsigned)nc), cy = (int)((key / nc) % nc), cx = (int)((key / ((unsigned)nc * nc)) % nc);
-    const float4 mf = spf[i];
-    const float mar = margin + 1e-6f * mf.w;
-    const double4 me = sp[i];
-    long long o = o0;
-    for (int r = 0; r < 14; ++r) {
-      int q, dz;
-      if (r < 2) { q = 0; dz = r; }
-      else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
-      const int z = (cz + dz + nc) % nc;
-      const int ox = q < 2 ? 0 : 1;
-      const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
-      const long long k = kb + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc + z;
-      const int g1 = cs[k + 1];
-      for (int g = r == 0 ? i + 1 : cs[k]; g < g1; ++g) {
-        if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
-        if (!overlap_near(me, sp[g], L, cw)) continue;
-        if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
-        ++o;
-      }
-    }
-  }
+  // FP32 radius first (rounding is monotone: r > cw / 2 implies float(r) >= float(cw / 2))
+  return mf.w >= (float)(0.5 * cw) && sp[i].w > 0.5 * cw;
 }
 
 // ---- wide droplets ------------------------------------------------------------------------------
@@ -579,11 +466,10 @@ __global__ void k_emit_pairs(const double4* __restrict__ sp, const float4* __res
 // cw) + 1 cells of its own along each axis (all nc when 2 R + 1 >= nc), since its partner is closer
 // than rs + rt <= 2 rs.  The owner's pairs follow the pairs of its neighbour-cell search in its
 // run of the output.  Work items of a wide droplet: the 14 cells of the neighbour search (emit
-// only), then the cells of the wide search in (x, y, z) order; a block of WIDE_THREADS threads
-// takes them in contiguous runs, counts, scans the counts and writes, so the order is that of a
-// serial visit.
-constexpr int WIDE_THREADS = 256;  // one work item per thread for reaches up to two cells
-constexpr int kWideBlocks = 148;
+// only), then the cells of the wide search in (x, y, z) order; the block that meets a wide droplet
+// (the column visit for the count, the emit pass for the pairs) takes its items in contiguous
+// runs, one run per thread, counts, scans the counts and writes, so the order is that of a serial
+// visit.
 
 struct WideCell {
   long long kb;  // the box's first cell
@@ -646,8 +532,9 @@ __device__ unsigned wide_item(int it, bool with_near, int s, const WideCell& w, 
   return c;
 }
 
-// Block-wide exclusive scan of one count per thread (WIDE_THREADS threads); returns the prefix,
-// *total the sum.
+// Block-wide exclusive scan of one count per thread (NTH threads, all of them calling); returns
+// the prefix, *total the sum.
+template <int NTH>
 __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsum, unsigned* total) {
   const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   unsigned x = v;
@@ -660,7 +547,7 @@ __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsum, 
   __syncthreads();
   unsigned before = 0, all = 0;
 #pragma unroll
-  for (int q = 0; q < WIDE_THREADS / 32; ++q) {
+  for (int q = 0; q < NTH / 32; ++q) {
     before += q < wp ? wsum[q] : 0u;
     all += wsum[q];
   }
@@ -669,28 +556,28 @@ __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned* wsum, 
   return before + x - v;
 }
 
-// Block per wide droplet (grid-stride over the list): its wide-search partners are added to its
-// count, and its record is marked (scr = -1) so that k_emit_pairs leaves it to k_wide_emit.
-__global__ void __launch_bounds__(WIDE_THREADS)
-k_wide_count(const unsigned* __restrict__ wlist, const unsigned* __restrict__ nwide, const double4* __restrict__ sp,
-             const float4* __restrict__ spf, const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc,
-             double L, double cw, unsigned* __restrict__ cnt, int* __restrict__ scr) {
-  __shared__ unsigned wsum[WIDE_THREADS / 32];
+// The block's wide droplets (sorted indices in list[0..nw)), one after another: the partners of
+// the wide search are added to each droplet's count and its record is marked (scr = -1), so that
+// the emit pass writes its pairs by wide_emit_block.
+template <int NTH>
+__device__ void wide_count_block(const unsigned* list, int nw, const double4* __restrict__ sp,
+                                 const float4* __restrict__ spf, const unsigned* __restrict__ skey,
+                                 const int* __restrict__ cs, int nc, double L, double cw, unsigned* __restrict__ cnt,
+                                 int* __restrict__ scr, unsigned* wsum) {
   const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
-  const unsigned nw = *nwide;
-  for (unsigned e = blockIdx.x; e < nw; e += gridDim.x) {
-    const int s = (int)wlist[e];
+  for (int e = 0; e < nw; ++e) {
+    const int s = (int)list[e];
     const double4 me = sp[s];
     const float4 mf = spf[s];
     const WideCell w = wide_cell(skey[s], nc, me.w, cw);
     const int items = w.ax * w.ax * w.ax;
-    const int per = (items + WIDE_THREADS - 1) / WIDE_THREADS;
+    const int per = (items + NTH - 1) / NTH;
     unsigned c = 0;
     for (int it = threadIdx.x * per; it < items && it < (int)(threadIdx.x + 1) * per; ++it)
       c += wide_item<false>(it, false, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, margin + 1e-6f * mf.w, nullptr,
                             0, 0);
     unsigned total;
-    block_excl_scan(c, wsum, &total);
+    block_excl_scan<NTH>(c, wsum, &total);
     if (threadIdx.x == 0) {
       cnt[s] += total;
       scr[(long long)KEEP * s] = -1;
@@ -698,30 +585,163 @@ k_wide_count(const unsigned* __restrict__ wlist, const unsigned* __restrict__ nw
   }
 }
 
-// Block per wide droplet: all its pairs (neighbour search, then wide search) at off[s]...
-__global__ void __launch_bounds__(WIDE_THREADS)
-k_wide_emit(const unsigned* __restrict__ wlist, const unsigned* __restrict__ nwide, const double4* __restrict__ sp,
-            const float4* __restrict__ spf, const unsigned* __restrict__ skey, const int* __restrict__ cs, int nc,
-            double L, double cw, const unsigned* __restrict__ off, int* __restrict__ pairs, long long cap) {
-  __shared__ unsigned wsum[WIDE_THREADS / 32];
+// All pairs of the block's wide droplets (neighbour search, then wide search) at off[s]...
+template <int NTH>
+__device__ void wide_emit_block(const unsigned* list, int nw, const double4* __restrict__ sp,
+                                const float4* __restrict__ spf, const unsigned* __restrict__ skey,
+                                const int* __restrict__ cs, int nc, double L, double cw,
+                                const unsigned* __restrict__ off, int* __restrict__ pairs, long long cap,
+                                unsigned* wsum) {
   const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
-  const unsigned nw = *nwide;
-  for (unsigned e = blockIdx.x; e < nw; e += gridDim.x) {
-    const int s = (int)wlist[e];
+  for (int e = 0; e < nw; ++e) {
+    const int s = (int)list[e];
     const double4 me = sp[s];
     const float4 mf = spf[s];
     const float mar = margin + 1e-6f * mf.w;
     const WideCell w = wide_cell(skey[s], nc, me.w, cw);
     const int items = 14 + w.ax * w.ax * w.ax;
-    const int per = (items + WIDE_THREADS - 1) / WIDE_THREADS;
+    const int per = (items + NTH - 1) / NTH;
     const int i0 = threadIdx.x * per, i1 = i0 + per < items ? i0 + per : items;
     unsigned c = 0;
     for (int it = i0; it < i1; ++it)
       c += wide_item<false>(it, true, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, mar, nullptr, 0, 0);
     unsigned total;
-    long long o = (long long)off[s] + block_excl_scan(c, wsum, &total);
+    long long o = (long long)off[s] + block_excl_scan<NTH>(c, wsum, &total);
     for (int it = i0; it < i1; ++it)
       o += wide_item<true>(it, true, s, w, me, mf, sp, spf, cs, nc, L, cw, Lf, hf, mar, pairs, o, cap);
+  }
+}
+
+template <int CT>  // threads per block: fewer for sparse columns (a multi-box collider's small boxes)
+__global__ void __launch_bounds__(CT)
+k_col_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
+            const int* __restrict__ cs, int nc, int parts, double L, double cw, int cap_smem,
+            unsigned* __restrict__ cnt, int* __restrict__ scr) {
+  extern __shared__ __align__(16) unsigned char cp_smem[];
+  float4* colbuf = reinterpret_cast<float4*>(cp_smem);
+  int* cst = reinterpret_cast<int*>(cp_smem + sizeof(float4) * (size_t)cap_smem);  // 5 x (nc + 1) cell starts
+  __shared__ long long kq[5];
+  __shared__ int lo[5], so[6], dl[5];
+  __shared__ float shx[5], shy[5];
+  __shared__ unsigned wlist[CT], nwide, wsum[CT / 32];
+  if (threadIdx.x == 0) nwide = 0u;
+  const long long colg = blockIdx.x / parts;  // (box, cx, cy) of a multi-box collider
+  const int part = (int)(blockIdx.x % parts);
+  const long long ncol = (long long)nc * nc;
+  const long long bbase = (colg / ncol) * ncol * nc;  // the box's first cell
+  const long long col = colg % ncol;
+  const int cx = (int)(col / nc), cy = (int)(col % nc);
+  const float Lf = (float)L, margin = (float)(1e-6 * L);
+  if (threadIdx.x < 5) {
+    int ox, oy;
+    col_offset(threadIdx.x, ox, oy);
+    kq[threadIdx.x] = bbase + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc;
+    shx[threadIdx.x] = (cx + ox >= nc) ? -Lf : 0.f;
+    shy[threadIdx.x] = (cy + oy >= nc) ? -Lf : ((cy + oy < 0) ? Lf : 0.f);
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < 5 * (nc + 1); e += CT) {
+    const int q = e / (nc + 1), z = e - q * (nc + 1);
+    cst[e] = cs[kq[q] + z];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int q = 0; q < 5; ++q) {
+      lo[q] = cst[q * (nc + 1)];
+      so[q] = acc;
+      acc += cst[q * (nc + 1) + nc] - lo[q];
+    }
+    so[5] = acc;
+  }
+  __syncthreads();
+  const bool staged = so[5] <= cap_smem;  // block-uniform
+  if (threadIdx.x < 5) dl[threadIdx.x] = staged ? lo[threadIdx.x] - so[threadIdx.x] : 0;
+  if (staged) {
+    for (int q = 0; q < 5; ++q) {
+      const int n_q = so[q + 1] - so[q];
+      for (int t = threadIdx.x; t < n_q; t += CT) colbuf[so[q] + t] = spf[lo[q] + t];
+    }
+  }
+  __syncthreads();
+  const int len0 = so[1] - so[0];
+  // rounds of CT droplets; after each, the block counts the round's wide droplets' partners
+  // beyond the neighbour cells together
+  for (int t0 = part * CT; t0 < len0; t0 += parts * CT) {
+    const int t = t0 + threadIdx.x;
+    if (t < len0) {
+      const int i = lo[0] + t;
+      const int cz = (int)(skey[i] - (unsigned)kq[0]);
+      const bool wide =
+          staged ? col_visit<true>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr)
+                 : col_visit<false>(i, t, sp, spf, colbuf, cst, dl, shx, shy, cz, nc, L, cw, Lf, margin, cnt, scr);
+      if (wide) wlist[atomicAdd(&nwide, 1u)] = (unsigned)i;
+    }
+    __syncthreads();
+    const int nw = (int)nwide;  // block-uniform
+    if (nw) wide_count_block<CT>(wlist, nw, sp, spf, skey, cs, nc, L, cw, cnt, scr, wsum);
+    __syncthreads();
+    if (threadIdx.x == 0) nwide = 0u;
+    __syncthreads();
+  }
+}
+
+// Pairs of sorted droplet i at off[i]..: copied from scr when it has at most KEEP partners,
+// otherwise found again from global memory in the same visiting order.  The block takes rounds
+// of EMIT_THREADS droplets; the round's wide droplets (scr marked by the column visit) are
+// emitted by the whole block after the round (wide_emit_block).
+constexpr int EMIT_THREADS = 256;
+
+__global__ void __launch_bounds__(EMIT_THREADS)
+k_emit_pairs(const double4* __restrict__ sp, const float4* __restrict__ spf, const unsigned* __restrict__ skey,
+             const int* __restrict__ cs, int nc, double L, double cw, long long n, const unsigned* __restrict__ off,
+             const int* __restrict__ scr, int* __restrict__ pairs, long long cap) {
+  __shared__ unsigned wlist[EMIT_THREADS], nwide, wsum[EMIT_THREADS / 32];
+  if (threadIdx.x == 0) nwide = 0u;
+  __syncthreads();
+  const float Lf = (float)L, hf = 0.5f * Lf, margin = (float)(1e-6 * L);
+  for (long long base = (long long)blockIdx.x * EMIT_THREADS; base < n; base += (long long)gridDim.x * EMIT_THREADS) {
+    const long long ii = base + threadIdx.x;
+    const int i = (int)ii;
+    const unsigned cnt = ii < n ? off[i + 1] - off[i] : 0u;
+    if (cnt > 0 && scr[(long long)KEEP * i] < 0) {
+      wlist[atomicAdd(&nwide, 1u)] = (unsigned)i;
+    } else if (cnt > 0 && cnt <= (unsigned)KEEP) {
+      const long long o0 = off[i];
+      for (unsigned k = 0; k < cnt; ++k)
+        if (o0 + k < cap) { pairs[2 * (o0 + k)] = i; pairs[2 * (o0 + k) + 1] = scr[(long long)KEEP * i + k]; }
+    } else if (cnt > 0) {
+      const unsigned key = skey[i];
+      const unsigned nc3 = (unsigned)nc * nc * nc;
+      const long long kb = (long long)(key / nc3) * nc3;  // the box's first cell
+      const int cz = (int)(key % (unsigned)nc), cy = (int)((key / nc) % nc), cx = (int)((key / ((unsigned)nc * nc)) % nc);
+      const float4 mf = spf[i];
+      const float mar = margin + 1e-6f * mf.w;
+      const double4 me = sp[i];
+      long long o = off[i];
+      for (int r = 0; r < 14; ++r) {
+        int q, dz;
+        if (r < 2) { q = 0; dz = r; }
+        else { q = 1 + (r - 2) / 3; dz = (r - 2) % 3 - 1; }
+        const int z = (cz + dz + nc) % nc;
+        const int ox = q < 2 ? 0 : 1;
+        const int oy = q == 0 ? 0 : (q == 1 ? 1 : q - 3);
+        const long long k = kb + ((long long)((cx + ox) % nc) * nc + (cy + oy + nc) % nc) * nc + z;
+        const int g1 = cs[k + 1];
+        for (int g = r == 0 ? i + 1 : cs[k]; g < g1; ++g) {
+          if (!near_f(mf, spf[g], Lf, hf, mar)) continue;
+          if (!overlap_near(me, sp[g], L, cw)) continue;
+          if (o < cap) { pairs[2 * o] = i; pairs[2 * o + 1] = g; }
+          ++o;
+        }
+      }
+    }
+    __syncthreads();
+    const int nw = (int)nwide;  // block-uniform
+    if (nw) wide_emit_block<EMIT_THREADS>(wlist, nw, sp, spf, skey, cs, nc, L, cw, off, pairs, cap, wsum);
+    __syncthreads();
+    if (threadIdx.x == 0) nwide = 0u;
+    __syncthreads();
   }
 }
 
@@ -790,8 +810,6 @@ struct ld_collider {
   int* scr = nullptr;  // first KEEP partners of each sorted droplet
   unsigned* status = nullptr;
   unsigned* nbig = nullptr;  // number of cells above kSmallCell droplets (counting sort)
-  unsigned* wide = nullptr;  // sorted indices of the wide droplets (radius above half a cell)
-  unsigned* nwide = nullptr;
   unsigned* sums = nullptr;  // scan tile totals
   int nblocks = 0;
   ld_plan* trace = nullptr;  // plan whose event trace records this collider's launches
@@ -843,8 +861,6 @@ int ld_collider_create_boxes(ld_collider** out, int64_t nmax, int32_t nc, int32_
   A((void**)&c->scr, sizeof(int) * KEEP * nmax);
   A((void**)&c->status, sizeof(unsigned));
   A((void**)&c->nbig, sizeof(unsigned));
-  A((void**)&c->wide, sizeof(unsigned) * nmax);
-  A((void**)&c->nwide, sizeof(unsigned));
   {
     long long m = (nmax + 1) > (long long)RADIX * c->nblocks ? (nmax + 1) : (long long)RADIX * c->nblocks;
     if (ncell + 1 > m) m = ncell + 1;
@@ -865,8 +881,6 @@ int ld_collider_destroy(ld_collider* c) {
   cudaFree(c->key); cudaFree(c->val); cudaFree(c->key2); cudaFree(c->val2); cudaFree(c->hist);
   cudaFree(c->cnt); cudaFree(c->start); cudaFree(c->sp); cudaFree(c->spf); cudaFree(c->scr); cudaFree(c->status);
   cudaFree(c->nbig);
-  cudaFree(c->wide);
-  cudaFree(c->nwide);
   cudaFree(c->sums);
   delete c;
   return LD_OK;
@@ -917,10 +931,8 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
     LD_CUDA_CHECK(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
     return LD_OK;
   }
-  const WideList wide{0.5 * cw, c->wide, c->nwide};
   {
     ProfScope ps(c->trace, KID_COLL_SORT, s);
-    LD_CUDA_CHECK(cudaMemsetAsync(c->nwide, 0, sizeof(unsigned), s));
     if (ncell + 1 > (long long)SCAN_TILE * SCAN_TILE) {
       // more cells than one scan handles: stable radix sort of the keys, starts by binary search
       k_cell_keys<<<gridn(n, 256), 256, 0, s>>>(pos, n, L, cw, nc, c->key, c->val, box);
@@ -928,7 +940,7 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
       while ((1LL << bits) < ncell) ++bits;
       if (int rc = ld_radix_sort_u32(c, c->key, c->val, n, bits, stream)) return rc;
       k_cell_starts<<<gridn(ncell + 1, 256), 256, 0, s>>>(c->key, n, ncell, c->start);
-      k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf, wide);
+      k_sorted_copy<<<gridn(n, 256), 256, 0, s>>>(pos, radius, c->val, n, L, c->sp, c->spf);
     } else {
       // counting sort by cell (the same order): keys (c->key2) and arrival ranks (c->val2),
       // occupancies -> starts in c->start, unordered runs scattered into c->cnt, then every
@@ -941,9 +953,9 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
       if (int rc = scan_u32(c, occ, ncell + 1, s)) return rc;
       k_cell_scatter<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->val2, c->start, n, c->cnt);
       k_cell_place<<<gridn(n, 256), 256, 0, s>>>(c->key2, c->start, c->cnt, n, pos, radius, L, c->val, c->key, c->sp,
-                                                 c->spf, c->val2, c->nbig, wide);
+                                                 c->spf, c->val2, c->nbig);
       k_cell_big<<<148, 512, 0, s>>>(c->start, c->val2, c->nbig, c->cnt, pos, radius, L, c->val, c->key, c->sp,
-                                     c->spf, wide);
+                                     c->spf);
     }
   }
   ProfScope ps(c->trace, KID_COLL_PAIRS, s);
@@ -979,15 +991,9 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
       k_col_pairs<COL_THREADS><<<(unsigned)(ncol * parts), COL_THREADS, smem, s>>>(
           c->sp, c->spf, c->key, c->start, nc, (int)parts, L, cw, cap_smem, c->cnt, c->scr);
     }
-    // wide droplets (a block each; none unless the cells are narrower than twice the largest
-    // radius): their partners beyond the neighbour cells
-    k_wide_count<<<kWideBlocks, WIDE_THREADS, 0, s>>>(c->wide, c->nwide, c->sp, c->spf, c->key, c->start, nc, L, cw,
-                                                      c->cnt, c->scr);
     if (int rc = scan_u32(c, c->cnt, n + 1, s)) return rc;
-    k_emit_pairs<<<gridn(n, 256), 256, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, cw, n, c->cnt, c->scr, pairs,
-                                               cap);
-    k_wide_emit<<<kWideBlocks, WIDE_THREADS, 0, s>>>(c->wide, c->nwide, c->sp, c->spf, c->key, c->start, nc, L, cw,
-                                                     c->cnt, pairs, cap);
+    k_emit_pairs<<<gridn(n, EMIT_THREADS), EMIT_THREADS, 0, s>>>(c->sp, c->spf, c->key, c->start, nc, L, cw, n,
+                                                                 c->cnt, c->scr, pairs, cap);
     k_map_pairs<<<gridn(cap, 256), 256, 0, s>>>(c->cnt + n, cap, c->val, pairs);
     if (box_counts)
       k_box_counts_sorted<<<(c->nbox + 255) / 256, 256, 0, s>>>(c->cnt, c->start, nc3, c->nbox, box_counts);
