@@ -556,10 +556,13 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
 // ------------------------------------------------------------------------------------------
 // z passes (contiguous axis): one thread group of NTZ threads per row unit, inside one warp
 // ------------------------------------------------------------------------------------------
-// Exchange barrier of the z passes: warp-level when a row unit owns a whole warp (N >= 256),
-// block-wide when several row units share a warp (the warp-level form gave wrong results for
-// N <= 32 in the fused pass; the block-wide form is verified at every size).
-template <int N> using ZSync = typename std::conditional<(Cfg<N>::NTZ == 32), SyncWarp, SyncBlock>::type;
+// Exchange barrier of the z passes: warp-level when the row units of a warp lie inside it (a row
+// per warp at N >= 256; at N = 64 and 128 four and two rows per warp, every lane of the warp
+// taking part in every exchange), block-wide for rows that span warps (mixed-radix lengths) and
+// for N <= 32 (where the warp-level form gave wrong results in the fused pass).
+template <int N>
+using ZSync = typename std::conditional<(Cfg<N>::NTZ == 32 || (N >= 64 && Cfg<N>::P2 && 32 % Cfg<N>::NTZ == 0)),
+                                        SyncWarp, SyncBlock>::type;
 // Row-buffer slot of element i: the same map as the FFT exchange of the row (sidx with PAD).
 template <typename T, int N> struct ZIdx {
   static __device__ __forceinline__ int p(int i) { return sidx<T, N, Cfg<N>::EZ, true>(i); }
