@@ -316,6 +316,15 @@ LD_API int64_t ld_mlp_partial_floats(int64_t nb);
  * fixed-order reductions.  grad: n_params floats; loss: 1 float. */
 LD_API int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb, const float* params,
                        const void* packed, float* work, float* grad, float* loss, void* stream);
+/* One epoch of mini-batch training: for batch b = 0 .. nbatch-1, samples order[b*batch ..
+ * (b+1)*batch) of X, T, W (as in ld_mlp_grad) give the loss and gradient, then one Adam step
+ * (step0 + b + 1, learning rate lr * (lr_final / lr)^(min(step, total) / total), or lr when
+ * lr_final <= 0) updates params, m, v and the BF16 copy; *loss_acc += each batch loss.  work:
+ * ld_mlp_partial_floats(batch) floats.  Same result as ld_mlp_grad then ld_mlp_adam per batch on
+ * the gathered rows.  A batch whose kernel gave up a bounded wait adds NaN to *loss_acc. */
+LD_API int ld_mlp_train_epoch(const void* X, const float* T, const float* W, const uint32_t* order, int64_t nbatch,
+                              int64_t batch, float* params, void* packed, float* m, float* v, int64_t step0,
+                              double lr, double lr_final, int64_t total, float* work, float* loss_acc, void* stream);
 /* One Adam step (beta 0.9/0.999, eps 1e-8) on the FP32 parameters, then re-packs the BF16 copy. */
 LD_API int ld_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t step, float lr, void* packed,
                        void* stream);

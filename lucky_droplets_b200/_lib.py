@@ -107,6 +107,8 @@ SIGNATURES = {
     "ld_droplet_update": (_c_i, [_c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_d, _c_p]),
     "ld_mlp_grad": (_c_i, [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]),
     "ld_mlp_adam": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, ctypes.c_float, _c_p, _c_p]),
+    "ld_mlp_train_epoch": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_i64, _c_d,
+                                  _c_d, _c_i64, _c_p, _c_p, _c_p]),
     "ld_collider_create": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32]),
     "ld_collider_create_boxes": (_c_i, [ctypes.POINTER(_c_p), _c_i64, _c_i32, _c_i32]),
     "ld_collide_boxes": (_c_i, [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d, _c_p, _c_i64, _c_p, _c_p, _c_p]),

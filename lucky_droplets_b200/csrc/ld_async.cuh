@@ -39,6 +39,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// bytes (a multiple of 16) from 16-byte aligned shared memory to 16-byte aligned global memory,
+// in the issuing thread's current bulk group
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the issuing thread's committed bulk stores have completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   unsigned ok;
   asm volatile(
@@ -64,9 +75,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 namespace ld {
 
 // ---- 5th-generation tensor cores (tcgen05): tensor memory, MMA issue, commit, loads -----------
-// Shared-memory operand descriptor of a K-major, non-swizzled operand made of 8x8 core matrices
-// (8 rows x 16 bytes, 128 contiguous bytes each): lbo = byte distance between the two K-adjacent
-// core matrices of one MMA (K = 16 bf16), sbo = byte distance between M/N-adjacent 8-row groups.
+// Shared-memory operand descriptor of a non-swizzled operand made of core matrices of 128
+// contiguous bytes (8 lines of 16 bytes): lbo = byte distance between the two K-adjacent core
+// matrices of one MMA (K = 16 bf16), sbo = byte distance between M/N-adjacent core matrices.
+// K-major operands have their K elements along a line (8 M/N rows per core matrix); MN-major
+// operands (bits 15 / 16 of the instruction descriptor) have 8 M/N elements along a line and
+// 8 K rows per core matrix.
 __device__ __forceinline__ uint64_t umma_desc(const void* smem_ptr, unsigned lbo_bytes, unsigned sbo_bytes) {
   const unsigned a = smem_u32(smem_ptr);
   uint64_t d = (uint64_t)((a >> 4) & 0x3FFFu);

@@ -3,7 +3,8 @@
 // fractional cell offset.  No counterpart in the reference.
 //
 // Network: 195 inputs -> 128 SiLU -> 128 SiLU -> 3.  Operands are BF16 on the tensor cores
-// (mma.sync m16n8k16, FP32 accumulation); master weights, biases and the optimiser are FP32.
+// (tcgen05.mma, FP32 accumulators in tensor memory), for inference and training alike; master
+// weights, biases and the optimiser are FP32.
 //
 // Features of a point with stencil values s (192 = 3 components x 64 taps, tap order
 // c*64 + a*16 + b*4 + q for offsets a, b, q in -1..2 along x, y, z) and cell offsets t (3):
@@ -36,6 +37,8 @@
 //   fs [64]       os [8] (os[0]: output scale, os[1]: scale mode)
 // Packed BF16 copies for the tensor cores ("packed"), output-major with padded rows:
 //   W1t [128][KP1]   W2t [128][KP2]   W2n [128][KP2] (= W2, input-major)   W3t [8][KP2]   W3n [128][8]
+//   then W1t, W2t and W3t (16 rows) once more in the tensor-core tile layout (tile_elem), which the
+//   training kernel copies to shared memory as three bulk copies
 #include <cmath>
 
 #include <cuda_bf16.h>
@@ -48,9 +51,8 @@ namespace {
 using namespace ld;
 
 constexpr int D_IN = 195, K1 = 208, H = 128, D_OUT = 3, N3 = 8;
-constexpr int KP1 = 216;  // padded row stride (bf16) of 208-long rows: conflict-free fragment loads
-constexpr int KP2 = 136;  // padded row stride of 128-long rows
-constexpr int XP = 216;   // feature rows in shared memory
+constexpr int KP1 = 216;  // padded row stride (bf16) of the packed 208-long rows
+constexpr int KP2 = 136;  // padded row stride of the packed 128-long rows
 
 constexpr int OFF_W1 = 0;
 constexpr int OFF_B1 = OFF_W1 + K1 * H;
@@ -67,21 +69,24 @@ constexpr int P_W2T = P_W1T + H * KP1;
 constexpr int P_W2N = P_W2T + H * KP2;
 constexpr int P_W3T = P_W2N + H * KP2;
 constexpr int P_W3N = P_W3T + N3 * KP2;
-constexpr int N_PACKED = P_W3N + H * N3;
+constexpr int N3P = 16;                     // layer-3 N padded for M = 128
+constexpr int P_TW1 = P_W3N + H * N3;       // W1 in the tensor-core tile layout (rows o, K = k)
+constexpr int P_TW2 = P_TW1 + H * K1;       // W2 in the tile layout (rows o, K = i)
+constexpr int P_TW3 = P_TW2 + H * H;        // W3 in the tile layout (16 rows c, K = i; rows 3..15 zero)
+constexpr int N_PACKED = P_TW3 + N3P * H;
+static_assert((P_TW1 * 2) % 16 == 0 && (P_TW2 * 2) % 16 == 0 && (P_TW3 * 2) % 16 == 0, "bulk-copy alignment");
+
+// Element index of (row, k) in the tensor-core tile layout of a K-major operand with `rows` rows:
+// 8x8 core matrices (8 rows of 8 consecutive k, 128 contiguous bytes), K-chunk major.
+__host__ __device__ constexpr int tile_elem(int row, int k, int rows) {
+  return ((k / 8) * (rows / 8) + row / 8) * 64 + (row % 8) * 8 + k % 8;
+}
 
 using bf16 = __nv_bfloat16;
 
 __device__ __forceinline__ unsigned pack2(float lo, float hi) {
   const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
   return *reinterpret_cast<const unsigned*>(&v);
-}
-
-__device__ __forceinline__ void mma16816(float* d, const unsigned* a, const unsigned* b) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
 // SiLU with the logistic function from the hardware tanh approximation, sigma(z) = (1 + tanh(z/2))/2
@@ -93,42 +98,13 @@ __device__ __forceinline__ float tanh_fast(float x) {
   return y;
 }
 __device__ __forceinline__ float sigm(float z) { return fmaf(0.5f, tanh_fast(0.5f * z), 0.5f); }
-__device__ __forceinline__ float silu(float z) {
-  const float h = 0.5f * z;
-  return fmaf(h, tanh_fast(h), h);
-}
 __device__ __forceinline__ float dsilu(float z) {
   const float s = sigm(z);
   return s * (1.f + z * (1.f - s));
 }
 
-// Warp tile: 16 rows of A (row-major, stride lda bf16) times B^T given output-major (Bt[n][k],
-// stride ldb): acc[nt][4] for NT n8 tiles over K (multiple of 16).
-template <int NT, int K>
-__device__ __forceinline__ void warp_gemm(float (*acc)[4], const bf16* A, int lda, const bf16* Bt, int ldb, int lane) {
-  const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-  for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-#pragma unroll
-  for (int k0 = 0; k0 < K; k0 += 16) {
-    unsigned a[4];
-    a[0] = *reinterpret_cast<const unsigned*>(A + g * lda + k0 + 2 * t);
-    a[1] = *reinterpret_cast<const unsigned*>(A + (g + 8) * lda + k0 + 2 * t);
-    a[2] = *reinterpret_cast<const unsigned*>(A + g * lda + k0 + 8 + 2 * t);
-    a[3] = *reinterpret_cast<const unsigned*>(A + (g + 8) * lda + k0 + 8 + 2 * t);
-#pragma unroll
-    for (int nt = 0; nt < NT; ++nt) {
-      unsigned b[2];
-      const bf16* bp = Bt + (nt * 8 + g) * ldb + k0 + 2 * t;
-      b[0] = *reinterpret_cast<const unsigned*>(bp);
-      b[1] = *reinterpret_cast<const unsigned*>(bp + 8);
-      mma16816(acc[nt], a, b);
-    }
-  }
-}
-
 // ---- features of one point ------------------------------------------------------------------------
-// The building blocks below are shared by the thread-per-sample training kernel and the
+// The building blocks below are shared by the thread-per-sample training-sample kernel and the
 // warp-cooperative inference kernel; every element goes through the same arithmetic in both,
 // so training and inference features agree bit for bit.
 
@@ -434,65 +410,21 @@ __global__ void k_mlp_pack(const float* __restrict__ p, bf16* __restrict__ q) {
     } else if (e < P_W3N) {  // W3t[o][i] = W3[i][o]
       const int o = (e - P_W3T) / KP2, i = (e - P_W3T) % KP2;
       v = i < H ? p[OFF_W3 + i * N3 + o] : 0.f;
-    } else {  // W3n[i][o] = W3[i][o]
+    } else if (e < P_TW1) {  // W3n[i][o] = W3[i][o]
       const int r = e - P_W3N;
       v = p[OFF_W3 + r];
+    } else {  // the tile copies: element t of a tile with `rows` rows holds (row, k)
+      const bool w1 = e < P_TW2, w2 = !w1 && e < P_TW3;
+      const int t = e - (w1 ? P_TW1 : (w2 ? P_TW2 : P_TW3));
+      const int rows = w1 || w2 ? H : N3P;
+      const int cm = t / 64, w = t % 64;
+      const int row = (cm % (rows / 8)) * 8 + w / 8, k = (cm / (rows / 8)) * 8 + w % 8;
+      if (w1) v = p[OFF_W1 + k * H + row];
+      else if (w2) v = p[OFF_W2 + k * H + row];
+      else v = row < N3 ? p[OFF_W3 + k * N3 + row] : 0.f;
     }
     q[e] = __float2bfloat16_rn(v);
   }
-}
-
-// ---- shared forward of one 16-row warp tile ------------------------------------------------------
-// X (16 x XP bf16) -> h1, h2 (16 x KP2 bf16, activations), z1, z2 (pre-activations, fp32, optional),
-// y (16 x 3 fp32 in registers, held by lanes with (lane&3) < 2 as in the C fragment layout).
-struct MlpSmemW {
-  bf16* W1t;
-  bf16* W2t;
-  bf16* W3t;
-  const float* b;  // params (biases read from global/L1)
-};
-
-__device__ __forceinline__ void tile_forward(const bf16* X, bf16* h1, bf16* h2, float* z1s, float* z2s,
-                                             const MlpSmemW& w, const float* __restrict__ params, float (&y)[4],
-                                             int lane) {
-  const int g = lane >> 2, t = lane & 3;
-  float acc[16][4];
-  warp_gemm<16, K1>(acc, X, XP, w.W1t, KP1, lane);
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    const int c = nt * 8 + 2 * t;
-    const float b0 = params[OFF_B1 + c], b1v = params[OFF_B1 + c + 1];
-    const float z00 = acc[nt][0] + b0, z01 = acc[nt][1] + b1v, z10 = acc[nt][2] + b0, z11 = acc[nt][3] + b1v;
-    if (z1s) {
-      z1s[g * H + c] = z00; z1s[g * H + c + 1] = z01;
-      z1s[(g + 8) * H + c] = z10; z1s[(g + 8) * H + c + 1] = z11;
-    }
-    *reinterpret_cast<unsigned*>(h1 + g * KP2 + c) = pack2(silu(z00), silu(z01));
-    *reinterpret_cast<unsigned*>(h1 + (g + 8) * KP2 + c) = pack2(silu(z10), silu(z11));
-  }
-  __syncwarp();
-  warp_gemm<16, H>(acc, h1, KP2, w.W2t, KP2, lane);
-#pragma unroll
-  for (int nt = 0; nt < 16; ++nt) {
-    const int c = nt * 8 + 2 * t;
-    const float b0 = params[OFF_B2 + c], b1v = params[OFF_B2 + c + 1];
-    const float z00 = acc[nt][0] + b0, z01 = acc[nt][1] + b1v, z10 = acc[nt][2] + b0, z11 = acc[nt][3] + b1v;
-    if (z2s) {
-      z2s[g * H + c] = z00; z2s[g * H + c + 1] = z01;
-      z2s[(g + 8) * H + c] = z10; z2s[(g + 8) * H + c + 1] = z11;
-    }
-    *reinterpret_cast<unsigned*>(h2 + g * KP2 + c) = pack2(silu(z00), silu(z01));
-    *reinterpret_cast<unsigned*>(h2 + (g + 8) * KP2 + c) = pack2(silu(z10), silu(z11));
-  }
-  __syncwarp();
-  float a3[1][4];
-  warp_gemm<1, H>(a3, h2, KP2, w.W3t, KP2, lane);
-  // C fragment: rows g, g+8; cols 2t, 2t+1 (only cols < 3 are outputs)
-  const int c = 2 * t;
-  y[0] = a3[0][0] + (c < N3 ? params[OFF_B3 + c] : 0.f);
-  y[1] = a3[0][1] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
-  y[2] = a3[0][2] + (c < N3 ? params[OFF_B3 + c] : 0.f);
-  y[3] = a3[0][3] + (c + 1 < N3 ? params[OFF_B3 + c + 1] : 0.f);
 }
 
 // ---- inference, in two kernels ------------------------------------------------------------------
@@ -633,7 +565,6 @@ k_mlp_features(const vec4<T>* __restrict__ u4, int N, double L, const double* __
 // completes, while the CTA's first feature copy is in flight.
 constexpr int FT_THREADS = 512;
 constexpr int FT_GROUP = 256;                         // threads of a group
-constexpr int N3P = 16;                               // layer-3 N padded for M = 128
 constexpr int SM_W1 = 0;
 constexpr int SM_W2 = SM_W1 + H * K1 * 2;             // 53248
 constexpr int SM_W3 = SM_W2 + H * H * 2;              // + 32768
@@ -921,157 +852,476 @@ __global__ void k_phase_shift(const ld::cplx<T>* __restrict__ in, ld::cplx<T>* _
   }
 }
 
-// ---- training: forward + backward of a batch, per-CTA gradient partials ---------------------------
-// CTA = 4 warps = 64 samples.  B operands come straight from the packed weights in global memory
-// (L1/L2 resident); shared memory holds the CTA's X, H1, H2 (bf16), Z1, Z2 (fp32, overwritten by
-// dZ1, dZ2) and dY.  Weight gradients are fixed-order sums over the 64 rows (deterministic).
-constexpr int TWARPS = 4;
-constexpr int TB = TWARPS * 16;
-constexpr size_t SMEM_TRAIN = sizeof(bf16) * ((size_t)TB * XP + 2 * (size_t)TB * KP2) +
-                              sizeof(float) * (2 * (size_t)TB * H + (size_t)TB * 4);
+// ---- training on the 5th-generation tensor cores -----------------------------------------------
+// One CTA of 512 threads takes TBT = 128 samples of a batch (the M of every MMA) through the
+// forward and backward passes and writes its gradient partial; the partials are summed in a fixed
+// order afterwards (deterministic):
+//   forward  Z1 = X W1 + b1, H1 = bf16(SiLU(Z1)), Z2 = H1 W2 + b2, H2 = bf16(SiLU(Z2)),
+//            Y = H2 W3 + b3 (the MMAs and epilogue arithmetic of the inference kernel);
+//   dY       = 2 w (Y - T) / B on valid rows (zero on the padding rows of a partial tile);
+//   dZ2      = (dY W3^T) * SiLU'(Z2),  dZ1 = dH1 * SiLU'(Z1)   (FP32, in the epilogues);
+//   dW3 = H2^T dY, dW2 = H1^T dZ2, dH1 = dZ2 W2^T, dW1 = X^T dZ1 on the tensor cores.
+// The weight gradients contract over the samples: their operands are the shared tiles that the
+// forward MMAs read K-major (samples as rows), read MN-major (samples along K).  dY, dZ2 and dZ1
+// enter as two BF16 parts, hi = bf16(d) and lo = bf16(d - hi), accumulated into the same FP32
+// sums, so that the products carry about 16 bits of the FP32 values; X, H1, H2 and the weights are
+// BF16 already.  Bias gradients are column sums of the FP32 values: a butterfly over the 32 rows
+// of a warp, then the four row quadrants in order.
+// Warp w of the epilogues: TMEM lanes (samples, or weight rows for the gradients) 32 (w % 4) ..
+// + 31, columns 32 (w / 4) .. + 31.
+// TMEM columns (512): Z1 0..127, later dW1 rows 0..127; Z2 128..255, later dH1, later dW1 rows
+// 80..207; Y 256..271, later dW3; dW2 384..511.
+// Shared memory: W1 until layer 1 completes, then H1 | H2; W2; X; W3 until layer 3 completes,
+// then dZ hi | lo (dZ2, later dZ1); dY hi | lo (16 x 128 each).  The weights arrive as three bulk
+// copies of their tile-layout copies, the samples' rows as 16-byte asynchronous copies; dW2 and
+// dW1 leave as one bulk store per row from shared memory, the small gradients as plain stores.
+// Every wait is bounded (kWaitLimitMlp polls); a wait that runs out makes the CTA wait (bounded)
+// for the MMAs in flight, write NaN as its loss partial (the batch loss, and so the epoch loss,
+// become NaN) and free its tensor memory.
+constexpr int TR_THREADS = 512;
+constexpr int TR_PARTS = TR_THREADS / 128;            // column parts of the epilogues (4)
+constexpr int TR_COLS = H / TR_PARTS;                 // columns of a warp in the epilogues (32)
+constexpr int TBT = 128;                              // samples per CTA
+constexpr int TS_H1 = 0;                              // W1 (53248 B) until layer 1 completes
+constexpr int TS_H2 = TS_H1 + TBT * H * 2;            // 32768
+constexpr int TS_W2 = TS_H2 + TBT * H * 2;            // 65536
+constexpr int TS_X = TS_W2 + H * H * 2;               // 98304
+constexpr int TS_D = TS_X + TBT * K1 * 2;             // 151552: W3 until layer 3 completes, then dZ hi
+constexpr int TS_DLO = TS_D + TBT * H * 2;            // 184320
+constexpr int TS_Y = TS_DLO + TBT * H * 2;            // 217088: dY hi
+constexpr int TS_YLO = TS_Y + N3P * TBT * 2;          // 221184
+constexpr int TS_BIAS = TS_YLO + N3P * TBT * 2;       // 225280: b1 / 2, b2 / 2, b3 (272 floats)
+constexpr int TS_DYF = TS_BIAS + (2 * H + N3P) * 4;   // 226368: dY FP32 [128][4]
+constexpr int TS_CS = TS_DYF + TBT * 4 * 4;           // 228416: column sums of the quadrants [4][128]
+constexpr int TS_CS3 = TS_CS + 4 * H * 4;             // 230464: dY column sums [4][4]
+constexpr int TS_LOSS = TS_CS3 + 16 * 4;              // 230528: loss of warps 0..3
+constexpr int TS_BAR = TS_LOSS + 8 * 4;               // 230560
+constexpr int TS_TMEM = TS_BAR + 8;                   // 230568
+constexpr int TS_W3F = TS_TMEM + 8;                   // 230576: W3 columns 0..2 as FP32 [3][128]
+constexpr int TS_WBAR = TS_W3F + D_OUT * H * 4;       // 232112: the weights' bulk copies
+constexpr size_t SMEM_TRAIN_TC = TS_WBAR + 8;         // 232120
+// FP32 gradient rows staged for bulk stores, 16 bytes of padding per row (the rows of a warp's
+// 16-byte writes fall on distinct bank groups): dW2 over H1 | H2 | W2, dW1 over X | dZ
+constexpr int ST_ROW = H * 4 + 16;
+static_assert(H * ST_ROW <= TS_X && K1 * ST_ROW <= TS_Y - TS_X, "gradient staging");
+static_assert(SMEM_TRAIN_TC <= 227 * 1024, "training kernel exceeds shared memory");
+static_assert(H * K1 * 2 <= TS_W2 && N3P * H * 2 <= TBT * H * 2, "W1 / W3 overlays");
+constexpr unsigned T_Z1 = 0, T_Z2 = 128, T_Y = 256, T_DW2 = 384;
 
-__global__ void __launch_bounds__(TWARPS * 32)
-k_mlp_train(const bf16* __restrict__ Xg, const float* __restrict__ Tg, const float* __restrict__ Wg, long long nb,
-            float inv_norm,
-            const bf16* __restrict__ packed, const float* __restrict__ params, float* __restrict__ gpart,
-            float* __restrict__ lpart) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  bf16* X = reinterpret_cast<bf16*>(smem_raw);
-  bf16* h1 = X + TB * XP;
-  bf16* h2 = h1 + TB * KP2;
-  float* z1 = reinterpret_cast<float*>(h2 + TB * KP2);
-  float* z2 = z1 + TB * H;
-  float* dy = z2 + TB * H;  // [TB][4]
-  __shared__ float lw[TWARPS];
-  const long long r0 = (long long)blockIdx.x * TB;
-  for (int e = threadIdx.x; e < TB * K1 / 2; e += blockDim.x) {
-    const int r = e / (K1 / 2), k2 = e % (K1 / 2);
-    unsigned v = 0u;
-    if (r0 + r < nb) v = reinterpret_cast<const unsigned*>(Xg + (r0 + r) * K1)[k2];
-    reinterpret_cast<unsigned*>(X + r * XP)[k2] = v;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane >> 2, t = lane & 3;
-  const bf16* W1t = packed + P_W1T;
-  const bf16* W2t = packed + P_W2T;
-  const bf16* W2n = packed + P_W2N;
-  const bf16* W3t = packed + P_W3T;
-  const bf16* W3n = packed + P_W3N;
-  MlpSmemW w{const_cast<bf16*>(W1t), const_cast<bf16*>(W2t), const_cast<bf16*>(W3t), params};
-  float y[4];
-  const int rw = warp * 16;
-  tile_forward(X + rw * XP, h1 + rw * KP2, h2 + rw * KP2, z1 + rw * H, z2 + rw * H, w, params, y, lane);
-  // dY = 2 w (Y - T) / B on valid rows (zero elsewhere); loss partial
-  float lsum = 0.f;
+// h = fma(0.5, acc, b / 2) (= z / 2 exactly) and SiLU(z) = fma(h, tanh(h), h) on 32 columns, as the
+// inference epilogue computes them, packed to 16 BF16 pairs
+__device__ __forceinline__ void silu_pack32(const float (&v)[32], const float* bh, unsigned (&w)[16]) {
+  const float4* b4p = reinterpret_cast<const float4*>(bh);
 #pragma unroll
-  for (int hh = 0; hh < 2; ++hh) {
-    const int r = rw + g + 8 * hh;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = 2 * t + q;
-      float d = 0.f;
-      if (c < D_OUT && r0 + r < nb) {
-        const float e = y[2 * hh + q] - Tg[(r0 + r) * 3 + c];
-        const float wr = Wg ? Wg[r0 + r] : 1.f;
-        lsum += wr * e * e;
-        d = 2.f * e * wr * inv_norm;
-      }
-      if (c < 4) dy[r * 4 + c] = d;
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-  if (lane == 0) lw[warp] = lsum;
-  __syncthreads();
-  float* G = gpart + (long long)blockIdx.x * N_PARAMS;
-  // dW3[i][c] = sum_r H2[r][i] dY[r][c];  db3[c] = sum_r dY[r][c]
-  for (int e = threadIdx.x; e < H * N3; e += blockDim.x) {
-    const int i = e / N3, c = e % N3;
-    float s = 0.f;
-    if (c < D_OUT)
-      for (int r = 0; r < TB; ++r) s += __bfloat162float(h2[r * KP2 + i]) * dy[r * 4 + c];
-    G[OFF_W3 + e] = s;
-  }
-  for (int c = threadIdx.x; c < N3; c += blockDim.x) {
-    float s = 0.f;
-    if (c < D_OUT)
-      for (int r = 0; r < TB; ++r) s += dy[r * 4 + c];
-    G[OFF_B3 + c] = s;
-  }
-  __syncthreads();
-  // dZ2 = (dY W3^T) * silu'(Z2)  (fp32, in z2) and as bf16 rows in h2 (A operand of dH1)
-  for (int e = threadIdx.x; e < TB * H; e += blockDim.x) {
-    const int r = e / H, i = e % H;
-    float s = 0.f;
-#pragma unroll
-    for (int c = 0; c < D_OUT; ++c) s += dy[r * 4 + c] * __bfloat162float(W3n[i * N3 + c]);
-    const float d = s * dsilu(z2[r * H + i]);
-    z2[r * H + i] = d;
-  }
-  __syncthreads();
-  // dW2[i][o] = sum_r H1[r][i] dZ2[r][o];  db2[o] = sum_r dZ2[r][o]
-  for (int e = threadIdx.x; e < H * H; e += blockDim.x) {
-    const int i = e / H, o = e % H;
-    float s = 0.f;
-    for (int r = 0; r < TB; ++r) s += __bfloat162float(h1[r * KP2 + i]) * z2[r * H + o];
-    G[OFF_W2 + e] = s;
-  }
-  for (int o = threadIdx.x; o < H; o += blockDim.x) {
-    float s = 0.f;
-    for (int r = 0; r < TB; ++r) s += z2[r * H + o];
-    G[OFF_B2 + o] = s;
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < TB * H; e += blockDim.x) {
-    const int r = e / H, i = e % H;
-    h2[r * KP2 + i] = __float2bfloat16_rn(z2[r * H + i]);
-  }
-  __syncthreads();
-  // dH1 = dZ2 W2^T on the tensor cores (B^T[n=i][k=o] = W2[i][o] = W2n), then dZ1 = dH1 * silu'(Z1)
-  {
-    float acc[16][4];
-    warp_gemm<16, H>(acc, h2 + rw * KP2, KP2, W2n, KP2, lane);
-#pragma unroll
-    for (int nt = 0; nt < 16; ++nt) {
-      const int c = nt * 8 + 2 * t;
-      const int ra = rw + g, rb = rw + g + 8;
-      z1[ra * H + c] = acc[nt][0] * dsilu(z1[ra * H + c]);
-      z1[ra * H + c + 1] = acc[nt][1] * dsilu(z1[ra * H + c + 1]);
-      z1[rb * H + c] = acc[nt][2] * dsilu(z1[rb * H + c]);
-      z1[rb * H + c + 1] = acc[nt][3] * dsilu(z1[rb * H + c + 1]);
-    }
-  }
-  __syncthreads();
-  // dW1[k][o] = sum_r X[r][k] dZ1[r][o];  db1[o] = sum_r dZ1[r][o]
-  for (int e = threadIdx.x; e < K1 * H; e += blockDim.x) {
-    const int k = e / H, o = e % H;
-    float s = 0.f;
-    if (k < D_IN)
-      for (int r = 0; r < TB; ++r) s += __bfloat162float(X[r * XP + k]) * z1[r * H + o];
-    G[OFF_W1 + e] = s;
-  }
-  for (int o = threadIdx.x; o < H; o += blockDim.x) {
-    float s = 0.f;
-    for (int r = 0; r < TB; ++r) s += z1[r * H + o];
-    G[OFF_B1 + o] = s;
-  }
-  for (int e = OFF_FS + threadIdx.x; e < N_PARAMS; e += blockDim.x) G[e] = 0.f;  // scales are not trained
-  if (threadIdx.x == 0) {
-    float l = 0.f;
-    for (int q = 0; q < TWARPS; ++q) l += lw[q];
-    lpart[blockIdx.x] = l;
+  for (int j = 0; j < 8; ++j) {
+    const float4 b4 = b4p[j];
+    const float2 h0 = __ffma2_rn(make_float2(0.5f, 0.5f), make_float2(v[4 * j], v[4 * j + 1]), make_float2(b4.x, b4.y));
+    const float2 h1 =
+        __ffma2_rn(make_float2(0.5f, 0.5f), make_float2(v[4 * j + 2], v[4 * j + 3]), make_float2(b4.z, b4.w));
+    const float2 s0 = __ffma2_rn(h0, make_float2(tanh_fast(h0.x), tanh_fast(h0.y)), h0);
+    const float2 s1 = __ffma2_rn(h1, make_float2(tanh_fast(h1.x), tanh_fast(h1.y)), h1);
+    w[2 * j] = pack2(s0.x, s0.y);
+    w[2 * j + 1] = pack2(s1.x, s1.y);
   }
 }
+
+// 32 FP32 values of one row -> the row's hi | lo BF16 parts in the tile layout (4 16-byte chunks each)
+__device__ __forceinline__ void store_split32(const float (&d)[32], unsigned char* hi, unsigned char* lo, int row,
+                                              int kc0) {
+  unsigned wh[16], wl[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(d[2 * j], d[2 * j + 1]);
+    const float2 hf = __bfloat1622float2(h);
+    wh[j] = *reinterpret_cast<const unsigned*>(&h);
+    wl[j] = pack2(d[2 * j] - hf.x, d[2 * j + 1] - hf.y);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    *reinterpret_cast<uint4*>(hi + blk_off(row, kc0 + c, TBT)) = make_uint4(wh[4 * c], wh[4 * c + 1], wh[4 * c + 2], wh[4 * c + 3]);
+    *reinterpret_cast<uint4*>(lo + blk_off(row, kc0 + c, TBT)) = make_uint4(wl[4 * c], wl[4 * c + 1], wl[4 * c + 2], wl[4 * c + 3]);
+  }
+}
+
+// Column sums over the 32 rows (lanes) of a warp: lane l returns the sum of v[l] over the lanes
+// (recursive halving: each step keeps half of the columns and adds the partner lane's half;
+// 31 shuffles, a fixed order).
+__device__ __forceinline__ float warp_colsum32(const float (&v)[32], int lane) {
+  float a[16], b[8], c[4], d[2];
+  const bool u16 = lane & 16, u8 = lane & 8, u4 = lane & 4, u2 = lane & 2, u1 = lane & 1;
+#pragma unroll
+  for (int j = 0; j < 16; ++j)
+    a[j] = (u16 ? v[16 + j] : v[j]) + __shfl_xor_sync(0xffffffffu, u16 ? v[j] : v[16 + j], 16);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) b[j] = (u8 ? a[8 + j] : a[j]) + __shfl_xor_sync(0xffffffffu, u8 ? a[j] : a[8 + j], 8);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) c[j] = (u4 ? b[4 + j] : b[j]) + __shfl_xor_sync(0xffffffffu, u4 ? b[j] : b[4 + j], 4);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) d[j] = (u2 ? c[2 + j] : c[j]) + __shfl_xor_sync(0xffffffffu, u2 ? c[j] : c[2 + j], 2);
+  return (u1 ? d[1] : d[0]) + __shfl_xor_sync(0xffffffffu, u1 ? d[0] : d[1], 1);
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Programmatic dependent launch: the next kernel in the stream may start (its CTAs wait in
+// grid_dep_wait until this grid has completed and its writes are visible); both are no-ops for a
+// kernel launched without the attribute.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// 16-byte asynchronous copy global -> shared; bytes < 16 zero-fills the rest (0: no read)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, unsigned bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
+               : "memory");
+}
+
+// every thread waits for the MMAs committed to bar (bounded); the outcome is made block-uniform
+__device__ __forceinline__ bool train_wait(uint64_t* bar, unsigned& ph) {
+  const bool ok = mbar_wait_bounded(bar, ph, kWaitLimitMlp);
+  ph ^= 1u;
+  const bool all_ok = __syncthreads_or(!ok) == 0;
+  tc_fence_after();
+  return all_ok;
+}
+
+__device__ __forceinline__ void train_sync() {
+  fence_proxy_async_smem();  // the epilogue's shared writes are read by the tensor cores
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+// Xg (n, K1) bf16 rows, Tg (n, 3), Wg (n) or null; sample r of the batch is row order[r] (or r
+// when order is null); nb samples.
+__global__ void __launch_bounds__(TR_THREADS, 1)
+k_mlp_train_tc(const bf16* __restrict__ Xg, const float* __restrict__ Tg, const float* __restrict__ Wg,
+               const unsigned* __restrict__ order, long long nb, float inv_norm, const bf16* __restrict__ packed,
+               const float* __restrict__ params, float* __restrict__ gpart, float* __restrict__ lpart) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q = warp & 3, part = warp >> 2;
+  const int row = 32 * q + lane;  // the thread's TMEM lane in the epilogues
+  const long long r0 = (long long)blockIdx.x * TBT;
+  float* bias = reinterpret_cast<float*>(sm + TS_BIAS);
+  float* dyf = reinterpret_cast<float*>(sm + TS_DYF);
+  float* cs = reinterpret_cast<float*>(sm + TS_CS);
+  float* cs3 = reinterpret_cast<float*>(sm + TS_CS3);
+  float* lw = reinterpret_cast<float*>(sm + TS_LOSS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + TS_BAR);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + TS_TMEM);
+  float* w3s = reinterpret_cast<float*>(sm + TS_W3F);
+  uint64_t* wbar = reinterpret_cast<uint64_t*>(sm + TS_WBAR);
+  float* G = gpart + (long long)blockIdx.x * N_PARAMS;
+  grid_dep_launch();
+  // the CTA's samples gathered by order (16-byte asynchronous copies, all in flight together;
+  // rows past nb: zero fill); thread t copies chunks of sample t % 128.  X, T, W and order are
+  // not written by the kernels of a training step: they load before the wait for the previous
+  // step's parameter update (programmatic dependent launch)
+  {
+    const int r = tid % TBT;
+    const bool valid = r0 + r < nb;
+    const long long src = valid ? (order ? (long long)order[r0 + r] : r0 + r) : 0;
+    const bf16* xrow = Xg + src * K1;
+#pragma unroll
+    for (int kc = tid / TBT; kc < K1 / 8; kc += TR_THREADS / TBT)
+      cp_async16(sm + TS_X + blk_off(r, kc, TBT), xrow + 8 * kc, valid ? 16u : 0u);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  grid_dep_wait();  // the parameters and their packed copies are final; gpart may be written
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_init(wbar, 1);
+    mbar_init_fence();
+    mbar_expect_tx(wbar, (H * K1 + H * H + N3P * H) * 2);
+    bulk_g2s(sm + TS_H1, packed + P_TW1, H * K1 * 2, wbar);
+    bulk_g2s(sm + TS_W2, packed + P_TW2, H * H * 2, wbar);
+    bulk_g2s(sm + TS_D, packed + P_TW3, N3P * H * 2, wbar);
+  }
+  for (int e = tid; e < 2 * N3P * TBT * 2 / 16; e += TR_THREADS)  // dY hi | lo: columns 3..15 stay zero
+    reinterpret_cast<uint4*>(sm + TS_Y)[e] = make_uint4(0u, 0u, 0u, 0u);
+  for (int e = tid; e < 2 * H + N3P; e += TR_THREADS)
+    bias[e] = e < H ? 0.5f * params[OFF_B1 + e]
+                    : (e < 2 * H ? 0.5f * params[OFF_B2 + e - H] : (e - 2 * H < N3 ? params[OFF_B3 + e - 2 * H] : 0.f));
+  for (int e = tid; e < D_OUT * H; e += TR_THREADS)  // the BF16 W3 of the forward, column-major
+    w3s[e] = __bfloat162float(packed[P_W3N + (e % H) * N3 + e / H]);
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  __syncthreads();  // the barriers are initialised
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  const bool wok = mbar_wait_bounded(wbar, 0u, kWaitLimitMlp);
+  fence_proxy_async_smem();
+  tc_fence_before();
+  bool ok = __syncthreads_or(!wok) == 0;
+  tc_fence_after();
+  const unsigned tmem = *tmem_slot;
+  const unsigned tl = tmem + ((unsigned)(32 * q) << 16);  // the warp's TMEM lanes
+  constexpr unsigned CM = (TBT / 8) * 128;                // chunk stride of a 128-row tile (2048 B)
+  constexpr unsigned IDK = umma_idesc_bf16(128, 128);     // A and B K-major
+  constexpr unsigned ID3 = umma_idesc_bf16(128, N3P);
+  constexpr unsigned IDW3 = ID3 | (1u << 15);             // A MN-major
+  constexpr unsigned IDH = IDK | (1u << 16);              // B MN-major
+  constexpr unsigned IDW = IDK | (1u << 15) | (1u << 16); // A and B MN-major
+  unsigned ph = 0;
+  do {
+    if (!ok) break;
+    // layer 1: Z1 = X W1
+    if (tid == 0) {
+#pragma unroll 1
+      for (int k = 0; k < K1 / 16; ++k)
+        umma_bf16(tmem + T_Z1, umma_desc(sm + TS_X + 2 * k * CM, CM, 128),
+                  umma_desc(sm + TS_H1 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), IDK, k > 0);
+      umma_commit(bar);
+    }
+    if (!(ok = train_wait(bar, ph))) break;
+    // H1 over W1 (consumed)
+#pragma unroll
+    for (int cc = 0; cc < TR_COLS / 32; ++cc) {
+      const int col0 = TR_COLS * part + 32 * cc;
+      float v[32];
+      unsigned w[16];
+      tmem_ld32(tl + T_Z1 + col0, v);
+      silu_pack32(v, bias + col0, w);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4*>(sm + TS_H1 + blk_off(row, col0 / 8 + c, TBT)) =
+            make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+    }
+    train_sync();
+    // layer 2: Z2 = H1 W2
+    if (tid == 0) {
+#pragma unroll 1
+      for (int k = 0; k < H / 16; ++k)
+        umma_bf16(tmem + T_Z2, umma_desc(sm + TS_H1 + 2 * k * CM, CM, 128),
+                  umma_desc(sm + TS_W2 + 2 * k * (H / 8) * 128, (H / 8) * 128, 128), IDK, k > 0);
+      umma_commit(bar);
+    }
+    if (!(ok = train_wait(bar, ph))) break;
+#pragma unroll
+    for (int cc = 0; cc < TR_COLS / 32; ++cc) {
+      const int col0 = TR_COLS * part + 32 * cc;
+      float v[32];
+      unsigned w[16];
+      tmem_ld32(tl + T_Z2 + col0, v);
+      silu_pack32(v, bias + H + col0, w);
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4*>(sm + TS_H2 + blk_off(row, col0 / 8 + c, TBT)) =
+            make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+    }
+    train_sync();
+    // layer 3: Y = H2 W3
+    if (tid == 0) {
+#pragma unroll 1
+      for (int k = 0; k < H / 16; ++k)
+        umma_bf16(tmem + T_Y, umma_desc(sm + TS_H2 + 2 * k * CM, CM, 128),
+                  umma_desc(sm + TS_D + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), ID3, k > 0);
+      umma_commit(bar);
+    }
+    if (!(ok = train_wait(bar, ph))) break;
+    // dY, the loss and db3 (warps 0..3: one sample per thread)
+    if (part == 0) {
+      float v[16];
+      tmem_ld16(tl + T_Y, v);
+      const long long gr = r0 + row;
+      const bool valid = gr < nb;
+      const long long src = valid ? (order ? (long long)order[gr] : gr) : 0;
+      const float wr = (valid && Wg) ? Wg[src] : 1.f;
+      float d[3], ls = 0.f;
+#pragma unroll
+      for (int c = 0; c < D_OUT; ++c) {
+        d[c] = 0.f;
+        if (valid) {
+          const float e = (v[c] + bias[2 * H + c]) - Tg[src * 3 + c];
+          ls += wr * e * e;
+          d[c] = 2.f * e * wr * inv_norm;
+        }
+        dyf[row * 4 + c] = d[c];
+        // dY as the B operand of dW3 (N = output column, K = sample): 16-row K-major tile
+        const bf16 hi = __float2bfloat16_rn(d[c]);
+        const bf16 lo = __float2bfloat16_rn(d[c] - __bfloat162float(hi));
+        const int off = blk_off(c, row >> 3, N3P) + (row & 7) * 2;
+        *reinterpret_cast<bf16*>(sm + TS_Y + off) = hi;
+        *reinterpret_cast<bf16*>(sm + TS_YLO + off) = lo;
+      }
+      ls = warp_sum(ls);
+      const float s0 = warp_sum(d[0]), s1 = warp_sum(d[1]), s2 = warp_sum(d[2]);
+      if (lane == 0) {
+        lw[q] = ls;
+        cs3[4 * q] = s0;
+        cs3[4 * q + 1] = s1;
+        cs3[4 * q + 2] = s2;
+      }
+    }
+    __syncthreads();
+    // dZ2 = (dY W3^T) * SiLU'(Z2): hi | lo over the W3 tile (consumed); db2 quadrant sums
+    {
+      const float dy0 = dyf[row * 4], dy1 = dyf[row * 4 + 1], dy2 = dyf[row * 4 + 2];
+#pragma unroll
+      for (int cc = 0; cc < TR_COLS / 32; ++cc) {
+        const int col0 = TR_COLS * part + 32 * cc;
+        float v[32];
+        tmem_ld32(tl + T_Z2 + col0, v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int i = col0 + j;
+          float s = dy0 * w3s[i];
+          s = fmaf(dy1, w3s[H + i], s);
+          s = fmaf(dy2, w3s[2 * H + i], s);
+          const float z = 2.f * fmaf(0.5f, v[j], bias[H + i]);  // the forward's pre-activation, exactly
+          v[j] = s * dsilu(z);
+        }
+        store_split32(v, sm + TS_D, sm + TS_DLO, row, col0 / 8);
+        cs[q * H + col0 + lane] = warp_colsum32(v, lane);
+      }
+    }
+    train_sync();
+    // dW3 = H2^T dY, dH1 = dZ2 W2^T, dW2 = H1^T dZ2, each from the hi and the lo part
+    if (tid == 0) {
+#pragma unroll 1
+      for (int k = 0; k < TBT / 16; ++k)
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          const unsigned char* dz = sm + (part ? TS_DLO : TS_D);
+          const unsigned char* dy = sm + (part ? TS_YLO : TS_Y);
+          const unsigned acc = (k > 0 || part > 0) ? 1u : 0u;
+          // A: H2 with the samples along K (MN-major); B: the dY tile (K-major)
+          umma_bf16(tmem + T_Y, umma_desc(sm + TS_H2 + 2 * k * 128, 128, CM),
+                    umma_desc(dy + 2 * k * (N3P / 8) * 128, (N3P / 8) * 128, 128), IDW3, acc);
+          // A: dZ2 (K = hidden column o, K-major); B: the W2 tile (rows o) read with N = i (MN-major)
+          umma_bf16(tmem + T_Z2, umma_desc(dz + 2 * k * CM, CM, 128), umma_desc(sm + TS_W2 + 2 * k * 128, 128, CM),
+                    IDH, acc);
+          // A: H1, B: dZ2, both with the samples along K (MN-major)
+          umma_bf16(tmem + T_DW2, umma_desc(sm + TS_H1 + 2 * k * 128, 128, CM), umma_desc(dz + 2 * k * 128, 128, CM),
+                    IDW, acc);
+        }
+      umma_commit(bar);
+    }
+    static_assert(TR_THREADS >= 256 + (N_PARAMS - OFF_FS), "thread ranges of the partial writes");
+    if (tid >= 128 && tid < 256) {
+      const int o = tid - 128;
+      G[OFF_B2 + o] = ((cs[o] + cs[H + o]) + cs[2 * H + o]) + cs[3 * H + o];
+    } else if (tid >= 32 && tid < 32 + N3) {
+      const int c = tid - 32;
+      G[OFF_B3 + c] = c < D_OUT ? ((cs3[c] + cs3[4 + c]) + cs3[8 + c]) + cs3[12 + c] : 0.f;
+    } else if (tid >= 256 && tid < 256 + (N_PARAMS - OFF_FS)) {
+      G[OFF_FS + tid - 256] = 0.f;  // the scales are not trained
+    } else if (tid == 64) {
+      lpart[blockIdx.x] = ((lw[0] + lw[1]) + lw[2]) + lw[3];
+    }
+    if (!(ok = train_wait(bar, ph))) break;
+    // dZ1 = dH1 * SiLU'(Z1): hi | lo over dZ2 (consumed); db1 quadrant sums; dW2 and dW3 out
+#pragma unroll 1
+    for (int cc = 0; cc < TR_COLS / 32; ++cc) {
+      const int col0 = TR_COLS * part + 32 * cc;
+      float v[32], a1[32];
+      tmem_ld32(tl + T_Z2 + col0, v);
+      tmem_ld32(tl + T_Z1 + col0, a1);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] *= dsilu(2.f * fmaf(0.5f, a1[j], bias[col0 + j]));
+      store_split32(v, sm + TS_D, sm + TS_DLO, row, col0 / 8);
+      cs[q * H + col0 + lane] = warp_colsum32(v, lane);
+      tmem_ld32(tl + T_DW2 + col0, a1);  // dW2 row i = row, columns o: staged over H1 | H2 | W2 (consumed)
+      float4* s4 = reinterpret_cast<float4*>(sm + row * ST_ROW + col0 * 4);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s4[j] = make_float4(a1[4 * j], a1[4 * j + 1], a1[4 * j + 2], a1[4 * j + 3]);
+    }
+    if (part == 0) {
+      float v[16];
+      tmem_ld16(tl + T_Y, v);  // dW3 row i = row, columns c (3..7 are zero)
+      float4* g4 = reinterpret_cast<float4*>(G + OFF_W3 + row * N3);
+      g4[0] = make_float4(v[0], v[1], v[2], v[3]);
+      g4[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+    train_sync();
+    if (tid < H) {  // dW2 rows out
+      bulk_s2g(G + OFF_W2 + tid * H, sm + tid * ST_ROW, H * 4);
+      bulk_commit();
+    }
+    // dW1 = X^T dZ1: rows k 0..127 (X chunks 0..15) and 80..207 (chunks 10..25)
+    if (tid == 0) {
+#pragma unroll 1
+      for (int k = 0; k < TBT / 16; ++k)
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+          const unsigned char* dz = sm + (part ? TS_DLO : TS_D);
+          const unsigned acc = (k > 0 || part > 0) ? 1u : 0u;
+          umma_bf16(tmem + T_Z1, umma_desc(sm + TS_X + 2 * k * 128, 128, CM), umma_desc(dz + 2 * k * 128, 128, CM),
+                    IDW, acc);
+          umma_bf16(tmem + T_Z2, umma_desc(sm + TS_X + 10 * CM + 2 * k * 128, 128, CM),
+                    umma_desc(dz + 2 * k * 128, 128, CM), IDW, acc);
+        }
+      umma_commit(bar);
+    }
+    if (tid >= 128 && tid < 256) {
+      const int o = tid - 128;
+      G[OFF_B1 + o] = ((cs[o] + cs[H + o]) + cs[2 * H + o]) + cs[3 * H + o];
+    }
+    if (!(ok = train_wait(bar, ph))) break;
+    {
+      // parts 0 .. TR_PARTS/2 - 1: rows 0..127; the others: rows 80..207, stored from 128
+      constexpr int HP = TR_PARTS / 2, CW = H / HP;
+      const bool upper = part >= HP;
+      const int kr = upper ? 80 + row : row;  // the thread's dW1 row
+      const unsigned tc = (upper ? T_Z2 : T_Z1) + CW * (part % HP);
+      const bool st = !upper || kr >= 128;
+#pragma unroll 1
+      for (int cc = 0; cc < CW / 32; ++cc) {
+        float v[32];
+        tmem_ld32(tl + tc + 32 * cc, v);
+        if (st) {  // staged over X | dZ (consumed)
+          float4* s4 = reinterpret_cast<float4*>(sm + TS_X + kr * ST_ROW + (CW * (part % HP) + 32 * cc) * 4);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            s4[j] = kr < D_IN ? make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3])
+                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid < K1) {  // dW1 rows out
+      bulk_s2g(G + OFF_W1 + tid * H, sm + TS_X + tid * ST_ROW, H * 4);
+      bulk_commit();
+    }
+  } while (false);
+  if (!ok && tid == 0) {
+    mbar_wait_bounded(bar, ph ^ 1u, kWaitLimitMlp);  // the commit that was not seen
+    mbar_wait_bounded(wbar, 0u, kWaitLimitMlp);      // the weights' copies
+  }
+  bulk_wait_all();  // this thread's bulk stores have left shared memory
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (!ok && tid == 0) lpart[blockIdx.x] = __int_as_float(0x7fc00000);
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// sum_b gpart[b][e] in the order b = 0, 1, ..., with 32 loads in flight at a time
+__device__ __forceinline__ float sum_partials(const float* __restrict__ gpart, int nblk, int e) {
+  float s = 0.f;
+  for (int b0 = 0; b0 < nblk; b0 += 32) {
+    float t[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) t[j] = b0 + j < nblk ? gpart[(long long)(b0 + j) * N_PARAMS + e] : 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (b0 + j < nblk) s += t[j];
+  }
+  return s;
+}
+
 
 // Fixed-order sum of the per-CTA partials: grad[e] = sum_b gpart[b][e]; loss = sum_b lpart[b] / norm.
 __global__ void k_mlp_reduce(const float* __restrict__ gpart, const float* __restrict__ lpart, int nblk,
                              float* __restrict__ grad, float* __restrict__ loss, float inv_norm) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int b = 0; b < nblk; ++b) s += gpart[(long long)b * N_PARAMS + e];
-    grad[e] = s;
-  }
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x)
+    grad[e] = sum_partials(gpart, nblk, e);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     float l = 0.f;
     for (int b = 0; b < nblk; ++b) l += lpart[b];
@@ -1079,22 +1329,66 @@ __global__ void k_mlp_reduce(const float* __restrict__ gpart, const float* __res
   }
 }
 
-// Adam on the FP32 master weights; padded rows/columns stay zero.
+// Adam on the FP32 master weight e (gradient gg); padded rows/columns stay zero.  Returns false
+// for a padded entry.
+__device__ __forceinline__ bool adam_one(int e, float gg, float* __restrict__ p, float* __restrict__ m,
+                                         float* __restrict__ v, float lr, float b1, float b2, float eps, float c1,
+                                         float c2) {
+  bool pad = false;
+  if (e < OFF_B1) pad = (e - OFF_W1) / H >= D_IN;
+  else if (e >= OFF_W3 && e < OFF_B3) pad = (e - OFF_W3) % N3 >= D_OUT;
+  else if (e >= OFF_B3) pad = (e - OFF_B3) >= D_OUT;
+  if (pad) {
+    p[e] = 0.f;
+    return false;
+  }
+  const float mm = b1 * m[e] + (1.f - b1) * gg;
+  const float vv = b2 * v[e] + (1.f - b2) * gg * gg;
+  m[e] = mm;
+  v[e] = vv;
+  p[e] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  return true;
+}
+
 __global__ void k_mlp_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                            float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < N_PARAMS; e += gridDim.x * blockDim.x) {
-    if (e >= OFF_FS) continue;  // feature and output scales: fixed
-    bool pad = false;
-    if (e < OFF_B1) pad = (e - OFF_W1) / H >= D_IN;
-    else if (e >= OFF_W3 && e < OFF_B3) pad = (e - OFF_W3) % N3 >= D_OUT;
-    else if (e >= OFF_B3) pad = (e - OFF_B3) >= D_OUT;
-    if (pad) { p[e] = 0.f; continue; }
-    const float gg = g[e];
-    const float mm = b1 * m[e] + (1.f - b1) * gg;
-    const float vv = b2 * v[e] + (1.f - b2) * gg * gg;
-    m[e] = mm;
-    v[e] = vv;
-    p[e] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < OFF_FS; e += gridDim.x * blockDim.x)  // scales: fixed
+    adam_one(e, g[e], p, m, v, lr, b1, b2, eps, c1, c2);
+}
+
+// One training step after k_mlp_train_tc: the fixed-order sum of the CTA partials (as
+// k_mlp_reduce), Adam, and the BF16 copies of each changed weight written where k_mlp_pack puts
+// them (its zero padding stays); thread 0 of block 0 adds the batch loss to *loss_acc.
+__global__ void k_mlp_reduce_adam(const float* __restrict__ gpart, const float* __restrict__ lpart, int nblk,
+                                  float inv_norm, float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                                  bf16* __restrict__ q, float lr, float b1, float b2, float eps, float c1, float c2,
+                                  float* __restrict__ loss_acc) {
+  grid_dep_launch();
+  grid_dep_wait();  // the training kernel's partials are complete
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < OFF_FS; e += gridDim.x * blockDim.x) {
+    const float gg = sum_partials(gpart, nblk, e);
+    if (!adam_one(e, gg, p, m, v, lr, b1, b2, eps, c1, c2)) continue;
+    const bf16 w = __float2bfloat16_rn(p[e]);
+    if (e < OFF_B1) {
+      const int k = (e - OFF_W1) / H, o = (e - OFF_W1) % H;
+      q[P_W1T + o * KP1 + k] = w;
+      q[P_TW1 + tile_elem(o, k, H)] = w;
+    } else if (e >= OFF_W2 && e < OFF_B2) {
+      const int i = (e - OFF_W2) / H, o = (e - OFF_W2) % H;
+      q[P_W2T + o * KP2 + i] = w;
+      q[P_W2N + i * KP2 + o] = w;
+      q[P_TW2 + tile_elem(o, i, H)] = w;
+    } else if (e >= OFF_W3 && e < OFF_B3) {
+      const int i = (e - OFF_W3) / N3, c = (e - OFF_W3) % N3;
+      q[P_W3T + c * KP2 + i] = w;
+      q[P_W3N + i * N3 + c] = w;
+      q[P_TW3 + tile_elem(c, i, N3P)] = w;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    float l = 0.f;
+    for (int b = 0; b < nblk; ++b) l += lpart[b];
+    *loss_acc = __fadd_rn(*loss_acc, __fmul_rn(l, inv_norm));  // as the batch loss of k_mlp_reduce, then added
   }
 }
 
@@ -1140,6 +1434,21 @@ __global__ void k_interleave3(const T* __restrict__ in, vec4<T>* __restrict__ ou
     out[i] = mk4<T>(in[i], in[m + i], in[2 * m + i], T(0));
 }
 
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 inline int gridn(long long n, int th) {
   long long b = (n + th - 1) / th;
   if (b > 148LL * 16) b = 148LL * 16;
@@ -1154,7 +1463,7 @@ int ld_mlp_sizes(int64_t* n_params, int64_t* n_packed, int32_t* k_in, int32_t* b
   if (n_params) *n_params = N_PARAMS;
   if (n_packed) *n_packed = N_PACKED;
   if (k_in) *k_in = K1;
-  if (batch_tile) *batch_tile = TB;
+  if (batch_tile) *batch_tile = TBT;
   return LD_OK;
 }
 
@@ -1326,21 +1635,50 @@ int ld_droplet_update(ld_plan* p, int stage, const void* up, double* pos, void* 
   return LD_OK;
 }
 
-int64_t ld_mlp_partial_floats(int64_t nb) { return ((nb + TB - 1) / TB) * (int64_t)(N_PARAMS + 1); }
+int64_t ld_mlp_partial_floats(int64_t nb) { return ((nb + TBT - 1) / TBT) * (int64_t)(N_PARAMS + 1); }
 
 int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb, const float* params, const void* packed,
                 float* work, float* grad, float* loss, void* stream) {
   if (!X || !T || nb < 1 || !params || !packed || !work || !grad || !loss)
     return ld_fail(LD_ERR_ARG, "ld_mlp_grad: bad arguments");
   cudaStream_t s = (cudaStream_t)stream;
-  const int nblk = (int)((nb + TB - 1) / TB);
+  const int nblk = (int)((nb + TBT - 1) / TBT);
   float* gpart = work;
   float* lpart = work + (long long)nblk * N_PARAMS;
   const float inv_norm = 1.f / (float)nb;
-  LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN));
-  k_mlp_train<<<nblk, TWARPS * 32, SMEM_TRAIN, s>>>((const bf16*)X, T, W, nb, inv_norm, (const bf16*)packed,
-                                                    params, gpart, lpart);
+  LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN_TC));
+  k_mlp_train_tc<<<nblk, TR_THREADS, SMEM_TRAIN_TC, s>>>((const bf16*)X, T, W, nullptr, nb, inv_norm,
+                                                        (const bf16*)packed, params, gpart, lpart);
   k_mlp_reduce<<<gridn(N_PARAMS, 256), 256, 0, s>>>(gpart, lpart, nblk, grad, loss, inv_norm);
+  LD_LAUNCH_CHECK();
+  return LD_OK;
+}
+
+int ld_mlp_train_epoch(const void* X, const float* T, const float* W, const uint32_t* order, int64_t nbatch,
+                       int64_t batch, float* params, void* packed, float* m, float* v, int64_t step0, double lr,
+                       double lr_final, int64_t total, float* work, float* loss_acc, void* stream) {
+  if (!X || !T || !order || nbatch < 0 || batch < 1 || batch > (1LL << 30) || !params || !packed || !m || !v ||
+      step0 < 0 || !(lr > 0.0) || total < 1 || !work || !loss_acc)
+    return ld_fail(LD_ERR_ARG, "ld_mlp_train_epoch: bad arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nblk = (int)((batch + TBT - 1) / TBT);
+  float* gpart = work;
+  float* lpart = work + (long long)nblk * N_PARAMS;
+  const float inv_norm = 1.f / (float)batch;
+  const float b1 = 0.9f, b2 = 0.999f;
+  LD_CUDA_CHECK(cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_TRAIN_TC));
+  for (int64_t b = 0; b < nbatch; ++b) {
+    const int64_t k = step0 + b + 1;  // Adam step of this batch
+    const double lrk = lr_final > 0.0 ? lr * pow(lr_final / lr, (double)(k < total ? k : total) / (double)total) : lr;
+    const float c1 = 1.f - powf(b1, (float)k), c2 = 1.f - powf(b2, (float)k);
+    // each launch may begin while the previous one finishes (programmatic dependent launch)
+    LD_CUDA_CHECK(launch_pdl(k_mlp_train_tc, nblk, TR_THREADS, SMEM_TRAIN_TC, s, (const bf16*)X, T, W,
+                             order + b * batch, (long long)batch, inv_norm, (const bf16*)packed, params, gpart,
+                             lpart));
+    LD_CUDA_CHECK(launch_pdl(k_mlp_reduce_adam, gridn(OFF_FS, 256), 256, 0, s, (const float*)gpart,
+                             (const float*)lpart, nblk, inv_norm, params, m, v, (bf16*)packed, (float)lrk, b1, b2,
+                             1e-8f, c1, c2, loss_acc));
+  }
   LD_LAUNCH_CHECK();
   return LD_OK;
 }

@@ -19,6 +19,7 @@ drives the kernels of csrc/ld_mlp.cu:
   tricubic (off only when it misses the tolerance and loses to tricubic).
 """
 import ctypes
+import time
 
 import numpy as np
 
@@ -41,6 +42,9 @@ def sizes():
 
 
 D_IN, H, D_OUT, K1, N3 = 195, 128, 3, 208, 8
+# algorithmic FLOPs of one training sample: forward 2 (195*128 + 128*128 + 128*3), backward the
+# weight gradients and the two activation gradients 2 (128*3 + 3*128 + 128*128 + 128*128 + 195*128)
+TRAIN_FLOP_PER_SAMPLE = 2 * (D_IN * H + H * H + H * D_OUT) + 2 * (2 * H * D_OUT + 2 * H * H + D_IN * H)
 OFF_W1 = 0
 OFF_B1 = OFF_W1 + K1 * H
 OFF_W2 = OFF_B1 + H
@@ -223,38 +227,35 @@ class LearnedInterp:
 
     def train(self, X, T, W=None, epochs=1, batch=4096, lr=1e-3, lr_final=None, seed=0, log_every=0):
         """Adam over shuffled mini-batches; returns the per-epoch mean loss (host floats).  W: sample
-        weights, used normalised to mean 1."""
+        weights, used normalised to mean 1.  Each epoch is one native call (ld_mlp_train_epoch: per
+        batch, the tensor-core forward/backward kernel on the permuted rows, then the fixed-order
+        gradient sum fused with Adam and the BF16 re-pack)."""
         torch = _torch()
         n = int(X.shape[0])
+        if n < 1:
+            raise ValueError("MLP training: no samples")
         L = _lib.lib()
-        work = torch.empty(int(L.ld_mlp_partial_floats(batch)), dtype=torch.float32, device=self.plan.device)
-        xb = torch.empty((batch, K1), dtype=torch.bfloat16, device=self.plan.device)
-        tb = torch.empty((batch, 3), dtype=torch.float32, device=self.plan.device)
-        wn = wb = None
-        if W is not None:
-            wn = (W / W.mean()).contiguous()
-            wb = torch.empty(batch, dtype=torch.float32, device=self.plan.device)
-        g = torch.Generator(device="cpu").manual_seed(seed)
-        nbatch = max(1, n // batch)
+        dev = self.plan.device
+        wn = (W / W.mean()).contiguous() if W is not None else None
+        g = torch.Generator(device=dev).manual_seed(seed)  # the permutations are drawn on the device
+        batch = min(batch, n)  # fewer samples than a batch: one batch of all of them
+        nbatch = n // batch
         total = epochs * nbatch
+        work = torch.empty(int(L.ld_mlp_partial_floats(batch)), dtype=torch.float32, device=dev)
         out = []
         for ep in range(epochs):
-            perm = torch.randperm(n, generator=g).to(torch.int32).to(self.plan.device)
-            acc = torch.zeros(1, dtype=torch.float32, device=self.plan.device)
-            for b in range(nbatch):
-                idx = perm[b * batch:(b + 1) * batch]
-                check(L.ld_permute_rows(ptr(X), ptr(xb), ptr(idx), batch, K1 * 2, stream_ptr()))
-                check(L.ld_permute_rows(ptr(T), ptr(tb), ptr(idx), batch, 12, stream_ptr()))
-                if wn is not None:
-                    check(L.ld_permute_rows(ptr(wn), ptr(wb), ptr(idx), batch, 4, stream_ptr()))
-                self.loss_and_grad(xb, tb, wb, work)
-                acc += self.loss
-                self.step_count += 1
-                k = self.step_count
-                lr_k = lr if lr_final is None else lr * (lr_final / lr) ** (min(k, total) / total)
-                check(L.ld_mlp_adam(ptr(self.params), ptr(self.grad), ptr(self.m), ptr(self.v), k, float(lr_k),
-                                    ptr(self.packed), stream_ptr()))
-            out.append(float(acc.item()) / nbatch)
+            perm = torch.randperm(n, generator=g, device=dev).to(torch.int32)
+            acc = torch.zeros(1, dtype=torch.float32, device=dev)
+            check(L.ld_mlp_train_epoch(ptr(X), ptr(T), ptr(wn) if wn is not None else None, ptr(perm), nbatch, batch,
+                                       ptr(self.params), ptr(self.packed), ptr(self.m), ptr(self.v), self.step_count,
+                                       float(lr), float(lr_final) if lr_final is not None else 0.0, max(total, 1),
+                                       ptr(work), ptr(acc), stream_ptr()))
+            self.step_count += nbatch
+            loss = float(acc.item()) / max(nbatch, 1)
+            if not np.isfinite(loss):
+                raise RuntimeError("MLP training: non-finite epoch loss (diverged, or a kernel gave up a "
+                                   "bounded wait)")
+            out.append(loss)
             if log_every and (ep + 1) % log_every == 0:
                 print(f"epoch {ep + 1}: loss {out[-1]:.4e}")
         return out
@@ -270,6 +271,8 @@ class LearnedInterp:
         ns = len(snapshots)
         n_shifts = max(1, int(n_pairs) // (ns * per_shift))
         total = ns * n_shifts * per_shift
+        torch.cuda.synchronize(p.device)
+        t0 = time.perf_counter()
         self.calibrate(snapshots[-1], seed=seed + 7)
         X = torch.empty((total, K1), dtype=torch.bfloat16, device=p.device)
         T = torch.empty((total, 3), dtype=torch.float32, device=p.device)
@@ -278,13 +281,19 @@ class LearnedInterp:
             self.make_samples(uk, n_shifts, per_shift, seed=seed * 1009 + k, X=X, T=T, W=W,
                               offset=k * n_shifts * per_shift)
         self.normalise_targets(T, W)
+        torch.cuda.synchronize(p.device)
+        t1 = time.perf_counter()
         losses = []
         for ep in range(epochs):
             losses += self.train(X, T, W, epochs=1, batch=batch, lr=lr * decay ** ep, seed=seed * 1009 + ep)
             if log:
                 log(f"epoch {ep}: weighted loss {losses[-1]:.4e}")
+        t2 = time.perf_counter()  # train() read the last epoch's loss: the device is idle
         del X, T, W
-        return {"pairs": total, "snapshots": ns, "epochs": epochs, "batch": batch, "losses": losses}
+        trained = epochs * (total // min(batch, total)) * min(batch, total)
+        return {"pairs": total, "snapshots": ns, "epochs": epochs, "batch": batch, "losses": losses,
+                "samples_s": t1 - t0, "epochs_s": t2 - t1, "train_flop_per_sample": TRAIN_FLOP_PER_SAMPLE,
+                "train_tflops": trained * TRAIN_FLOP_PER_SAMPLE / (t2 - t1) / 1e12}
 
     # ---- judge ------------------------------------------------------------------------------------
     def judge(self, uk, u4, pos, n_sample=None, seed=0):

@@ -200,3 +200,51 @@ def test_inference_features_equal_training_features(torch):
     ax = wb[tiles * tile_bytes:].view(np.float32)[:8 * per].reshape(per, 8)
     a = aux.cpu().numpy()
     assert np.array_equal(ax[:, :3], a[:, :3]) and np.array_equal(ax[:, 3], a[:, 3])
+
+
+def test_epoch_call_equals_grad_then_adam(torch):
+    """ld_mlp_train_epoch (rows gathered inside the tensor-core kernel, the partial sums fused with
+    Adam and the BF16 re-pack) against ld_mlp_grad then ld_mlp_adam on the gathered rows, batch
+    by batch: bit-identical parameters, moments, packed copy and epoch losses."""
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    from lucky_droplets_b200 import _lib
+    from lucky_droplets_b200._lib import check, ptr, stream_ptr
+    rng = np.random.default_rng(4)
+    n, batch, epochs, lr, lr_final = 1000, 300, 2, 1e-3, 1e-4  # 300 = 2 x 128 + 44: a partial tile
+    X = np.zeros((n, G.K1), np.float32)
+    X[:, :M.D_IN] = rng.standard_normal((n, M.D_IN))
+    T = rng.standard_normal((n, 3)).astype(np.float32) * 0.3
+    W = rng.uniform(0.1, 3.0, n).astype(np.float32)
+    p = M.init_params(7)
+    flat = G.flat_from_mats(p["W1"], p["b1"], p["W2"], p["b2"], p["W3"], p["b3"])
+    plan = Plan(16, "f32")
+    a = G.LearnedInterp(plan, params=flat.copy())
+    b = G.LearnedInterp(plan, params=flat.copy())
+    Xg = torch.as_tensor(X).to("cuda", torch.bfloat16)
+    Tg = torch.as_tensor(T).cuda()
+    Wg = torch.as_tensor(W).cuda()
+    la = a.train(Xg, Tg, Wg, epochs=epochs, batch=batch, lr=lr, lr_final=lr_final, seed=5)
+    L = _lib.lib()
+    wn = (Wg / Wg.mean()).contiguous()
+    g = torch.Generator(device="cuda").manual_seed(5)
+    nbatch = n // batch
+    total = epochs * nbatch
+    lb = []
+    for _ in range(epochs):
+        perm = torch.randperm(n, generator=g, device="cuda").to(torch.int32)
+        acc = torch.zeros(1, dtype=torch.float32, device="cuda")
+        for k in range(nbatch):
+            idx = perm[k * batch:(k + 1) * batch].long()
+            loss, _ = b.loss_and_grad(Xg[idx].contiguous(), Tg[idx].contiguous(), wn[idx].contiguous())
+            acc += loss
+            b.step_count += 1
+            s = b.step_count
+            lr_k = lr * (lr_final / lr) ** (min(s, total) / total)
+            check(L.ld_mlp_adam(ptr(b.params), ptr(b.grad), ptr(b.m), ptr(b.v), s, float(lr_k), ptr(b.packed),
+                                stream_ptr()))
+        lb.append(float(acc.item()) / nbatch)
+    assert la == lb
+    for name in ("params", "m", "v", "packed"):
+        assert torch.equal(getattr(a, name), getattr(b, name)), name
+    assert la[-1] < la[0]
