@@ -444,14 +444,36 @@ __device__ __forceinline__ bool col_visit(int i, int t, const double4* __restric
     }
     const float ax = mf.x + shx[q], ay = mf.y + shy[q], az = mf.z + sz;
     const int d = dl[q];
-    for (int g = g0; g < g1; ++g) {
+    // two candidates at a time on packed FP32 pairs (each half rounds as the scalar operation);
+    // b - a instead of a - b: the squares are the same
+    const float2 nax = make_float2(-ax, -ax), nay = make_float2(-ay, -ay), naz = make_float2(-az, -az);
+    const float2 mw = make_float2(mf.w, mf.w), mr = make_float2(mar, mar);
+    int g = g0;
+    for (; g + 1 < g1; g += 2) {
+      const float4 b0 = STAGED ? colbuf[g - d] : spf[g];
+      const float4 b1 = STAGED ? colbuf[g + 1 - d] : spf[g + 1];
+      const float2 dx = __fadd2_rn(make_float2(b0.x, b1.x), nax), dy = __fadd2_rn(make_float2(b0.y, b1.y), nay),
+                   dz = __fadd2_rn(make_float2(b0.z, b1.z), naz);
+      const float2 rr = __fadd2_rn(__fadd2_rn(mw, make_float2(b0.w, b1.w)), mr);
+      const float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+      const float2 r2 = __fmul2_rn(rr, rr);
+      if (d2.x < r2.x && overlap_near(sp[i], sp[g], L, cw)) {
+        if (c < KEEP) scr[(long long)KEEP * i + c] = g;
+        ++c;
+      }
+      if (d2.y < r2.y && overlap_near(sp[i], sp[g + 1], L, cw)) {
+        if (c < KEEP) scr[(long long)KEEP * i + c] = g + 1;
+        ++c;
+      }
+    }
+    if (g < g1) {
       const float4 b = STAGED ? colbuf[g - d] : spf[g];
       const float dxf = ax - b.x, dyf = ay - b.y, dzf = az - b.z;
       const float rr = mf.w + b.w + mar;
-      if (dxf * dxf + dyf * dyf + dzf * dzf >= rr * rr) continue;
-      if (!overlap_near(sp[i], sp[g], L, cw)) continue;
-      if (c < KEEP) scr[(long long)KEEP * i + c] = g;
-      ++c;
+      if (dxf * dxf + dyf * dyf + dzf * dzf < rr * rr && overlap_near(sp[i], sp[g], L, cw)) {
+        if (c < KEEP) scr[(long long)KEEP * i + c] = g;
+        ++c;
+      }
     }
   }
   cnt[i] = c;
@@ -975,8 +997,9 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
     if (want > room) want = room;
     const int cap_smem = (int)want;
     const size_t smem = sizeof(float4) * (size_t)cap_smem + starts_bytes;
-    // blocks of 64 or 128 threads where columns hold few droplets (as the boxes of an ensemble
-    // do), 256 otherwise
+    // blocks of 64, 128 or 192 threads where columns hold few droplets (the boxes of an ensemble;
+    // about 150 per column at 1e6 droplets in 82^3 cells), 256 otherwise: threads without a
+    // droplet would only wait at the block's barriers
     if (per_col <= 64) {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_col_pairs<64><<<(unsigned)(ncol * parts), 64, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
@@ -984,6 +1007,12 @@ int ld_collide_boxes(ld_collider* c, const double* pos, const double* radius, co
     } else if (per_col <= 128) {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_col_pairs<128><<<(unsigned)(ncol * parts), 128, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
+                                                                   cw, cap_smem, c->cnt, c->scr);
+    } else if (per_col <= 192) {
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<192>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      // shared memory, not registers, would otherwise hold it to 5 blocks per SM
+      LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<192>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      k_col_pairs<192><<<(unsigned)(ncol * parts), 192, smem, s>>>(c->sp, c->spf, c->key, c->start, nc, (int)parts, L,
                                                                    cw, cap_smem, c->cnt, c->scr);
     } else {
       LD_CUDA_CHECK(cudaFuncSetAttribute(k_col_pairs<COL_THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize,

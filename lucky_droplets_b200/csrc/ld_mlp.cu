@@ -572,8 +572,8 @@ constexpr int SM_X = SM_W3 + N3P * H * 2;             // + 4096
 constexpr int SM_H0 = SM_X + TILE_X_BYTES;
 constexpr int SM_H1 = SM_H0 + TM * H * 2;
 constexpr int SM_BIAS = SM_H1 + TM * H * 2;           // b1[128], b2[128], b3[16]
-constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma[2], bar_stall
-constexpr int SM_TMEM = SM_BAR + 5 * 8;
+constexpr int SM_BAR = SM_BIAS + (2 * H + N3P) * 4;   // bar_x[2], bar_mma[2], bar_stall, bar_w
+constexpr int SM_TMEM = SM_BAR + 6 * 8;
 constexpr int SM_CNT = SM_TMEM + 16;
 constexpr size_t SMEM_FWD = SM_CNT + 8 * 4;
 constexpr unsigned TMEM_COLS = 512;                   // group g: columns 256 g .. 256 g + 143
@@ -612,67 +612,53 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
   uint64_t* bar_x = reinterpret_cast<uint64_t*>(sm + SM_BAR);
   uint64_t* bar_mma = bar_x + 2;
   uint64_t* bar_stall = bar_x + 4;  // completed by nothing: the first wait of a stall test
+  uint64_t* bar_w = bar_x + 5;      // the weights' bulk copies
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + SM_TMEM);
   // drain bookkeeping: X copies issued to / waited on each bar_x, MMA commits to / waits on each
   // bar_mma; each counter has one writer (a group leader; cnt[0] leaves out the first copy, which
   // thread 0 issues before the loop) and thread 0 reads them after the final barrier
   unsigned* cnt = reinterpret_cast<unsigned*>(sm + SM_CNT);  // [x_issued 2][x_waited 2][mma_commit 2][mma_wait 2]
-  // weights into the tile layout (from the packed, row-padded copies); consecutive threads take
-  // consecutive rows of one 16-byte K chunk, so that eight of them fill one 128-byte core-matrix
-  // line (a quarter-warp's stores on distinct banks; with chunks fastest the stores of a warp
-  // fell 2 KB apart, on the same banks)
-#pragma unroll 4
-  for (int e = tid; e < H * (K1 / 8); e += FT_THREADS) {
-    const int nrow = e % H, kc = e / H;
-    *reinterpret_cast<uint4*>(sm + SM_W1 + blk_off(nrow, kc, H)) =
-        *reinterpret_cast<const uint4*>(packed + P_W1T + nrow * KP1 + 8 * kc);
-  }
-#pragma unroll 4
-  for (int e = tid; e < H * (H / 8); e += FT_THREADS) {
-    const int nrow = e % H, kc = e / H;
-    *reinterpret_cast<uint4*>(sm + SM_W2 + blk_off(nrow, kc, H)) =
-        *reinterpret_cast<const uint4*>(packed + P_W2T + nrow * KP2 + 8 * kc);
-  }
-  for (int e = tid; e < N3P * (H / 8); e += FT_THREADS) {
-    const int nrow = e % N3P, kc = e / N3P;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (nrow < N3) v = *reinterpret_cast<const uint4*>(packed + P_W3T + nrow * KP2 + 8 * kc);
-    *reinterpret_cast<uint4*>(sm + SM_W3 + blk_off(nrow, kc, N3P)) = v;
-  }
   // b1, b2 halved: the epilogues form h = z / 2 = fma(0.5, acc, b / 2), which is exactly
   // 0.5 * (acc + b) (halving is exact), and SiLU(z) = h + h tanh(h); b3 as is
   for (int e = tid; e < 2 * H + N3P; e += FT_THREADS)
     bias[e] = e < H ? 0.5f * params[OFF_B1 + e]
                     : (e < 2 * H ? 0.5f * params[OFF_B2 + e - H] : (e - 2 * H < N3 ? params[OFF_B3 + e - 2 * H] : 0.f));
+  const long long ntiles = (n + TM - 1) / TM;
+  const long long mine = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // CTA's tiles
   if (tid == 0) {
     mbar_init(&bar_x[0], 1);
     mbar_init(&bar_x[1], 1);
     mbar_init(&bar_mma[0], 1);
     mbar_init(&bar_mma[1], 1);
     mbar_init(bar_stall, 1);
+    mbar_init(bar_w, 1);
     mbar_init_fence();
+    // the weights (their tile-layout copies) and the CTA's first feature tile, as bulk copies in
+    // flight together
+    mbar_expect_tx(bar_w, (H * K1 + H * H + N3P * H) * 2);
+    bulk_g2s(sm + SM_W1, packed + P_TW1, H * K1 * 2, bar_w);
+    bulk_g2s(sm + SM_W2, packed + P_TW2, H * H * 2, bar_w);
+    bulk_g2s(sm + SM_W3, packed + P_TW3, N3P * H * 2, bar_w);
+    if (mine > 0) {  // the first copy is counted at the end (x_issued[0] + 1)
+      mbar_expect_tx(&bar_x[0], TILE_X_BYTES);
+      bulk_g2s(sm + SM_X, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
+    }
   }
   if (tid < 8) cnt[tid] = 0u;
   if (warp == 0) {
     tmem_alloc(tmem_slot, TMEM_COLS);
     tmem_relinquish();
   }
-  fence_proxy_async_smem();  // the weights are read by the tensor cores
   tc_fence_before();
-  __syncthreads();
+  __syncthreads();  // the barriers are initialised
   tc_fence_after();
   const unsigned tmem = *tmem_slot + 256u * (unsigned)g;
   unsigned char* Hs = sm + (g ? SM_H1 : SM_H0);
   const float os = params[OFF_OS];
-  const long long ntiles = (n + TM - 1) / TM;
-  const long long mine = ntiles > blockIdx.x ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // CTA's tiles
   constexpr unsigned ID1 = umma_idesc_bf16(128, 128), ID3 = umma_idesc_bf16(128, N3P);
-  if (tid == 0 && mine > 0) {  // the first copy is counted at the end (x_issued[0] + 1)
-    mbar_expect_tx(&bar_x[0], TILE_X_BYTES);
-    bulk_g2s(sm + SM_X, Xg + blockIdx.x * (long long)TILE_X_BYTES, TILE_X_BYTES, &bar_x[0]);
-  }
   unsigned ph = 0;
-  bool failed = false;
+  // the weights are in shared memory before any MMA (group-uniform outcome)
+  bool failed = group_or(g, !mbar_wait_bounded(bar_w, 0u, wait_limit));
   for (long long i = g; i < mine && !failed; i += 2) {
     const long long tile = blockIdx.x + i * (long long)gridDim.x;
     // the output warps' aux rows (tricubic xyz, scale, frame code) load while the layers run
@@ -790,6 +776,7 @@ k_mlp_forward_tc(const unsigned char* __restrict__ Xg, const float* __restrict__
     // flight; wait for each barrier's outstanding completion (the k-th completion of a barrier
     // has parity k % 2) before the tensor memory is freed and the shared memory released
     if (tid == 0) {
+      mbar_wait_bounded(bar_w, 0u, kWaitLimitMlp);  // the weights' copies
       for (int b = 0; b < 2; ++b) {
         const unsigned x_issued = cnt[b] + (b == 0 && mine > 0 ? 1u : 0u);
         if (x_issued > cnt[2 + b]) mbar_wait_bounded(&bar_x[b], cnt[2 + b] & 1u, kWaitLimitMlp);
