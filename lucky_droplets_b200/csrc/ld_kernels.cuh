@@ -418,12 +418,16 @@ k_xfwd_update(UpdArgs<T> A, int ncols, const cplx<T>* __restrict__ tw) {
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  // the three components' loads in flight together, then their transforms (the registers of all
+  // three are live through the last transform either way)
   cplx<T> res[3][E];
 #pragma unroll
-  for (int f = 0; f < 3; ++f) {
+  for (int f = 0; f < 3; ++f)
 #pragma unroll
     for (int m = 0; m < E; ++m)
       res[f][m] = ok ? A.nl[f * A.nls + (long long)(j + NT * m) * ncols + col] : czero<cplx<T>>();
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
     if (f) __syncthreads();
     fft_run<T, N, E, false, false>(res[f], sbuf + c, TB, j, tw, SyncBlock());
   }
