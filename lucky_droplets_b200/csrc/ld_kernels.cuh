@@ -785,8 +785,10 @@ __device__ __forceinline__ void zcross_row(const cplx<T>* const* in, cplx<T>* sb
 
 // Fused z pass, one row unit per NTZ threads, rows read straight from global memory.
 // W: (6, N*N, Mzp) in; P: (3, N*N, Mzp) out.
+// 64-point FP32 rows (the ensemble's boxes): three CTAs per SM (80 registers, no spills; 86 and
+// two CTAs per SM without the bound: ensemble step 1.50 -> 1.42 ms)
 template <typename T, int N>
-__global__ void __launch_bounds__(Cfg<N>::ZTHREADS)
+__global__ void __launch_bounds__(Cfg<N>::ZTHREADS, (sizeof(T) == 4 && N == 64) ? 3 : 1)
 k_z_cross(const cplx<T>* __restrict__ W, cplx<T>* __restrict__ P, T* __restrict__ uphys, int ulayout, int Mzp,
           int kc, T s, const cplx<T>* __restrict__ tw, long long NR) {
   constexpr int NT = Cfg<N>::NTZ;
