@@ -25,7 +25,7 @@ def test_gradients_match_oracle(torch):
     from lucky_droplets_b200.spectral import Plan
     from lucky_droplets_b200 import mlp as G
     rng = np.random.default_rng(0)
-    nb = 200  # not a multiple of the 64-sample tile: padded rows must not contribute
+    nb = 200  # not a multiple of the 128-sample tile: padded rows must not contribute
     X = np.zeros((nb, G.K1), np.float32)
     X[:, :M.D_IN] = M.bf16(rng.standard_normal((nb, M.D_IN)).astype(np.float32))
     T = rng.standard_normal((nb, 3)).astype(np.float32) * 0.3
@@ -43,10 +43,10 @@ def test_gradients_match_oracle(torch):
     assert np.all(gm["fs"] == 0) and gm["os"] == 0  # the scales get no gradient
     ref_loss, ref = M.mse_loss_and_grads(p, X[:, :M.D_IN], T, w=w)
     assert abs(float(loss.item()) - ref_loss) / ref_loss < 1e-4
-    for k in ("W3", "b3", "W2", "b2"):
-        assert rel(gm[k], ref[k]) < 2e-3, k
-    for k in ("W1", "b1"):  # dH1 uses the BF16 dZ2 on the tensor cores
-        assert rel(gm[k], ref[k]) < 2e-2, k
+    # dY, dZ2 and dZ1 enter the tensor-core products as two BF16 parts (about 16 bits of the FP32
+    # values): every gradient within 1e-3 of the FP64 oracle (measured: 1e-5 .. 3e-4)
+    for k in ("W3", "b3", "W2", "b2", "W1", "b1"):
+        assert rel(gm[k], ref[k]) < 1e-3, k
 
 
 def _oracle_infer(u, pos, p, fs, os):
