@@ -248,3 +248,36 @@ def test_epoch_call_equals_grad_then_adam(torch):
     for name in ("params", "m", "v", "packed"):
         assert torch.equal(getattr(a, name), getattr(b, name)), name
     assert la[-1] < la[0]
+
+
+def test_packed_tile_copies(torch):
+    """The packed BF16 weights hold W1t, W2t and W3t twice: row-major with padded rows, and in the
+    tensor-core tile layout (8x8 core matrices, K-chunk major) that the kernels bulk-copy; the two
+    agree element for element and the padding is zero."""
+    from lucky_droplets_b200.spectral import Plan
+    from lucky_droplets_b200 import mlp as G
+    H, K1, N3, N3P, KP1, KP2 = 128, G.K1, 8, 16, 216, 136
+    P_W2T = H * KP1
+    P_W2N = P_W2T + H * KP2
+    P_W3T = P_W2N + H * KP2
+    P_W3N = P_W3T + N3 * KP2
+    P_TW1 = P_W3N + H * N3
+    P_TW2 = P_TW1 + H * K1
+    P_TW3 = P_TW2 + H * H
+    assert G.sizes()[1] == P_TW3 + N3P * H
+    p = M.init_params(11)
+    li = G.LearnedInterp(Plan(16, "f32"), params=G.flat_from_mats(p["W1"], p["b1"], p["W2"], p["b2"], p["W3"], p["b3"]))
+    q = li.packed.float().cpu().numpy()
+
+    def tile(start, rows, kdim):  # element (row, k) of a tile -> (rows, kdim) matrix
+        t = q[start:start + rows * kdim].reshape(kdim // 8, rows // 8, 8, 8)  # [kc][row/8][row%8][k%8]
+        return t.transpose(1, 2, 0, 3).reshape(rows, kdim)
+
+    w1t = q[:P_W2T].reshape(H, KP1)
+    assert np.array_equal(tile(P_TW1, H, K1), w1t[:, :K1]) and not w1t[:, K1:].any()
+    w2t = q[P_W2T:P_W2N].reshape(H, KP2)
+    assert np.array_equal(tile(P_TW2, H, H), w2t[:, :H])
+    w3t = q[P_W3T:P_W3N].reshape(N3, KP2)
+    t3 = tile(P_TW3, N3P, H)
+    assert np.array_equal(t3[:N3], w3t[:, :H]) and not t3[N3:].any()
+    assert np.array_equal(w1t[:, :M.D_IN], M.bf16(p["W1"]).T)  # W1t[o][k] = bf16(W1[k][o])
