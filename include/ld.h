@@ -321,7 +321,9 @@ LD_API int ld_mlp_grad(const void* X, const float* T, const float* W, int64_t nb
  * (step0 + b + 1, learning rate lr * (lr_final / lr)^(min(step, total) / total), or lr when
  * lr_final <= 0) updates params, m, v and the BF16 copy; *loss_acc += each batch loss.  work:
  * ld_mlp_partial_floats(batch) floats.  Same result as ld_mlp_grad then ld_mlp_adam per batch on
- * the gathered rows.  A batch whose kernel gave up a bounded wait adds NaN to *loss_acc. */
+ * the gathered rows.  order holds nbatch * batch row indices of X, T, W, each below their row
+ * count (the caller's permutation; the kernels read the rows it names unchecked).  A batch whose
+ * kernel gave up a bounded wait adds NaN to *loss_acc. */
 LD_API int ld_mlp_train_epoch(const void* X, const float* T, const float* W, const uint32_t* order, int64_t nbatch,
                               int64_t batch, float* params, void* packed, float* m, float* v, int64_t step0,
                               double lr, double lr_final, int64_t total, float* work, float* loss_acc, void* stream);
