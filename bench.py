@@ -664,9 +664,9 @@ def run_ours(a):
         train_s = fit_info["calibration_run_s"] + fit_info["fit_s"]
         out["training_cost"] = {
             "seconds": train_s, "production_steps_equivalent": train_s / (ms_per_step * 1e-3),
-            "note": "calibration run + sample generation + 16 epochs of Adam, once per configuration; not in "
-                    "value. It equals this many production steps of the timed step; a run of that many "
-                    "steps doubles its wall time, longer runs amortise it"}
+            "note": f"calibration run + sample generation + {fit_info['epochs']} epochs of Adam, once per "
+                    "configuration; not in value. It equals this many production steps of the timed step; a run "
+                    "of that many steps doubles its wall time, longer runs amortise it"}
     if not a.no_e2e:
         Ke = max(3, min(a.steps, 10))
         for layout, key in (("full", "e2e"), ("cube", "e2e_cube_layout")):
